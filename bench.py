@@ -1,0 +1,350 @@
+"""Benchmark of the per-step transport path (bulk -> cells -> LOD_3D diffusion).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (default): 256^3 voxels x 10 substrates FP64, 100k agents, central
+bulk sphere (biofvm_b200.workloads.lod_256), seeded synthetic inputs.  A step
+is one full transport step; the metric is voxel-substrate updates per second
+(N voxels x S substrates per step).  The 1.34 GB field is larger than L2
+(126 MB), so no L2 flush is needed between steps.
+
+N > 1 (torchrun, one process per GPU): every rank advances its own
+independent microenvironment of the same size (instances shard across GPUs
+with no data-path collective), so per-GPU work is fixed: weak scaling.  Time
+is the max over ranks of the device time.
+
+--impl reference times the unmodified BioFVM reference (compiled from its
+sources into oracle/_ref/) on this host's cores, on a bounded sample of the
+same workload, and prints the same metric.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "voxel-substrate updates/s per LOD step"
+UNIT = "voxel-substrate updates/s"
+BYTES_PER_VS_SWEEP = 16  # one FP64 read + one FP64 write per element per sweep
+BYTES_PER_VS_STEP = 3 * BYTES_PER_VS_SWEEP
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def ncu_traffic(kernel_key: str):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu
+    summary (a line `traffic_bytes_per_launch <kernel> <bytes> <units>`)."""
+    path = os.path.join(ROOT, "profiles", "lod_sweeps_lod256.md")
+    if not os.path.exists(path):
+        return None
+    pat = re.compile(r"traffic_bytes_per_launch\s+(\S+)\s+([0-9.eE+]+)")
+    with open(path) as f:
+        for line in f:
+            m = pat.search(line)
+            if m and m.group(1) == kernel_key:
+                return float(m.group(2))
+    return None
+
+
+def dist_init(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+
+def reference_sample(threads: int):
+    """A bounded sample of the headline workload for the CPU reference:
+    128^3 voxels x 10 substrates (1/8 of the voxels), agents at the same
+    density (12.5k), the bulk sphere at the same radius."""
+    from biofvm_b200 import workloads as W
+
+    return W.lod_cube(128, 10, 12_500, steps=1, name="lod_128_sample")
+
+
+def time_reference(steps: int, warmup: int, threads: int):
+    from oracle import oracle as O
+
+    variant = "v3" if (O.reference_available("v3") and _host_has_avx2()) else "core2"
+    scn = reference_sample(threads)
+    t0 = time.perf_counter()
+    ref = O.Reference(scn, variant, threads=threads, cells_single_thread=False)
+    setup = time.perf_counter() - t0
+    ref.run(warmup)
+    secs = ref.run(steps)
+    ref.close()
+    vs = scn.num_voxels * scn.S * steps / secs
+    return vs, secs, setup, variant, scn
+
+
+def _host_has_avx2() -> bool:
+    try:
+        with open("/proc/cpuinfo") as f:
+            flags = f.read()
+        return " avx2" in flags and " fma" in flags
+    except OSError:
+        return False
+
+
+def run_reference_arm(args, world, rank):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    # a step of the sample is ~0.05-0.5 s on a many-core host; keep the run bounded
+    steps = max(1, min(args.steps, 20))
+    warmup = max(1, min(args.warmup, 3))
+    vs, secs, setup, variant, scn = time_reference(steps, warmup, threads)
+    sample = (f"{scn.shape[0]}^3 x {scn.S} substrates, {scn.num_agents} agents, {steps} timed "
+              f"steps after {warmup} warm-up (1/8 of the 256^3 workload's voxels, same density "
+              f"of agents); reference build {variant}; OpenMP threads {threads}")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": vs, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": steps, "warmup": warmup, "ms_per_step": 1e3 * secs / steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded)",
+        "config": {"workload": "lod_256 sample: lod_128 (256^3 x 10 FP64 workload at 1/8 the "
+                               "voxels)", "threads": threads},
+        "cpu_baseline": {"value": vs, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": vs, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "setup_s": setup,
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+
+def run_ours(args, world, rank, local):
+    import numpy as np
+    import torch
+
+    from biofvm_b200 import STEP_ALL, Solver, load_scenario
+    from biofvm_b200 import workloads as W
+
+    scn = W.lod_256(steps=args.steps)
+    N, S = scn.num_voxels, scn.S
+    sv = Solver(local)
+    load_scenario(sv, scn)
+    dt = scn.dt
+    stream = torch.cuda.ExternalStream(sv.stream, device=torch.device("cuda", local))
+
+    # warm-up (also builds the Thomas coefficients and the device lists)
+    sv.step(dt, args.warmup, STEP_ALL)
+    sv.synchronize()
+
+    launches0 = sv.launch_count
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        barrier(world)
+        torch.cuda.synchronize(local)
+        sv.synchronize()
+        ev0.record(stream)
+        sv.step(dt, args.steps, STEP_ALL)
+        ev1.record(stream)
+        ev1.synchronize()
+        sv.synchronize()
+        barrier(world)
+    launches = sv.launch_count - launches0
+    ms = ev0.elapsed_time(ev1)
+    ms = max_over_ranks(ms, world)
+    value = N * S * args.steps * world / (ms / 1e3)
+    ms_step = ms / args.steps
+
+    # per-kernel device times on the solver's stream (CUDA events between sweeps)
+    kx, ky, kz = sv.profile_step(dt, max(3, min(args.steps, 10)), STEP_ALL)
+    per = {"x_sweep_fused": kx, "y_sweep": ky, "z_sweep": kz}
+    dom = max(per, key=per.get)
+    hbm, peak_kind = peaks()
+    achieved = BYTES_PER_VS_SWEEP * N * S / (per[dom] / 1e3) / 1e9
+    traffic = ncu_traffic(dom)
+
+    # end to end through the C ABI with host buffers: every step uploads the
+    # agents' voxels and secretion/uptake constants (as when agents move and
+    # change rates each step) and reads back the densities at the agents.
+    e2e = None
+    if not args.no_e2e:
+        vox, t1, t2 = scn.agent_arrays()
+        out = np.empty((scn.num_agents, S))
+        e_steps = max(1, min(args.steps, 20))
+        sv.synchronize()
+        barrier(world)
+        t0 = time.perf_counter()
+        for _ in range(e_steps):
+            sv.set_agents(vox, t1, t2)
+            sv.step(dt, 1, STEP_ALL)
+            sv.get_agent_densities(out)
+        e_secs = time.perf_counter() - t0
+        e_secs = max_over_ranks(e_secs, world)
+        e2e = {"value": N * S * e_steps * world / e_secs, "unit": UNIT,
+               "h2d_bytes_per_step": int(vox.nbytes + t1.nbytes + t2.nbytes),
+               "d2h_bytes_per_step": int(out.nbytes), "steps": e_steps,
+               "what": "per step: bfvm_set_agents (host voxel+temp1+temp2), bfvm_step, "
+                       "bfvm_get_agent_densities (host [A][S])"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            threads = os.cpu_count() or 1
+            vs, secs, setup, variant, sscn = time_reference(3, 1, threads)
+            cpu = {"value": vs, "unit": UNIT, "cores": threads, "kind": "reference",
+                   "sample": f"{sscn.shape[0]}^3 x {sscn.S}, {sscn.num_agents} agents, 3 steps "
+                             f"(1/8 of the workload's voxels), reference build {variant}"}
+        except Exception as exc:  # reported, not fatal
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                   "sample": f"unavailable: {exc}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)",
+            "config": {"workload": "lod_256: 256^3 voxels x 10 substrates FP64, 100k agents, "
+                                   "bulk sphere r=500um, dt=0.01",
+                       "voxels": N, "substrates": S, "agents": scn.num_agents,
+                       "l2": "inputs (1.34 GB field) larger than L2; no flush",
+                       "parallelism": f"instances x{world}" if world > 1 else "1 GPU"},
+            "hbm_gbs_step": BYTES_PER_VS_STEP * N * S / (ms_step / 1e3) / 1e9,
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / hbm,
+                         "traffic": traffic,
+                         "algorithmic_bytes_per_launch": BYTES_PER_VS_SWEEP * N * S},
+            "kernel_ms": per,
+            "gpu_launches": int(launches),
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    sv.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+    world, rank, local = dist_init(args)
+    try:
+        if args.impl == "reference":
+            run_reference_arm(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,72 @@
+// Host-side numerics that must reproduce the reference bit for bit.  This
+// file is compiled with -ffp-contract=off so that no multiply-add is fused,
+// matching the reference's shipped x86-64 build (-march=core2, no FMA).
+#include "bfvm_host_math.h"
+
+#include <cmath>
+
+namespace bfvm {
+
+int nodes_from_spacing(double start, double end, double d) {
+  // Cartesian_Mesh::resize(..., dx, dy, dz), BioFVM_mesh.cpp:802-805
+  double eps = 1e-16;
+  return (int)std::ceil(eps + (end - start) / d);
+}
+
+void thomas_axis(int n, int S, double dx, double dt, const double* D, const double* decay,
+                 double* c1, double* denom, double* cx) {
+  for (int s = 0; s < S; ++s) {
+    // BioFVM_solvers.cpp:105-126: the constants are built by the same
+    // sequence of elementwise operations.
+    double k1 = D[s];
+    k1 *= dt;
+    k1 /= dx;
+    k1 /= dx;
+    double k1a = k1;
+    k1a *= -1.0;
+    double k2 = decay[s];
+    k2 *= dt;
+    k2 /= 3.0;
+    double k3 = 1.0;
+    k3 += k1;
+    k3 += k1;
+    k3 += k2;
+    double k3a = 1.0;
+    k3a += k1;
+    k3a += k2;
+    c1[s] = k1;
+    // :130-135 boundary rows carry 1 + c1 + c2 (Neumann); a single point 1 + c2
+    for (int i = 0; i < n; ++i) {
+      cx[(size_t)i * S + s] = k1a;
+      denom[(size_t)i * S + s] = k3;
+    }
+    denom[s] = k3a;
+    denom[(size_t)(n - 1) * S + s] = k3a;
+    if (n == 1) {
+      denom[s] = 1.0;
+      denom[s] += k2;
+    }
+    // :137-142 forward elimination of the constant matrix
+    cx[s] /= denom[s];
+    for (int i = 1; i <= n - 1; ++i) {
+      denom[(size_t)i * S + s] += k1 * cx[(size_t)(i - 1) * S + s];
+      cx[(size_t)i * S + s] /= denom[(size_t)i * S + s];
+    }
+  }
+}
+
+void bulk_coefficients(int S, const double* supply, const double* target, const double* uptake,
+                       double* st, double* su) {
+  // BioFVM_microenvironment.cpp:603,605: temp2 = T*S, temp3 = U+S
+  for (int s = 0; s < S; ++s) {
+    double t1 = supply ? supply[s] : 0.0;
+    double t2 = target ? target[s] : 0.0;
+    double t3 = uptake ? uptake[s] : 0.0;
+    t2 *= t1;
+    t3 += t1;
+    st[s] = t2;
+    su[s] = t3;
+  }
+}
+
+}  // namespace bfvm

@@ -1,0 +1,329 @@
+// Device kernels of the B200 transport path.
+//
+// Density field: one array [nz][ny][nx][S] (substrate innermost), the
+// reference's logical [voxel][substrate] order made contiguous.
+//
+// LOD sweep (BioFVM_solvers.cpp:175-273).  Along one axis every (line,
+// substrate) pair is an independent tridiagonal system solved by the Thomas
+// algorithm with precomputed coefficients:
+//   forward   q_0 = p_0/d_0,  q_k = (p_k + c1*q_{k-1})/d_k     (:186-194)
+//   backward  x_{n-1} = q_{n-1},  x_k = q_k - cx_k*x_{k+1}       (:196-200)
+// Both are first-order linear recurrences, so a line is cut into chunks of
+// CH points, one chunk per thread, held in registers:
+//   1. each thread runs the recurrence over its chunk with carry-in 0 and
+//      records the chunk's transfer (end value, product of slopes);
+//   2. the transfers of the chunks of one line are folded through shared
+//      memory to give every chunk its true carry-in;
+//   3. each thread corrects its chunk: value += (running slope product)*carry.
+// Every density element is read once and written once per sweep.
+//
+// A thread block is TW columns x NC chunks (blockDim = (TW, NC)); a
+// "column" is one (line, substrate) pair and consecutive columns are
+// consecutive addresses for the y and z sweeps, so every warp load/store is a
+// contiguous TW*sizeof(T) run.  For the x sweep the S substrates of a row are
+// the contiguous run.
+//
+// The x sweep also carries the rest of the step in its prologue: bulk
+// sources/sinks, then cell sources/sinks (agents in reference order), then
+// the Dirichlet overwrite; its epilogue is the Dirichlet overwrite that the
+// reference does before the y sweep, and the y sweep's epilogue is the one
+// before the z sweep.  These per-voxel updates use the same IEEE operations
+// in the same order as the reference (no FMA contraction), so they are
+// bit-exact; only the sweeps' rounding differs.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace bfvm {
+
+enum : int {
+  kFuseBulk = 1,
+  kFuseCells = 2,
+  kFuseDirPro = 4,   // Dirichlet before the sweep
+  kFuseDirEpi = 8,   // Dirichlet after the sweep (= before the next axis)
+};
+
+// Coefficients of one axis, [n][S] each, in the sweep's precision.
+template <typename T>
+struct AxisCoef {
+  const T* inv_den;  // 1 / thomas_denom
+  const T* fwd;      // c1 / thomas_denom: slope of the forward recurrence
+  const T* bwd;      // -thomas_c: slope of the back substitution
+  const T* c1;       // [S] dt*D/dx^2
+};
+
+// Entries grouped by (line, chunk) segment: off[line*NC + c] .. off[+1].
+// pos = point index along the line; a/b = per-substrate payload [E][S].
+struct SegList {
+  const int* off = nullptr;
+  const int* pos = nullptr;
+  const double* a = nullptr;
+  const double* b = nullptr;
+};
+
+template <typename T>
+struct SweepArgs {
+  T* p;
+  int64_t ncols;         // number of (line, substrate) columns
+  int64_t C;             // columns per outer block
+  int64_t outer_stride;  // elements between outer blocks
+  int64_t line_stride;   // elements between consecutive points of a line
+  int n;                 // points per line
+  int nchunks;           // NC = ceil(n / CH)
+  int S;
+  AxisCoef<T> coef;
+  SegList bulk, cells, dir_pro, dir_epi;
+  double dt;
+  int fuse;
+};
+
+template <typename T, int CH>
+__device__ __forceinline__ T reg_get(const T (&v)[CH], int m) {
+  T r = v[0];
+#pragma unroll
+  for (int q = 1; q < CH; ++q) r = (q == m) ? v[q] : r;
+  return r;
+}
+
+template <typename T, int CH>
+__device__ __forceinline__ void reg_set(T (&v)[CH], int m, T x) {
+#pragma unroll
+  for (int q = 0; q < CH; ++q) v[q] = (q == m) ? x : v[q];
+}
+
+// Bulk update of one voxel-substrate (BioFVM_microenvironment.cpp:603-609):
+// p += dt*(S*T); p /= (U+S)*dt + 1.  st = S*T and su = U+S are stored.
+__device__ __forceinline__ double bulk_update(double x, double st, double su, double dt) {
+  x = __dadd_rn(x, __dmul_rn(dt, st));
+  return __ddiv_rn(x, __dadd_rn(__dmul_rn(su, dt), 1.0));
+}
+
+// One agent's update (BioFVM_basic_agent.cpp:234-235): p += temp1; p /= temp2.
+__device__ __forceinline__ double cell_update(double x, double t1, double t2) {
+  return __ddiv_rn(__dadd_rn(x, t1), t2);
+}
+
+template <typename T, int CH>
+__device__ __forceinline__ void apply_dirichlet_seg(T (&v)[CH], const SegList& L, int64_t seg,
+                                                    int k0, int S, int s) {
+  const int e0 = __ldg(L.off + seg), e1 = __ldg(L.off + seg + 1);
+  for (int e = e0; e < e1; ++e) {
+    const int m = __ldg(L.pos + e) - k0;
+    reg_set<T, CH>(v, m, (T)__ldg(L.a + (int64_t)e * S + s));
+  }
+}
+
+// MODE selects the fused work: kSweepPlain (z), kSweepDirEpi (y: Dirichlet
+// after the sweep), kSweepFull (x: bulk/cells/Dirichlet prologue + Dirichlet
+// epilogue, each switched by SweepArgs::fuse).  Separate instantiations keep
+// the plain sweeps free of the prologue's registers.
+enum : int { kSweepPlain = 0, kSweepDirEpi = 1, kSweepFull = 2 };
+
+template <typename T, int CH, int MODE>
+__global__ void __launch_bounds__(512) lod_sweep_kernel(const SweepArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int TW = blockDim.x;
+  const int NC = blockDim.y;
+  T* sQ = reinterpret_cast<T*>(smem_raw);  // [NC][TW] forward chunk end values
+  T* sP = sQ + NC * TW;                    // forward chunk slope products
+  T* sX = sP + NC * TW;                    // backward chunk start values
+  T* sR = sX + NC * TW;                    // backward chunk slope products
+
+  const int tx = threadIdx.x;
+  const int c = threadIdx.y;
+  const int64_t vcol = (int64_t)blockIdx.x * TW + tx;
+  const bool active = vcol < a.ncols;
+  const int S = a.S;
+  const int k0 = c * CH;
+  // points of this chunk that exist (partial last chunk, empty chunks)
+  const int len = active ? max(0, min(CH, a.n - k0)) : 0;
+
+  T* ptr = a.p;
+  int s = 0;
+  int64_t seg = 0;
+  if (active) {
+    const int64_t outer = vcol / a.C;
+    const int64_t col = vcol - outer * a.C;
+    ptr = a.p + outer * a.outer_stride + col + (int64_t)k0 * a.line_stride;
+    s = (int)(col % S);
+    seg = (vcol / S) * a.nchunks + c;
+  }
+  const int64_t ls = a.line_stride;
+
+  T v[CH];
+#pragma unroll
+  for (int m = 0; m < CH; ++m) v[m] = (m < len) ? ptr[m * ls] : T(0);
+
+  if (MODE == kSweepFull && active) {
+    if (a.fuse & kFuseBulk) {
+      const int e0 = __ldg(a.bulk.off + seg), e1 = __ldg(a.bulk.off + seg + 1);
+      for (int e = e0; e < e1; ++e) {
+        const int m = __ldg(a.bulk.pos + e) - k0;
+        const int64_t q = (int64_t)e * S + s;
+        double x = (double)reg_get<T, CH>(v, m);
+        x = bulk_update(x, __ldg(a.bulk.a + q), __ldg(a.bulk.b + q), a.dt);
+        reg_set<T, CH>(v, m, (T)x);
+      }
+    }
+    if (a.fuse & kFuseCells) {
+      // Agents of this chunk sorted by (voxel, list order): applying them in
+      // sequence keeps the reference's order for agents sharing a voxel.
+      // Consecutive agents of one voxel accumulate in FP64 before rounding.
+      const int e0 = __ldg(a.cells.off + seg), e1 = __ldg(a.cells.off + seg + 1);
+      int e = e0;
+      while (e < e1) {
+        const int pos = __ldg(a.cells.pos + e);
+        const int m = pos - k0;
+        double x = (double)reg_get<T, CH>(v, m);
+        do {
+          const int64_t q = (int64_t)e * S + s;
+          x = cell_update(x, __ldg(a.cells.a + q), __ldg(a.cells.b + q));
+          ++e;
+        } while (e < e1 && __ldg(a.cells.pos + e) == pos);
+        reg_set<T, CH>(v, m, (T)x);
+      }
+    }
+    if (a.fuse & kFuseDirPro) apply_dirichlet_seg<T, CH>(v, a.dir_pro, seg, k0, S, s);
+  }
+
+  // Coefficient rows of this chunk: [k][S] tables, stride S along the line.
+  const T* c_inv = a.coef.inv_den + (int64_t)k0 * S + s;
+  const T* c_fwd = a.coef.fwd + (int64_t)k0 * S + s;
+  const T* c_bwd = a.coef.bwd + (int64_t)k0 * S + s;
+
+  // ---- forward elimination, chunk-local with carry-in 0 ----
+  const T c1 = active ? __ldg(a.coef.c1 + s) : T(0);
+  T q = T(0), P = T(1);
+#pragma unroll
+  for (int m = 0; m < CH; ++m) {
+    if (m < len) {
+      q = (v[m] + c1 * q) * __ldg(c_inv + m * S);
+      P = P * __ldg(c_fwd + m * S);
+      v[m] = q;
+    }
+  }
+  sQ[c * TW + tx] = q;
+  sP[c * TW + tx] = P;
+  __syncthreads();
+  if (c > 0 && len > 0) {
+    T carry = T(0);
+    for (int cc = 0; cc < c; ++cc) carry = sP[cc * TW + tx] * carry + sQ[cc * TW + tx];
+    T Pm = T(1);
+#pragma unroll
+    for (int m = 0; m < CH; ++m) {
+      if (m < len) {
+        Pm = Pm * __ldg(c_fwd + m * S);
+        v[m] = v[m] + Pm * carry;
+      }
+    }
+  }
+
+  // ---- back substitution, chunk-local with carry-in 0 ----
+  T x = T(0), R = T(1);
+#pragma unroll
+  for (int m = CH - 1; m >= 0; --m) {
+    if (m < len) {
+      const T b = __ldg(c_bwd + m * S);
+      x = v[m] + b * x;
+      R = R * b;
+      v[m] = x;
+    }
+  }
+  sX[c * TW + tx] = x;
+  sR[c * TW + tx] = R;
+  __syncthreads();
+  if (c < NC - 1 && len > 0) {
+    T carry = T(0);
+    for (int cc = NC - 1; cc > c; --cc) carry = sR[cc * TW + tx] * carry + sX[cc * TW + tx];
+    T Rm = T(1);
+#pragma unroll
+    for (int m = CH - 1; m >= 0; --m) {
+      if (m < len) {
+        Rm = Rm * __ldg(c_bwd + m * S);
+        v[m] = v[m] + Rm * carry;
+      }
+    }
+  }
+
+  if (MODE != kSweepPlain && active && (a.fuse & kFuseDirEpi))
+    apply_dirichlet_seg<T, CH>(v, a.dir_epi, seg, k0, S, s);
+
+#pragma unroll
+  for (int m = 0; m < CH; ++m)
+    if (m < len) ptr[m * ls] = v[m];
+}
+
+// ---------------------------------------------------------------------------
+// Stand-alone per-voxel kernels (the individual simulate_* / apply_* calls).
+
+// simulate_bulk_sources_and_sinks over the stored (non-identity) voxels.
+template <typename T>
+__global__ void bulk_kernel(T* __restrict__ p, int S, int64_t E, const int64_t* __restrict__ voxel,
+                            const double* __restrict__ st, const double* __restrict__ su,
+                            double dt) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= E * S) return;
+  const int64_t e = t / S;
+  const int s = (int)(t - e * S);
+  const int64_t q = voxel[e] * S + s;
+  p[q] = (T)bulk_update((double)p[q], st[t], su[t], dt);
+}
+
+// simulate_cell_sources_and_sinks: one thread per (voxel group, substrate);
+// the agents of a group are applied in list order.
+template <typename T>
+__global__ void cells_kernel(T* __restrict__ p, int S, int64_t G, const int64_t* __restrict__ gvoxel,
+                             const int* __restrict__ gstart, const double* __restrict__ t1,
+                             const double* __restrict__ t2) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= G * S) return;
+  const int64_t g = t / S;
+  const int s = (int)(t - g * S);
+  const int64_t q = gvoxel[g] * S + s;
+  double x = (double)p[q];
+  for (int e = gstart[g]; e < gstart[g + 1]; ++e)
+    x = cell_update(x, t1[(int64_t)e * S + s], t2[(int64_t)e * S + s]);
+  p[q] = (T)x;
+}
+
+// apply_dirichlet_conditions over the de-duplicated node list.
+template <typename T>
+__global__ void dirichlet_kernel(T* __restrict__ p, int S, int64_t E, const int64_t* __restrict__ voxel,
+                                 const double* __restrict__ val) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= E * S) return;
+  const int64_t e = t / S;
+  const int s = (int)(t - e * S);
+  p[voxel[e] * S + s] = (T)val[t];
+}
+
+// out[e][s] = p[voxel[e]][s]
+template <typename T>
+__global__ void gather_kernel(const T* __restrict__ p, int S, int64_t E, const int64_t* __restrict__ voxel,
+                              double* __restrict__ out) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= E * S) return;
+  const int64_t e = t / S;
+  const int s = (int)(t - e * S);
+  out[t] = (double)p[voxel[e] * S + s];
+}
+
+// p[voxel[e]][s] = in[e][s]
+template <typename T>
+__global__ void scatter_kernel(T* __restrict__ p, int S, int64_t E, const int64_t* __restrict__ voxel,
+                               const double* __restrict__ in) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= E * S) return;
+  const int64_t e = t / S;
+  const int s = (int)(t - e * S);
+  p[voxel[e] * S + s] = (T)in[t];
+}
+
+template <typename Dst, typename Src>
+__global__ void convert_kernel(Dst* __restrict__ dst, const Src* __restrict__ src, int64_t count) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < count) dst[t] = (Dst)src[t];
+}
+
+}  // namespace bfvm

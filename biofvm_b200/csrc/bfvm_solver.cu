@@ -1,0 +1,1156 @@
+// Host side of libbfvm.so: the C ABI of include/bfvm.h, the solver state
+// (one BioFVM Microenvironment resident on one GPU) and the kernel launches.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <stdexcept>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "bfvm.h"
+#include "bfvm_host_math.h"
+#include "bfvm_kernels.cuh"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define BFVM_CUDA(call)                                                                   \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess)                                                                \
+      throw Error(e_ == cudaErrorMemoryAllocation ? BFVM_ERR_NOMEM : BFVM_ERR_CUDA,       \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                    \
+  } while (0)
+
+void require(bool ok, const std::string& msg, int code = BFVM_ERR_ARG) {
+  if (!ok) throw Error(code, msg);
+}
+
+// A growable device allocation.
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  void ensure(size_t nbytes) {
+    if (nbytes <= bytes && ptr) return;
+    release();
+    if (nbytes == 0) return;
+    BFVM_CUDA(cudaMalloc(&ptr, nbytes));
+    bytes = nbytes;
+  }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+  }
+  template <typename T>
+  T* as() const {
+    return static_cast<T*>(ptr);
+  }
+};
+
+template <typename T>
+void upload(DevBuf& b, const std::vector<T>& v, cudaStream_t st) {
+  b.ensure(std::max<size_t>(v.size() * sizeof(T), 16));
+  if (!v.empty())
+    BFVM_CUDA(cudaMemcpyAsync(b.ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+}
+
+// Device copy of a segment list (see SegList in bfvm_kernels.cuh).
+struct DevSegList {
+  DevBuf off, pos, a, b;
+  bool present = false;
+  bfvm::SegList view() const {
+    bfvm::SegList L;
+    L.off = off.as<int>();
+    L.pos = pos.as<int>();
+    L.a = a.as<double>();
+    L.b = b.as<double>();
+    return L;
+  }
+  void release() {
+    off.release();
+    pos.release();
+    a.release();
+    b.release();
+    present = false;
+  }
+};
+
+// Groups entries (already in non-decreasing (line, pos) order) by
+// (line, chunk) segment.
+std::vector<int> segment_offsets(int64_t nlines, int nchunks, int ch,
+                                 const std::vector<int64_t>& line, const std::vector<int>& pos) {
+  std::vector<int> off((size_t)(nlines * nchunks + 1), 0);
+  for (size_t e = 0; e < line.size(); ++e) off[(size_t)(line[e] * nchunks + pos[e] / ch) + 1]++;
+  for (size_t i = 1; i < off.size(); ++i) off[i] += off[i - 1];
+  return off;
+}
+
+struct Axis {
+  int ch = 16;  // points per thread
+  int tw = 32;  // columns per block
+};
+
+}  // namespace
+
+struct bfvm_solver {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int64_t launches = 0;
+
+  // mesh (Cartesian_Mesh, BioFVM_mesh.h:146-188)
+  int nx = 1, ny = 1, nz = 1;
+  double dx = 1, dy = 1, dz = 1, dV = 1;
+  double bbox[6] = {-0.5, -0.5, -0.5, 0.5, 0.5, 0.5};
+  bool uniform = true;
+
+  // densities
+  int S = 1;
+  std::vector<double> D{0.0}, decay{0.0};
+  int precision = BFVM_FP64;
+  DevBuf p;
+
+  // Thomas coefficients (computed once, BioFVM_solvers.cpp:87,172)
+  bool setup_done = false;
+  DevBuf coef[3];  // per axis: inv_den, fwd, bwd [n*S] then c1 [S], in the sweep precision
+  Axis axis[3];
+
+  // bulk sources/sinks: non-identity voxels, ascending
+  std::vector<int64_t> bulk_vox;
+  std::vector<double> bulk_st, bulk_su;
+  bool bulk_dirty = true;
+  DevBuf d_bulk_vox, d_bulk_st, d_bulk_su;
+  DevSegList seg_bulk;
+
+  // Dirichlet nodes in insertion order (BioFVM_microenvironment.h:102-103)
+  std::vector<int64_t> dir_vox;
+  std::vector<double> dir_val;
+  bool dir_dirty = true;
+  int64_t dir_unique = 0;
+  DevBuf d_dir_vox, d_dir_val;
+  DevSegList seg_dir_x, seg_dir_y;
+
+  // agents in list order
+  std::vector<int64_t> ag_vox;
+  std::vector<double> ag_t1, ag_t2;
+  bool ag_dirty = true;
+  int64_t n_groups = 0;
+  DevBuf d_ag_vox_orig, d_group_vox, d_group_start, d_gather;
+  DevSegList seg_cells;
+
+  int64_t N() const { return (int64_t)nx * ny * nz; }
+  int64_t NS() const { return N() * S; }
+  size_t elem() const { return precision == BFVM_FP64 ? sizeof(double) : sizeof(float); }
+};
+
+namespace {
+
+int64_t blocks_for(int64_t work, int threads) { return (work + threads - 1) / threads; }
+
+void check_launch(bfvm_solver* m) {
+  m->launches++;
+  BFVM_CUDA(cudaGetLastError());
+}
+
+// Chunk length CH (points per thread) and block width TW (columns per block)
+// per axis; a block is TW x NC threads with NC = ceil(n/CH) <= 512/TW.
+void choose_axes(bfvm_solver* m) {
+  const int ns[3] = {m->nx, m->ny, m->nz};
+  for (int a = 0; a < 3; ++a) {
+    const int n = ns[a];
+    int ch = (n <= 64) ? 8 : 16;
+    while ((n + ch - 1) / ch > 16 && ch < 32) ch *= 2;
+    int tw = 32;
+    if ((n + ch - 1) / ch > 16) tw = 16;
+    require((n + ch - 1) / ch <= 512 / tw,
+            "axis with " + std::to_string(n) + " points exceeds the 1024-point line limit");
+    m->axis[a].ch = ch;
+    m->axis[a].tw = tw;
+  }
+}
+
+void clear_state_after_resize(bfvm_solver* m) {
+  m->p.ensure(std::max<size_t>(m->NS() * m->elem(), 16));
+  BFVM_CUDA(cudaMemsetAsync(m->p.ptr, 0, m->NS() * m->elem(), m->stream));
+  m->setup_done = false;
+  m->bulk_vox.clear();
+  m->bulk_st.clear();
+  m->bulk_su.clear();
+  m->bulk_dirty = true;
+  m->dir_vox.clear();
+  m->dir_val.clear();
+  m->dir_dirty = true;
+  m->ag_vox.clear();
+  m->ag_t1.clear();
+  m->ag_t2.clear();
+  m->ag_dirty = true;
+  choose_axes(m);
+}
+
+// ---- Thomas coefficients ---------------------------------------------------
+
+void thomas_setup(bfvm_solver* m, double dt) {
+  const int ns[3] = {m->nx, m->ny, m->nz};
+  for (int a = 0; a < 3; ++a) {
+    const int n = ns[a], S = m->S;
+    std::vector<double> c1(S), den((size_t)n * S), cx((size_t)n * S);
+    // The reference uses mesh.dx for every axis (BioFVM_solvers.cpp:112-113).
+    bfvm::thomas_axis(n, S, m->dx, dt, m->D.data(), m->decay.data(), c1.data(), den.data(),
+                      cx.data());
+    std::vector<double> tab((size_t)3 * n * S + S);
+    for (size_t i = 0; i < (size_t)n * S; ++i) {
+      const int s = (int)(i % S);
+      tab[i] = 1.0 / den[i];
+      tab[(size_t)n * S + i] = c1[s] / den[i];
+      tab[(size_t)2 * n * S + i] = -cx[i];
+    }
+    for (int s = 0; s < S; ++s) tab[(size_t)3 * n * S + s] = c1[s];
+    if (m->precision == BFVM_FP64) {
+      upload(m->coef[a], tab, m->stream);
+    } else {
+      std::vector<float> tf(tab.begin(), tab.end());
+      upload(m->coef[a], tf, m->stream);
+    }
+  }
+  m->setup_done = true;
+}
+
+template <typename T>
+bfvm::AxisCoef<T> coef_view(const bfvm_solver* m, int a) {
+  const int ns[3] = {m->nx, m->ny, m->nz};
+  const size_t nS = (size_t)ns[a] * m->S;
+  const T* base = m->coef[a].as<T>();
+  bfvm::AxisCoef<T> c;
+  c.inv_den = base;
+  c.fwd = base + nS;
+  c.bwd = base + 2 * nS;
+  c.c1 = base + 3 * nS;
+  return c;
+}
+
+// ---- host lists -> device ---------------------------------------------------
+
+void build_bulk(bfvm_solver* m) {
+  if (!m->bulk_dirty) return;
+  cudaStream_t st = m->stream;
+  const int S = m->S;
+  const int64_t E = (int64_t)m->bulk_vox.size();
+  if (E == 0) {
+    m->seg_bulk.present = false;
+    m->bulk_dirty = false;
+    return;
+  }
+  upload(m->d_bulk_vox, m->bulk_vox, st);
+  upload(m->d_bulk_st, m->bulk_st, st);
+  upload(m->d_bulk_su, m->bulk_su, st);
+  const int ch = m->axis[0].ch, nc = (m->nx + ch - 1) / ch;
+  std::vector<int64_t> line(E);
+  std::vector<int> pos(E);
+  for (int64_t e = 0; e < E; ++e) {
+    line[e] = m->bulk_vox[e] / m->nx;
+    pos[e] = (int)(m->bulk_vox[e] % m->nx);
+  }
+  std::vector<int> off = segment_offsets((int64_t)m->ny * m->nz, nc, ch, line, pos);
+  upload(m->seg_bulk.off, off, st);
+  upload(m->seg_bulk.pos, pos, st);
+  upload(m->seg_bulk.a, m->bulk_st, st);
+  upload(m->seg_bulk.b, m->bulk_su, st);
+  m->seg_bulk.present = true;
+  m->bulk_dirty = false;
+  (void)S;
+}
+
+void build_dirichlet(bfvm_solver* m) {
+  if (!m->dir_dirty) return;
+  cudaStream_t st = m->stream;
+  const int S = m->S;
+  // Nodes are applied in list order, so for a repeated voxel the last one
+  // wins: keep the last occurrence only.
+  std::unordered_map<int64_t, size_t> last;
+  for (size_t d = 0; d < m->dir_vox.size(); ++d) last[m->dir_vox[d]] = d;
+  std::vector<int64_t> vox;
+  vox.reserve(last.size());
+  for (auto& kv : last) vox.push_back(kv.first);
+  std::sort(vox.begin(), vox.end());
+  const int64_t E = (int64_t)vox.size();
+  m->dir_unique = E;
+  if (E == 0) {
+    m->seg_dir_x.present = m->seg_dir_y.present = false;
+    m->dir_dirty = false;
+    return;
+  }
+  std::vector<double> val((size_t)E * S);
+  for (int64_t e = 0; e < E; ++e)
+    std::copy_n(&m->dir_val[last[vox[e]] * S], S, &val[(size_t)e * S]);
+  upload(m->d_dir_vox, vox, st);
+  upload(m->d_dir_val, val, st);
+
+  // x sweep: lines are rows (k, j), points i
+  {
+    const int ch = m->axis[0].ch, nc = (m->nx + ch - 1) / ch;
+    std::vector<int64_t> line(E);
+    std::vector<int> pos(E);
+    for (int64_t e = 0; e < E; ++e) {
+      line[e] = vox[e] / m->nx;
+      pos[e] = (int)(vox[e] % m->nx);
+    }
+    upload(m->seg_dir_x.off, segment_offsets((int64_t)m->ny * m->nz, nc, ch, line, pos), st);
+    upload(m->seg_dir_x.pos, pos, st);
+    upload(m->seg_dir_x.a, val, st);
+    m->seg_dir_x.present = true;
+  }
+  // y sweep: lines are (k, i), points j
+  {
+    const int ch = m->axis[1].ch, nc = (m->ny + ch - 1) / ch;
+    std::vector<int64_t> key(E);
+    for (int64_t e = 0; e < E; ++e) {
+      const int64_t v = vox[e];
+      const int64_t i = v % m->nx, j = (v / m->nx) % m->ny, k = v / ((int64_t)m->nx * m->ny);
+      key[e] = (k * m->nx + i) * m->ny + j;
+    }
+    std::vector<int64_t> order(E);
+    std::iota(order.begin(), order.end(), 0);
+    std::sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return key[a] < key[b]; });
+    std::vector<int64_t> line(E);
+    std::vector<int> pos(E);
+    std::vector<double> vy((size_t)E * S);
+    for (int64_t r = 0; r < E; ++r) {
+      const int64_t e = order[r];
+      line[r] = key[e] / m->ny;
+      pos[r] = (int)(key[e] % m->ny);
+      std::copy_n(&val[(size_t)e * S], S, &vy[(size_t)r * S]);
+    }
+    upload(m->seg_dir_y.off, segment_offsets((int64_t)m->nz * m->nx, nc, ch, line, pos), st);
+    upload(m->seg_dir_y.pos, pos, st);
+    upload(m->seg_dir_y.a, vy, st);
+    m->seg_dir_y.present = true;
+  }
+  m->dir_dirty = false;
+}
+
+void build_agents(bfvm_solver* m) {
+  if (!m->ag_dirty) return;
+  cudaStream_t st = m->stream;
+  const int S = m->S;
+  const int64_t A = (int64_t)m->ag_vox.size();
+  if (A == 0) {
+    m->seg_cells.present = false;
+    m->n_groups = 0;
+    m->ag_dirty = false;
+    return;
+  }
+  // Stable order by voxel keeps list order among agents of one voxel.
+  std::vector<int64_t> order(A);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int64_t a, int64_t b) { return m->ag_vox[a] < m->ag_vox[b]; });
+  std::vector<int64_t> line(A);
+  std::vector<int> pos(A);
+  std::vector<double> t1((size_t)A * S), t2((size_t)A * S);
+  std::vector<int64_t> gvox;
+  std::vector<int> gstart;
+  for (int64_t r = 0; r < A; ++r) {
+    const int64_t e = order[r];
+    const int64_t v = m->ag_vox[e];
+    line[r] = v / m->nx;
+    pos[r] = (int)(v % m->nx);
+    std::copy_n(&m->ag_t1[(size_t)e * S], S, &t1[(size_t)r * S]);
+    std::copy_n(&m->ag_t2[(size_t)e * S], S, &t2[(size_t)r * S]);
+    if (r == 0 || v != gvox.back()) {
+      gvox.push_back(v);
+      gstart.push_back((int)r);
+    }
+  }
+  gstart.push_back((int)A);
+  m->n_groups = (int64_t)gvox.size();
+  const int ch = m->axis[0].ch, nc = (m->nx + ch - 1) / ch;
+  upload(m->seg_cells.off, segment_offsets((int64_t)m->ny * m->nz, nc, ch, line, pos), st);
+  upload(m->seg_cells.pos, pos, st);
+  upload(m->seg_cells.a, t1, st);
+  upload(m->seg_cells.b, t2, st);
+  m->seg_cells.present = true;
+  upload(m->d_group_vox, gvox, st);
+  upload(m->d_group_start, gstart, st);
+  upload(m->d_ag_vox_orig, m->ag_vox, st);
+  m->ag_dirty = false;
+}
+
+void build_all(bfvm_solver* m) {
+  build_bulk(m);
+  build_dirichlet(m);
+  build_agents(m);
+}
+
+// ---- launches ---------------------------------------------------------------
+
+template <typename T, int CH>
+void launch_sweep_ch(const bfvm::SweepArgs<T>& a, int mode, dim3 grid, dim3 block, size_t smem,
+                     cudaStream_t st) {
+  if (mode == bfvm::kSweepFull)
+    bfvm::lod_sweep_kernel<T, CH, bfvm::kSweepFull><<<grid, block, smem, st>>>(a);
+  else if (mode == bfvm::kSweepDirEpi)
+    bfvm::lod_sweep_kernel<T, CH, bfvm::kSweepDirEpi><<<grid, block, smem, st>>>(a);
+  else
+    bfvm::lod_sweep_kernel<T, CH, bfvm::kSweepPlain><<<grid, block, smem, st>>>(a);
+}
+
+template <typename T>
+void launch_sweep(bfvm_solver* m, int ax, int fuse, double dt) {
+  const int S = m->S;
+  const int64_t nx = m->nx, ny = m->ny, nz = m->nz;
+  bfvm::SweepArgs<T> a{};
+  a.p = m->p.as<T>();
+  a.S = S;
+  a.dt = dt;
+  a.coef = coef_view<T>(m, ax);
+  if (ax == 0) {
+    a.n = (int)nx;
+    a.C = S;
+    a.outer_stride = nx * S;
+    a.line_stride = S;
+    a.ncols = ny * nz * S;
+  } else if (ax == 1) {
+    a.n = (int)ny;
+    a.C = nx * S;
+    a.outer_stride = nx * ny * S;
+    a.line_stride = nx * S;
+    a.ncols = nz * nx * S;
+  } else {
+    a.n = (int)nz;
+    a.C = nx * ny * S;
+    a.outer_stride = 0;
+    a.line_stride = nx * ny * S;
+    a.ncols = nx * ny * S;
+  }
+  const Axis& A = m->axis[ax];
+  a.nchunks = (a.n + A.ch - 1) / A.ch;
+  if ((fuse & bfvm::kFuseBulk) && !m->seg_bulk.present) fuse &= ~bfvm::kFuseBulk;
+  if ((fuse & bfvm::kFuseCells) && !m->seg_cells.present) fuse &= ~bfvm::kFuseCells;
+  const DevSegList& dseg = (ax == 0) ? m->seg_dir_x : m->seg_dir_y;
+  if (!dseg.present || ax == 2) fuse &= ~(bfvm::kFuseDirPro | bfvm::kFuseDirEpi);
+  a.fuse = fuse;
+  a.bulk = m->seg_bulk.view();
+  a.cells = m->seg_cells.view();
+  a.dir_pro = dseg.view();
+  a.dir_epi = dseg.view();
+  dim3 block(A.tw, a.nchunks);
+  dim3 grid((unsigned)blocks_for(a.ncols, A.tw));
+  const size_t smem = 4 * sizeof(T) * (size_t)A.tw * a.nchunks;
+  int mode = bfvm::kSweepPlain;
+  if (fuse & (bfvm::kFuseBulk | bfvm::kFuseCells | bfvm::kFuseDirPro))
+    mode = bfvm::kSweepFull;
+  else if (fuse & bfvm::kFuseDirEpi)
+    mode = bfvm::kSweepDirEpi;
+  switch (A.ch) {
+    case 8: launch_sweep_ch<T, 8>(a, mode, grid, block, smem, m->stream); break;
+    case 16: launch_sweep_ch<T, 16>(a, mode, grid, block, smem, m->stream); break;
+    case 32: launch_sweep_ch<T, 32>(a, mode, grid, block, smem, m->stream); break;
+    default: throw Error(BFVM_ERR_STATE, "unsupported chunk length");
+  }
+  check_launch(m);
+}
+
+void sweep(bfvm_solver* m, int ax, int fuse, double dt) {
+  if (m->precision == BFVM_FP64)
+    launch_sweep<double>(m, ax, fuse, dt);
+  else
+    launch_sweep<float>(m, ax, fuse, dt);
+}
+
+void check_lod_mesh(bfvm_solver* m) {
+  // BioFVM_solvers.cpp:79-83
+  require(m->uniform,
+          "Error: This algorithm is written for uniform Cartesian meshes. Try: other solvers!",
+          BFVM_ERR_MESH);
+}
+
+void diffusion(bfvm_solver* m, double dt, int fuse_x) {
+  check_lod_mesh(m);
+  if (!m->setup_done) thomas_setup(m, dt);
+  build_all(m);
+  sweep(m, 0, fuse_x | bfvm::kFuseDirPro | bfvm::kFuseDirEpi, dt);
+  sweep(m, 1, bfvm::kFuseDirEpi, dt);
+  sweep(m, 2, 0, dt);
+}
+
+template <typename T>
+void bulk_standalone(bfvm_solver* m, double dt) {
+  const int64_t E = (int64_t)m->bulk_vox.size();
+  if (E == 0) return;
+  const int64_t work = E * m->S;
+  bfvm::bulk_kernel<T><<<(unsigned)blocks_for(work, 256), 256, 0, m->stream>>>(
+      m->p.as<T>(), m->S, E, m->d_bulk_vox.as<int64_t>(), m->d_bulk_st.as<double>(),
+      m->d_bulk_su.as<double>(), dt);
+  check_launch(m);
+}
+
+template <typename T>
+void cells_standalone(bfvm_solver* m) {
+  if (m->n_groups == 0) return;
+  const int64_t work = m->n_groups * m->S;
+  bfvm::cells_kernel<T><<<(unsigned)blocks_for(work, 256), 256, 0, m->stream>>>(
+      m->p.as<T>(), m->S, m->n_groups, m->d_group_vox.as<int64_t>(), m->d_group_start.as<int>(),
+      m->seg_cells.a.as<double>(), m->seg_cells.b.as<double>());
+  check_launch(m);
+}
+
+template <typename T>
+void dirichlet_standalone(bfvm_solver* m) {
+  if (m->dir_unique == 0) return;
+  const int64_t work = m->dir_unique * m->S;
+  bfvm::dirichlet_kernel<T><<<(unsigned)blocks_for(work, 256), 256, 0, m->stream>>>(
+      m->p.as<T>(), m->S, m->dir_unique, m->d_dir_vox.as<int64_t>(), m->d_dir_val.as<double>());
+  check_launch(m);
+}
+
+template <typename T>
+void gather(bfvm_solver* m, int64_t count, const int64_t* d_vox, double* d_out) {
+  if (count == 0) return;
+  const int64_t work = count * m->S;
+  bfvm::gather_kernel<T><<<(unsigned)blocks_for(work, 256), 256, 0, m->stream>>>(
+      m->p.as<T>(), m->S, count, d_vox, d_out);
+  check_launch(m);
+}
+
+void bulk_any(bfvm_solver* m, double dt) {
+  if (m->precision == BFVM_FP64)
+    bulk_standalone<double>(m, dt);
+  else
+    bulk_standalone<float>(m, dt);
+}
+
+void cells_any(bfvm_solver* m) {
+  if (m->precision == BFVM_FP64)
+    cells_standalone<double>(m);
+  else
+    cells_standalone<float>(m);
+}
+
+void validate_voxels(const bfvm_solver* m, int64_t count, const int64_t* vox) {
+  const int64_t N = m->N();
+  for (int64_t e = 0; e < count; ++e)
+    require(vox[e] >= 0 && vox[e] < N,
+            "voxel index " + std::to_string(vox[e]) + " outside [0, " + std::to_string(N) + ")");
+}
+
+void resize_common(bfvm_solver* m, int nx, int ny, int nz) {
+  require(nx > 0 && ny > 0 && nz > 0, "node counts must be positive");
+  require((int64_t)nx * ny * nz * std::max(m->S, 1) < ((int64_t)1 << 40), "mesh too large");
+  m->nx = nx;
+  m->ny = ny;
+  m->nz = nz;
+  clear_state_after_resize(m);
+}
+
+template <typename F>
+int guarded(F&& f) {
+  try {
+    f();
+    return BFVM_OK;
+  } catch (const Error& e) {
+    g_last_error = e.what();
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    g_last_error = "host allocation failed";
+    return BFVM_ERR_NOMEM;
+  } catch (const std::exception& e) {
+    g_last_error = e.what();
+    return BFVM_ERR_STATE;
+  }
+}
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) BFVM_CUDA(cudaSetDevice(dev));
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+#define SOLVER_CALL(m, ...)                                     \
+  guarded([&] {                                                 \
+    require((m) != nullptr, "null solver handle");              \
+    DeviceGuard dg_((m)->device);                               \
+    __VA_ARGS__;                                                \
+  })
+
+}  // namespace
+
+extern "C" {
+
+const char* bfvm_last_error(void) { return g_last_error.c_str(); }
+int bfvm_version(void) { return 100; }
+
+int bfvm_create(bfvm_solver** out, int device) {
+  return guarded([&] {
+    require(out != nullptr, "null output pointer");
+    int ndev = 0;
+    BFVM_CUDA(cudaGetDeviceCount(&ndev));
+    require(device >= 0 && device < ndev, "no CUDA device " + std::to_string(device));
+    DeviceGuard dg(device);
+    bfvm_solver* m = new bfvm_solver;
+    m->device = device;
+    cudaError_t e = cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+      delete m;
+      throw Error(BFVM_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
+    }
+    // Microenvironment(): mesh.resize(1,1,1) (BioFVM_microenvironment.cpp:101)
+    // = resize(-0.5, 0.5, ..., 1, 1, 1) (BioFVM_mesh.cpp:924-925), dx = 1.
+    resize_common(m, 1, 1, 1);
+    *out = m;
+  });
+}
+
+int bfvm_destroy(bfvm_solver* m) {
+  return guarded([&] {
+    if (!m) return;
+    DeviceGuard dg(m->device);
+    cudaStreamSynchronize(m->stream);
+    m->p.release();
+    for (auto& c : m->coef) c.release();
+    m->d_bulk_vox.release();
+    m->d_bulk_st.release();
+    m->d_bulk_su.release();
+    m->seg_bulk.release();
+    m->d_dir_vox.release();
+    m->d_dir_val.release();
+    m->seg_dir_x.release();
+    m->seg_dir_y.release();
+    m->d_ag_vox_orig.release();
+    m->d_group_vox.release();
+    m->d_group_start.release();
+    m->d_gather.release();
+    m->seg_cells.release();
+    cudaStreamDestroy(m->stream);
+    delete m;
+  });
+}
+
+int bfvm_resize_space(bfvm_solver* m, double x0, double x1, double y0, double y1, double z0,
+                      double z1, double dx, double dy, double dz) {
+  return SOLVER_CALL(m, {
+    require(dx > 0 && dy > 0 && dz > 0, "voxel spacing must be positive");
+    require(x1 > x0 && y1 > y0 && z1 > z0, "empty domain");
+    // BioFVM_mesh.cpp:796-836
+    const int nx = bfvm::nodes_from_spacing(x0, x1, dx);
+    const int ny = bfvm::nodes_from_spacing(y0, y1, dy);
+    const int nz = bfvm::nodes_from_spacing(z0, z1, dz);
+    const double tol = 1e-16;
+    m->uniform = !(std::fabs(dx - dy) > tol || std::fabs(dy - dz) > tol ||
+                   std::fabs(dx - dz) > tol);
+    m->dx = dx;
+    m->dy = dy;
+    m->dz = dz;
+    m->dV = dx * dy * dz;
+    const double bb[6] = {x0, y0, z0, x1, y1, z1};
+    std::copy(bb, bb + 6, m->bbox);
+    resize_common(m, nx, ny, nz);
+  });
+}
+
+int bfvm_resize_space_nodes(bfvm_solver* m, double x0, double x1, double y0, double y1,
+                            double z0, double z1, int nx, int ny, int nz) {
+  return SOLVER_CALL(m, {
+    require(nx > 0 && ny > 0 && nz > 0, "node counts must be positive");
+    // BioFVM_mesh.cpp:669-704
+    double dx = (x1 - x0) / (double)nx;
+    if (nx < 2) dx = 1;
+    double dy = (y1 - y0) / (double)ny;
+    if (ny < 2) dy = 1;
+    double dz = (z1 - z0) / (double)nz;
+    if (nz < 2) dz = 1;
+    const double tol = 1e-16;
+    bool uni = true;
+    if (std::fabs(dx - dy) > tol && nx > 1 && ny > 1) uni = false;
+    if (std::fabs(dy - dz) > tol && ny > 1 && nz > 1) uni = false;
+    if (std::fabs(dx - dz) > tol && nx > 1 && nz > 1) uni = false;
+    m->uniform = uni;
+    m->dx = dx;
+    m->dy = dy;
+    m->dz = dz;
+    m->dV = dx * dy * dz;
+    const double bb[6] = {x0, y0, z0, x1, y1, z1};
+    std::copy(bb, bb + 6, m->bbox);
+    resize_common(m, nx, ny, nz);
+  });
+}
+
+int bfvm_get_mesh(bfvm_solver* m, int* nxyz, double* geom, int* flags) {
+  return SOLVER_CALL(m, {
+    if (nxyz) {
+      nxyz[0] = m->nx;
+      nxyz[1] = m->ny;
+      nxyz[2] = m->nz;
+    }
+    if (geom) {
+      geom[0] = m->dx;
+      geom[1] = m->dy;
+      geom[2] = m->dz;
+      geom[3] = m->dV;
+      std::copy(m->bbox, m->bbox + 6, geom + 4);
+    }
+    if (flags) {
+      flags[0] = m->uniform ? 1 : 0;
+      flags[1] = m->S;
+    }
+  });
+}
+
+int bfvm_resize_densities(bfvm_solver* m, int num_densities) {
+  return SOLVER_CALL(m, {
+    require(num_densities > 0, "need at least one density");
+    m->S = num_densities;
+    m->D.assign(num_densities, 0.0);
+    m->decay.assign(num_densities, 0.0);
+    m->p.ensure(std::max<size_t>(m->NS() * m->elem(), 16));
+    BFVM_CUDA(cudaMemsetAsync(m->p.ptr, 0, m->NS() * m->elem(), m->stream));
+    // resize_densities keeps the Dirichlet list but its value vectors no
+    // longer match S; the list is cleared so no stale node is applied.
+    m->dir_vox.clear();
+    m->dir_val.clear();
+    m->dir_dirty = true;
+    m->bulk_vox.clear();
+    m->bulk_st.clear();
+    m->bulk_su.clear();
+    m->bulk_dirty = true;
+    m->ag_vox.clear();
+    m->ag_t1.clear();
+    m->ag_t2.clear();
+    m->ag_dirty = true;
+  });
+}
+
+int bfvm_add_density(bfvm_solver* m, double diffusion_coefficient, double decay_rate) {
+  return SOLVER_CALL(m, {
+    // BioFVM_microenvironment.cpp:404-441: every voxel vector gets one more
+    // zero entry; existing densities keep their values.
+    const int S0 = m->S, S1 = S0 + 1;
+    const int64_t N = m->N();
+    DevBuf np;
+    np.ensure(std::max<size_t>((size_t)N * S1 * m->elem(), 16));
+    BFVM_CUDA(cudaMemsetAsync(np.ptr, 0, (size_t)N * S1 * m->elem(), m->stream));
+    BFVM_CUDA(cudaMemcpy2DAsync(np.ptr, S1 * m->elem(), m->p.ptr, S0 * m->elem(),
+                                S0 * m->elem(), N, cudaMemcpyDeviceToDevice, m->stream));
+    BFVM_CUDA(cudaStreamSynchronize(m->stream));
+    m->p.release();
+    m->p = np;
+    np.ptr = nullptr;
+    m->S = S1;
+    m->D.push_back(diffusion_coefficient);
+    m->decay.push_back(decay_rate);
+    // Per-density tables grow with zero entries for the new density.
+    auto widen = [&](std::vector<double>& v, double fill) {
+      if (v.empty()) return;
+      const size_t rows = v.size() / S0;
+      std::vector<double> w(rows * S1, fill);
+      for (size_t r = 0; r < rows; ++r) std::copy_n(&v[r * S0], S0, &w[r * S1]);
+      v.swap(w);
+    };
+    widen(m->dir_val, 0.0);
+    widen(m->bulk_st, 0.0);
+    widen(m->bulk_su, 0.0);
+    widen(m->ag_t1, 0.0);
+    widen(m->ag_t2, 1.0);
+    m->dir_dirty = m->bulk_dirty = m->ag_dirty = true;
+  });
+}
+
+int bfvm_set_density_coefficients(bfvm_solver* m, int index, double diffusion_coefficient,
+                                  double decay_rate) {
+  return SOLVER_CALL(m, {
+    require(index >= 0 && index < m->S, "density index out of range");
+    m->D[index] = diffusion_coefficient;
+    m->decay[index] = decay_rate;
+  });
+}
+
+int bfvm_get_num_densities(bfvm_solver* m, int* num_densities) {
+  return SOLVER_CALL(m, {
+    require(num_densities != nullptr, "null output pointer");
+    *num_densities = m->S;
+  });
+}
+
+int bfvm_set_densities(bfvm_solver* m, const double* host) {
+  return SOLVER_CALL(m, {
+    require(host != nullptr, "null host buffer");
+    const size_t NS = (size_t)m->NS();
+    if (m->precision == BFVM_FP64) {
+      BFVM_CUDA(cudaMemcpyAsync(m->p.ptr, host, NS * sizeof(double), cudaMemcpyHostToDevice,
+                                m->stream));
+    } else {
+      std::vector<float> tmp(host, host + NS);
+      BFVM_CUDA(cudaMemcpyAsync(m->p.ptr, tmp.data(), NS * sizeof(float),
+                                cudaMemcpyHostToDevice, m->stream));
+    }
+    BFVM_CUDA(cudaStreamSynchronize(m->stream));
+  });
+}
+
+int bfvm_get_densities(bfvm_solver* m, double* host) {
+  return SOLVER_CALL(m, {
+    require(host != nullptr, "null host buffer");
+    const size_t NS = (size_t)m->NS();
+    if (m->precision == BFVM_FP64) {
+      BFVM_CUDA(cudaMemcpyAsync(host, m->p.ptr, NS * sizeof(double), cudaMemcpyDeviceToHost,
+                                m->stream));
+      BFVM_CUDA(cudaStreamSynchronize(m->stream));
+    } else {
+      std::vector<float> tmp(NS);
+      BFVM_CUDA(cudaMemcpyAsync(tmp.data(), m->p.ptr, NS * sizeof(float),
+                                cudaMemcpyDeviceToHost, m->stream));
+      BFVM_CUDA(cudaStreamSynchronize(m->stream));
+      std::copy(tmp.begin(), tmp.end(), host);
+    }
+  });
+}
+
+int bfvm_get_voxel_densities(bfvm_solver* m, int64_t count, const int64_t* voxels,
+                             double* values) {
+  return SOLVER_CALL(m, {
+    require(count >= 0 && (count == 0 || (voxels && values)), "bad arguments");
+    validate_voxels(m, count, voxels);
+    if (count == 0) return;
+    DevBuf dv, dout;
+    dv.ensure(count * sizeof(int64_t));
+    dout.ensure(count * m->S * sizeof(double));
+    BFVM_CUDA(cudaMemcpyAsync(dv.ptr, voxels, count * sizeof(int64_t), cudaMemcpyHostToDevice,
+                              m->stream));
+    if (m->precision == BFVM_FP64)
+      gather<double>(m, count, dv.as<int64_t>(), dout.as<double>());
+    else
+      gather<float>(m, count, dv.as<int64_t>(), dout.as<double>());
+    BFVM_CUDA(cudaMemcpyAsync(values, dout.ptr, count * m->S * sizeof(double),
+                              cudaMemcpyDeviceToHost, m->stream));
+    BFVM_CUDA(cudaStreamSynchronize(m->stream));
+    dv.release();
+    dout.release();
+  });
+}
+
+int bfvm_set_voxel_densities(bfvm_solver* m, int64_t count, const int64_t* voxels,
+                             const double* values) {
+  return SOLVER_CALL(m, {
+    require(count >= 0 && (count == 0 || (voxels && values)), "bad arguments");
+    validate_voxels(m, count, voxels);
+    if (count == 0) return;
+    DevBuf dv, din;
+    dv.ensure(count * sizeof(int64_t));
+    din.ensure(count * m->S * sizeof(double));
+    BFVM_CUDA(cudaMemcpyAsync(dv.ptr, voxels, count * sizeof(int64_t), cudaMemcpyHostToDevice,
+                              m->stream));
+    BFVM_CUDA(cudaMemcpyAsync(din.ptr, values, count * m->S * sizeof(double),
+                              cudaMemcpyHostToDevice, m->stream));
+    const int64_t work = count * m->S;
+    if (m->precision == BFVM_FP64)
+      bfvm::scatter_kernel<double><<<(unsigned)blocks_for(work, 256), 256, 0, m->stream>>>(
+          m->p.as<double>(), m->S, count, dv.as<int64_t>(), din.as<double>());
+    else
+      bfvm::scatter_kernel<float><<<(unsigned)blocks_for(work, 256), 256, 0, m->stream>>>(
+          m->p.as<float>(), m->S, count, dv.as<int64_t>(), din.as<double>());
+    check_launch(m);
+    BFVM_CUDA(cudaStreamSynchronize(m->stream));
+    dv.release();
+    din.release();
+  });
+}
+
+int bfvm_device_densities(bfvm_solver* m, void** device_ptr) {
+  return SOLVER_CALL(m, {
+    require(device_ptr != nullptr, "null output pointer");
+    *device_ptr = m->p.ptr;
+  });
+}
+
+int bfvm_set_bulk_rates(bfvm_solver* m, const double* supply, const double* target,
+                        const double* uptake) {
+  return SOLVER_CALL(m, {
+    const int S = m->S;
+    const int64_t N = m->N();
+    m->bulk_vox.clear();
+    m->bulk_st.clear();
+    m->bulk_su.clear();
+    std::vector<double> st(S), su(S);
+    for (int64_t n = 0; n < N; ++n) {
+      const size_t o = (size_t)n * S;
+      bfvm::bulk_coefficients(S, supply ? supply + o : nullptr, target ? target + o : nullptr,
+                              uptake ? uptake + o : nullptr, st.data(), su.data());
+      bool identity = true;
+      for (int s = 0; s < S; ++s) identity = identity && st[s] == 0.0 && su[s] == 0.0;
+      if (identity) continue;
+      m->bulk_vox.push_back(n);
+      m->bulk_st.insert(m->bulk_st.end(), st.begin(), st.end());
+      m->bulk_su.insert(m->bulk_su.end(), su.begin(), su.end());
+    }
+    m->bulk_dirty = true;
+  });
+}
+
+int bfvm_set_bulk_rates_sparse(bfvm_solver* m, int64_t count, const int64_t* voxels,
+                               const double* supply, const double* target,
+                               const double* uptake) {
+  return SOLVER_CALL(m, {
+    require(count >= 0 && (count == 0 || voxels), "bad arguments");
+    validate_voxels(m, count, voxels);
+    const int S = m->S;
+    std::vector<int64_t> order(count);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int64_t a, int64_t b) { return voxels[a] < voxels[b]; });
+    m->bulk_vox.clear();
+    m->bulk_st.clear();
+    m->bulk_su.clear();
+    std::vector<double> st(S), su(S);
+    for (int64_t r = 0; r < count; ++r) {
+      const int64_t e = order[r];
+      require(r == 0 || voxels[e] != m->bulk_vox.back(), "repeated voxel in bulk list");
+      const size_t o = (size_t)e * S;
+      bfvm::bulk_coefficients(S, supply ? supply + o : nullptr, target ? target + o : nullptr,
+                              uptake ? uptake + o : nullptr, st.data(), su.data());
+      m->bulk_vox.push_back(voxels[e]);
+      m->bulk_st.insert(m->bulk_st.end(), st.begin(), st.end());
+      m->bulk_su.insert(m->bulk_su.end(), su.begin(), su.end());
+    }
+    m->bulk_dirty = true;
+  });
+}
+
+int bfvm_add_dirichlet_node(bfvm_solver* m, int64_t voxel, const double* value) {
+  return SOLVER_CALL(m, {
+    require(value != nullptr, "null value vector");
+    validate_voxels(m, 1, &voxel);
+    m->dir_vox.push_back(voxel);
+    m->dir_val.insert(m->dir_val.end(), value, value + m->S);
+    m->dir_dirty = true;
+  });
+}
+
+int bfvm_update_dirichlet_node(bfvm_solver* m, int64_t voxel, const double* value) {
+  return SOLVER_CALL(m, {
+    require(value != nullptr, "null value vector");
+    validate_voxels(m, 1, &voxel);
+    // BioFVM_microenvironment.cpp:153-167: first matching node, else a new one.
+    auto it = std::find(m->dir_vox.begin(), m->dir_vox.end(), voxel);
+    if (it == m->dir_vox.end()) {
+      m->dir_vox.push_back(voxel);
+      m->dir_val.insert(m->dir_val.end(), value, value + m->S);
+    } else {
+      std::copy_n(value, m->S, &m->dir_val[(size_t)(it - m->dir_vox.begin()) * m->S]);
+    }
+    m->dir_dirty = true;
+  });
+}
+
+int bfvm_remove_dirichlet_node(bfvm_solver* m, int64_t voxel) {
+  return SOLVER_CALL(m, {
+    // BioFVM_microenvironment.cpp:169-189 swaps the node with the last one;
+    // the reference then pops the value list twice and never the index list
+    // (:186-187), which leaves the lists inconsistent.  Here both lists lose
+    // exactly the removed node.
+    auto it = std::find(m->dir_vox.begin(), m->dir_vox.end(), voxel);
+    if (it == m->dir_vox.end()) return;
+    const size_t d = (size_t)(it - m->dir_vox.begin()), last = m->dir_vox.size() - 1;
+    m->dir_vox[d] = m->dir_vox[last];
+    std::copy_n(&m->dir_val[last * m->S], m->S, &m->dir_val[d * m->S]);
+    m->dir_vox.pop_back();
+    m->dir_val.resize(m->dir_vox.size() * m->S);
+    m->dir_dirty = true;
+  });
+}
+
+int bfvm_clear_dirichlet_nodes(bfvm_solver* m) {
+  return SOLVER_CALL(m, {
+    m->dir_vox.clear();
+    m->dir_val.clear();
+    m->dir_dirty = true;
+  });
+}
+
+int bfvm_get_num_dirichlet_nodes(bfvm_solver* m, int64_t* count) {
+  return SOLVER_CALL(m, {
+    require(count != nullptr, "null output pointer");
+    *count = (int64_t)m->dir_vox.size();
+  });
+}
+
+int bfvm_set_agents(bfvm_solver* m, int64_t count, const int64_t* voxel, const double* temp1,
+                    const double* temp2) {
+  return SOLVER_CALL(m, {
+    require(count >= 0 && (count == 0 || (voxel && temp1 && temp2)), "bad arguments");
+    require(count < ((int64_t)1 << 31), "too many agents");
+    validate_voxels(m, count, voxel);
+    m->ag_vox.assign(voxel, voxel + count);
+    m->ag_t1.assign(temp1, temp1 + count * m->S);
+    m->ag_t2.assign(temp2, temp2 + count * m->S);
+    m->ag_dirty = true;
+  });
+}
+
+int bfvm_get_agent_densities(bfvm_solver* m, double* values) {
+  return SOLVER_CALL(m, {
+    const int64_t A = (int64_t)m->ag_vox.size();
+    if (A == 0) return;
+    require(values != nullptr, "null output buffer");
+    build_agents(m);
+    m->d_gather.ensure(A * m->S * sizeof(double));
+    if (m->precision == BFVM_FP64)
+      gather<double>(m, A, m->d_ag_vox_orig.as<int64_t>(), m->d_gather.as<double>());
+    else
+      gather<float>(m, A, m->d_ag_vox_orig.as<int64_t>(), m->d_gather.as<double>());
+    BFVM_CUDA(cudaMemcpyAsync(values, m->d_gather.ptr, A * m->S * sizeof(double),
+                              cudaMemcpyDeviceToHost, m->stream));
+    BFVM_CUDA(cudaStreamSynchronize(m->stream));
+  });
+}
+
+int bfvm_simulate_bulk_sources_and_sinks(bfvm_solver* m, double dt) {
+  return SOLVER_CALL(m, {
+    build_bulk(m);
+    bulk_any(m, dt);
+  });
+}
+
+int bfvm_simulate_cell_sources_and_sinks(bfvm_solver* m, double dt) {
+  (void)dt;  // unused by the reference as well (BioFVM_basic_agent.cpp:229)
+  return SOLVER_CALL(m, {
+    build_agents(m);
+    cells_any(m);
+  });
+}
+
+int bfvm_simulate_diffusion_decay(bfvm_solver* m, double dt) {
+  return SOLVER_CALL(m, diffusion(m, dt, 0));
+}
+
+int bfvm_apply_dirichlet_conditions(bfvm_solver* m) {
+  return SOLVER_CALL(m, {
+    build_dirichlet(m);
+    if (m->precision == BFVM_FP64)
+      dirichlet_standalone<double>(m);
+    else
+      dirichlet_standalone<float>(m);
+  });
+}
+
+int bfvm_step(bfvm_solver* m, double dt, int nsteps, int flags) {
+  return SOLVER_CALL(m, {
+    require(nsteps >= 0, "negative step count");
+    require((flags & ~BFVM_STEP_ALL) == 0, "unknown step flags");
+    if (!(flags & BFVM_STEP_DIFFUSION)) {
+      // No sweep to fuse into: the per-voxel kernels alone.
+      build_bulk(m);
+      build_agents(m);
+      for (int it = 0; it < nsteps; ++it) {
+        if (flags & BFVM_STEP_BULK) bulk_any(m, dt);
+        if (flags & BFVM_STEP_CELLS) cells_any(m);
+      }
+      return;
+    }
+    int fuse = 0;
+    if (flags & BFVM_STEP_BULK) fuse |= bfvm::kFuseBulk;
+    if (flags & BFVM_STEP_CELLS) fuse |= bfvm::kFuseCells;
+    for (int it = 0; it < nsteps; ++it) diffusion(m, dt, fuse);
+  });
+}
+
+int bfvm_reset_diffusion_setup(bfvm_solver* m) {
+  return SOLVER_CALL(m, { m->setup_done = false; });
+}
+
+int bfvm_set_precision(bfvm_solver* m, int precision) {
+  return SOLVER_CALL(m, {
+    require(precision == BFVM_FP64 || precision == BFVM_FP32, "precision must be 64 or 32");
+    if (precision == m->precision) return;
+    const int64_t NS = m->NS();
+    DevBuf np;
+    np.ensure(std::max<size_t>(NS * (precision == BFVM_FP64 ? 8 : 4), 16));
+    if (NS > 0) {
+      if (precision == BFVM_FP32)
+        bfvm::convert_kernel<float, double><<<(unsigned)blocks_for(NS, 256), 256, 0, m->stream>>>(
+            np.as<float>(), m->p.as<double>(), NS);
+      else
+        bfvm::convert_kernel<double, float><<<(unsigned)blocks_for(NS, 256), 256, 0, m->stream>>>(
+            np.as<double>(), m->p.as<float>(), NS);
+      check_launch(m);
+    }
+    BFVM_CUDA(cudaStreamSynchronize(m->stream));
+    m->p.release();
+    m->p = np;
+    np.ptr = nullptr;
+    m->precision = precision;
+    m->setup_done = false;  // coefficient tables are kept in the sweep precision
+    choose_axes(m);
+    // segment lists depend on the chunk lengths
+    m->bulk_dirty = m->dir_dirty = m->ag_dirty = true;
+  });
+}
+
+int bfvm_synchronize(bfvm_solver* m) {
+  return SOLVER_CALL(m, BFVM_CUDA(cudaStreamSynchronize(m->stream)));
+}
+
+int bfvm_get_stream(bfvm_solver* m, void** stream) {
+  return SOLVER_CALL(m, {
+    require(stream != nullptr, "null output pointer");
+    *stream = (void*)m->stream;
+  });
+}
+
+int bfvm_get_launch_count(bfvm_solver* m, int64_t* count) {
+  return SOLVER_CALL(m, {
+    require(count != nullptr, "null output pointer");
+    *count = m->launches;
+  });
+}
+
+int bfvm_profile_step(bfvm_solver* m, double dt, int nsteps, int flags, double* ms) {
+  return SOLVER_CALL(m, {
+    require(ms != nullptr && nsteps > 0, "bad arguments");
+    require(flags & BFVM_STEP_DIFFUSION, "profiling needs the diffusion sweeps");
+    check_lod_mesh(m);
+    if (!m->setup_done) thomas_setup(m, dt);
+    build_all(m);
+    int fuse = 0;
+    if (flags & BFVM_STEP_BULK) fuse |= bfvm::kFuseBulk;
+    if (flags & BFVM_STEP_CELLS) fuse |= bfvm::kFuseCells;
+    cudaEvent_t ev[4];
+    for (auto& e : ev) BFVM_CUDA(cudaEventCreate(&e));
+    double acc[3] = {0, 0, 0};
+    for (int it = 0; it < nsteps; ++it) {
+      BFVM_CUDA(cudaEventRecord(ev[0], m->stream));
+      sweep(m, 0, fuse | bfvm::kFuseDirPro | bfvm::kFuseDirEpi, dt);
+      BFVM_CUDA(cudaEventRecord(ev[1], m->stream));
+      sweep(m, 1, bfvm::kFuseDirEpi, dt);
+      BFVM_CUDA(cudaEventRecord(ev[2], m->stream));
+      sweep(m, 2, 0, dt);
+      BFVM_CUDA(cudaEventRecord(ev[3], m->stream));
+      BFVM_CUDA(cudaEventSynchronize(ev[3]));
+      for (int a = 0; a < 3; ++a) {
+        float t = 0;
+        BFVM_CUDA(cudaEventElapsedTime(&t, ev[a], ev[a + 1]));
+        acc[a] += t;
+      }
+    }
+    for (int a = 0; a < 3; ++a) ms[a] = acc[a] / nsteps;
+    for (auto& e : ev) cudaEventDestroy(e);
+  });
+}
+
+}  // extern "C"

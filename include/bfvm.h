@@ -1,0 +1,175 @@
+/* bfvm.h -- C ABI of the B200-native BioFVM transport path (libbfvm.so).
+ *
+ * One bfvm_solver holds the device state of one BioFVM Microenvironment: the
+ * density field (resident in HBM, layout [voxel][substrate], voxel
+ * n = (k*ny + j)*nx + i, the reference's own logical order), the Thomas
+ * coefficients, the bulk source/sink table, the Dirichlet nodes and the
+ * agents' secretion/uptake constants.  Host pointers in every signature are
+ * plain host memory; nothing here takes or returns a torch type.
+ *
+ * Each entry point names the reference interface it replaces (file:line in
+ * the BioFVM 1.0.4 source tree).  Every call returns 0 on success or a
+ * BFVM_ERR_* code; bfvm_last_error() gives a message for the calling thread.
+ * Work is enqueued on the solver's CUDA stream; calls that return host data
+ * synchronise that stream.  Calls on one solver must not race from several
+ * host threads. */
+#ifndef BFVM_H
+#define BFVM_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define BFVM_API __attribute__((visibility("default")))
+#else
+#define BFVM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BFVM_OK 0
+#define BFVM_ERR_ARG 1     /* bad argument (size, index, pointer)            */
+#define BFVM_ERR_CUDA 2    /* a CUDA runtime call failed                      */
+#define BFVM_ERR_STATE 3   /* call not valid in the current state             */
+#define BFVM_ERR_NOMEM 4   /* device or host allocation failed                */
+#define BFVM_ERR_MESH 5    /* LOD_3D needs a uniform Cartesian mesh           */
+
+/* step flags for bfvm_step: the three simulate_* calls of one step */
+#define BFVM_STEP_BULK 1
+#define BFVM_STEP_CELLS 2
+#define BFVM_STEP_DIFFUSION 4
+#define BFVM_STEP_ALL 7
+
+/* precision of the density field and the sweeps */
+#define BFVM_FP64 64
+#define BFVM_FP32 32
+
+typedef struct bfvm_solver bfvm_solver;
+
+/* Message of the last failed call on this host thread ("" if none). */
+BFVM_API const char* bfvm_last_error(void);
+BFVM_API int bfvm_version(void);
+
+/* Microenvironment::Microenvironment() (BioFVM_microenvironment.cpp:88-139):
+ * a 1x1x1 mesh with one density, D = decay = 0, LOD_3D solver selected. */
+BFVM_API int bfvm_create(bfvm_solver** out, int device);
+BFVM_API int bfvm_destroy(bfvm_solver* m);
+
+/* Microenvironment::resize_space(x0,x1,y0,y1,z0,z1,dx,dy,dz)
+ * (BioFVM_microenvironment.cpp:267-285 -> Cartesian_Mesh::resize,
+ * BioFVM_mesh.cpp:796-922): node counts ceil(1e-16 + L/d).  Densities are
+ * reset to zero, Dirichlet nodes, bulk table and agents are cleared. */
+BFVM_API int bfvm_resize_space(bfvm_solver* m, double x0, double x1, double y0, double y1, double z0,
+                      double z1, double dx, double dy, double dz);
+/* Microenvironment::resize_space(x0,...,z1, nx, ny, nz)
+ * (BioFVM_microenvironment.cpp:246-265 -> BioFVM_mesh.cpp:663-794). */
+BFVM_API int bfvm_resize_space_nodes(bfvm_solver* m, double x0, double x1, double y0, double y1,
+                            double z0, double z1, int nx, int ny, int nz);
+/* nxyz[3] node counts; geom[10] = dx, dy, dz, dV, bounding box
+ * (xmin, ymin, zmin, xmax, ymax, zmax); flags[2] = uniform_mesh, S. */
+BFVM_API int bfvm_get_mesh(bfvm_solver* m, int* nxyz, double* geom, int* flags);
+
+/* Microenvironment::resize_densities (BioFVM_microenvironment.cpp:292-323):
+ * S densities, all zero, D = decay = 0. */
+BFVM_API int bfvm_resize_densities(bfvm_solver* m, int num_densities);
+/* Microenvironment::add_density(name, units, D, decay)
+ * (BioFVM_microenvironment.cpp:404-441): appends one zero density. */
+BFVM_API int bfvm_add_density(bfvm_solver* m, double diffusion_coefficient, double decay_rate);
+/* Microenvironment::set_density(index, name, units, D, decay)
+ * (BioFVM_microenvironment.cpp:450-458) and the public
+ * diffusion_coefficients / decay_rates vectors (BioFVM_microenvironment.h:118-119).
+ * Read by the next Thomas set-up (see bfvm_reset_diffusion_setup). */
+BFVM_API int bfvm_set_density_coefficients(bfvm_solver* m, int index, double diffusion_coefficient,
+                                  double decay_rate);
+BFVM_API int bfvm_get_num_densities(bfvm_solver* m, int* num_densities);
+
+/* Whole-field transfers of p_density_vectors (BioFVM_microenvironment.h:63),
+ * host buffer [N][S] doubles.  In FP32 mode values are converted. */
+BFVM_API int bfvm_set_densities(bfvm_solver* m, const double* host);
+BFVM_API int bfvm_get_densities(bfvm_solver* m, double* host);
+/* Per-voxel access, the device analogue of density_vector(n)
+ * (BioFVM_microenvironment.cpp:499-500): values [count][S]. */
+BFVM_API int bfvm_get_voxel_densities(bfvm_solver* m, int64_t count, const int64_t* voxels,
+                             double* values);
+BFVM_API int bfvm_set_voxel_densities(bfvm_solver* m, int64_t count, const int64_t* voxels,
+                             const double* values);
+/* Device address of the density field ([N][S], double or float per the
+ * precision); valid until the next resize or precision change. */
+BFVM_API int bfvm_device_densities(bfvm_solver* m, void** device_ptr);
+
+/* The three bulk callbacks bulk_supply_rate_function,
+ * bulk_supply_target_densities_function, bulk_uptake_rate_function
+ * (BioFVM_microenvironment.h:130-132), evaluated by the caller for every
+ * voxel: [N][S] each, NULL = the reference default zero_function.  Voxels
+ * whose supply and uptake are zero for every density are identities of
+ * simulate_bulk_sources_and_sinks and are not stored. */
+BFVM_API int bfvm_set_bulk_rates(bfvm_solver* m, const double* supply, const double* target,
+                        const double* uptake);
+/* Same, listing only the voxels with non-zero rates: [count][S] each. */
+BFVM_API int bfvm_set_bulk_rates_sparse(bfvm_solver* m, int64_t count, const int64_t* voxels,
+                               const double* supply, const double* target,
+                               const double* uptake);
+
+/* Microenvironment::add_dirichlet_node / update_dirichlet_node /
+ * remove_dirichlet_node (BioFVM_microenvironment.cpp:146-189); value [S].
+ * Nodes are applied in list order (a later node for the same voxel wins). */
+BFVM_API int bfvm_add_dirichlet_node(bfvm_solver* m, int64_t voxel, const double* value);
+BFVM_API int bfvm_update_dirichlet_node(bfvm_solver* m, int64_t voxel, const double* value);
+BFVM_API int bfvm_remove_dirichlet_node(bfvm_solver* m, int64_t voxel);
+BFVM_API int bfvm_clear_dirichlet_nodes(bfvm_solver* m);
+BFVM_API int bfvm_get_num_dirichlet_nodes(bfvm_solver* m, int64_t* count);
+
+/* The agents' cell_source_sink_solver_temp1/temp2 of
+ * Basic_Agent::set_internal_uptake_constants (BioFVM_basic_agent.cpp:114-148)
+ * with current_voxel_index, in agent-list order (all_basic_agents,
+ * BioFVM_basic_agent.cpp:35): voxel[A], temp1[A][S], temp2[A][S]. */
+BFVM_API int bfvm_set_agents(bfvm_solver* m, int64_t count, const int64_t* voxel, const double* temp1,
+                    const double* temp2);
+/* Densities at the agents' voxels, [A][S], agent order: the read a caller
+ * makes through Basic_Agent::nearest_density_vector (BioFVM_basic_agent.cpp:223). */
+BFVM_API int bfvm_get_agent_densities(bfvm_solver* m, double* values);
+
+/* Microenvironment::simulate_bulk_sources_and_sinks
+ * (BioFVM_microenvironment.cpp:584-613). */
+BFVM_API int bfvm_simulate_bulk_sources_and_sinks(bfvm_solver* m, double dt);
+/* Microenvironment::simulate_cell_sources_and_sinks
+ * (BioFVM_microenvironment.cpp:615-633): agents applied in list order. */
+BFVM_API int bfvm_simulate_cell_sources_and_sinks(bfvm_solver* m, double dt);
+/* Microenvironment::simulate_diffusion_decay (BioFVM_microenvironment.cpp:502-513)
+ * dispatching to diffusion_decay_solver__constant_coefficients_LOD_3D
+ * (BioFVM_solvers.cpp:77-276). */
+BFVM_API int bfvm_simulate_diffusion_decay(bfvm_solver* m, double dt);
+/* Microenvironment::apply_dirichlet_conditions (BioFVM_microenvironment.cpp:192-197). */
+BFVM_API int bfvm_apply_dirichlet_conditions(bfvm_solver* m);
+/* nsteps of the canonical step bulk -> cells -> diffusion
+ * (examples/performance_test_numcells.cpp:177-179), fused into three sweep
+ * kernels per step; flags selects the parts (BFVM_STEP_*). */
+BFVM_API int bfvm_step(bfvm_solver* m, double dt, int nsteps, int flags);
+
+/* The reference computes the Thomas coefficients on the first diffusion call
+ * and never again (diffusion_solver_setup_done, BioFVM_solvers.cpp:87,172),
+ * so later changes of dt, D or decay are ignored.  This keeps that behaviour
+ * and offers the explicit reset the reference lacks. */
+BFVM_API int bfvm_reset_diffusion_setup(bfvm_solver* m);
+
+/* FP64 (default, the reference's arithmetic) or FP32 sweeps (coefficients
+ * still computed in FP64, cell sources accumulated in FP64).  Converts the
+ * resident field. */
+BFVM_API int bfvm_set_precision(bfvm_solver* m, int precision);
+
+BFVM_API int bfvm_synchronize(bfvm_solver* m);
+/* The solver's cudaStream_t, for events and interop. */
+BFVM_API int bfvm_get_stream(bfvm_solver* m, void** stream);
+/* Kernel launches enqueued by this solver since creation. */
+BFVM_API int bfvm_get_launch_count(bfvm_solver* m, int64_t* count);
+
+/* Times one fused step's three sweep kernels with CUDA events on the solver's
+ * stream, averaged over nsteps steps: ms[3] = x (with bulk/cells/Dirichlet
+ * prologue), y, z. */
+BFVM_API int bfvm_profile_step(bfvm_solver* m, double dt, int nsteps, int flags, double* ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

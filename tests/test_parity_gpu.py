@@ -1,0 +1,203 @@
+"""Parity of the CUDA path (through the C ABI) with the reference.
+
+Tolerances: FP64 relative max-norm error per substrate
+<= 1e-12 against the oracle/reference; the per-voxel kernels (bulk, cells,
+Dirichlet) are bit-exact; FP32 sweeps <= 1e-5.
+"""
+import numpy as np
+import pytest
+
+from biofvm_b200 import STEP_BULK, STEP_CELLS, STEP_DIFFUSION, Solver, load_scenario
+from biofvm_b200 import workloads as W
+from biofvm_b200._abi import BfvmError
+from cases import CASES, sha
+from conftest import load_golden
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12
+TOL32 = 1e-5
+
+
+def rel_err(a, b):
+    return O.max_rel_err(a, b)
+
+
+def run_gpu(scn, steps, flags, fused=True, precision=64):
+    with Solver(0) as sv:
+        load_scenario(sv, scn)
+        if precision != 64:
+            sv.set_precision(precision)
+        if fused:
+            sv.step(scn.dt, steps, flags)
+        else:
+            for _ in range(steps):
+                if flags & STEP_BULK:
+                    sv.simulate_bulk_sources_and_sinks(scn.dt)
+                if flags & STEP_CELLS:
+                    sv.simulate_cell_sources_and_sinks(scn.dt)
+                if flags & STEP_DIFFUSION:
+                    sv.simulate_diffusion_decay(scn.dt)
+        return sv.get_densities()
+
+
+@pytest.mark.parametrize("fused", [True, False], ids=["fused", "per_call"])
+@pytest.mark.parametrize("name", list(CASES))
+def test_golden_cases(name, fused):
+    build, flags, steps, _ = CASES[name]
+    scn = build()
+    g = load_golden(name)
+    p = run_gpu(scn, steps, flags, fused)
+    assert p.shape == tuple(g["shape"])
+    if not flags & STEP_DIFFUSION:
+        # per-voxel updates only: same IEEE operations in the same order
+        assert sha(p) == str(g["sha"])
+        return
+    if "p" in g:
+        ref = g["p"]
+    else:
+        ref = O.oracle_run(scn, steps, flags)
+        assert sha(ref) == str(g["sha"])
+    err = rel_err(p, ref)
+    assert np.all(err <= TOL64), err
+    assert np.all(np.isfinite(p))
+
+
+def test_dirichlet_alone_is_exact():
+    scn = W.mixed_small(shape=(10, 9, 8), S=3, n_agents=0, seed=41)
+    with Solver(0) as sv:
+        load_scenario(sv, scn)
+        sv.apply_dirichlet_conditions()
+        got = sv.get_densities()
+    exp = scn.initial_field()
+    for v, x in zip(scn.dirichlet_voxels, scn.dirichlet_values):
+        exp[v] = x
+    assert np.array_equal(got, exp)
+
+
+def test_dirichlet_update_and_remove():
+    """update_dirichlet_node changes the first matching node; remove takes the
+    node out of both lists (the reference's remove pops the value list twice,
+    BioFVM_microenvironment.cpp:186-187; here the lists stay consistent)."""
+    scn = W.mixed_small(shape=(8, 8, 8), S=2, n_agents=0, seed=42, dirichlet=False, bulk=False)
+    with Solver(0) as sv:
+        load_scenario(sv, scn)
+        sv.add_dirichlet_node(5, [1.0, 2.0])
+        sv.add_dirichlet_node(77, [3.0, 4.0])
+        sv.add_dirichlet_node(300, [5.0, 6.0])
+        sv.update_dirichlet_node(77, [7.0, 8.0])
+        sv.remove_dirichlet_node(5)
+        sv.update_dirichlet_node(400, [9.0, 9.5])  # not present: added
+        sv.apply_dirichlet_conditions()
+        got = sv.get_densities()
+    exp = scn.initial_field()
+    exp[77] = [7.0, 8.0]
+    exp[300] = [5.0, 6.0]
+    exp[400] = [9.0, 9.5]
+    assert np.array_equal(got, exp)
+
+
+def test_voxel_and_agent_access():
+    scn = W.mixed_small(shape=(11, 7, 5), S=2, n_agents=50, seed=43)
+    with Solver(0) as sv:
+        load_scenario(sv, scn)
+        vox = np.array([0, 3, 384, 3], np.int64)
+        np.testing.assert_array_equal(sv.get_voxel_densities(vox), scn.p0[vox])
+        sv.set_voxel_densities([1, 2], [[10.0, 11.0], [12.0, 13.0]])
+        p = sv.get_densities()
+        assert np.array_equal(p[1:3], [[10.0, 11.0], [12.0, 13.0]])
+        out = np.empty((scn.num_agents, scn.S))
+        sv.get_agent_densities(out)
+        v, _, _ = scn.agent_arrays()
+        assert np.array_equal(out, p[v])
+
+
+def test_bad_arguments_are_reported():
+    with Solver(0) as sv:
+        sv.resize_space(0, 100, 0, 100, 0, 100, 10)
+        with pytest.raises(BfvmError) as e:
+            sv.set_agents([1000], [[0.0]], [[1.0]])
+        assert "outside" in str(e.value)
+        with pytest.raises(BfvmError):
+            sv.add_dirichlet_node(-1, [1.0])
+
+
+def test_non_uniform_mesh_is_rejected_like_the_reference():
+    with Solver(0) as sv:
+        sv.resize_space(0, 100, 0, 100, 0, 100, 10, 20, 10)
+        with pytest.raises(BfvmError) as e:
+            sv.simulate_diffusion_decay(0.01)
+        assert "uniform Cartesian" in str(e.value)
+
+
+def test_add_density_keeps_existing_values():
+    scn = W.mixed_small(shape=(6, 5, 4), S=2, n_agents=0, seed=44, dirichlet=False, bulk=False)
+    with Solver(0) as sv:
+        load_scenario(sv, scn)
+        sv.add_density(1e3, 0.1)
+        p = sv.get_densities()
+    assert p.shape == (scn.num_voxels, 3)
+    assert np.array_equal(p[:, :2], scn.p0) and np.all(p[:, 2] == 0)
+
+
+def test_stale_thomas_setup_matches_reference_and_can_be_reset():
+    """The reference computes its Thomas coefficients once, from the first
+    dt (BioFVM_solvers.cpp:87,172); a later dt only changes bulk/cells."""
+    scn = W.mixed_small(shape=(10, 8, 6), S=2, n_agents=0, seed=45, dirichlet=False, bulk=False)
+    with Solver(0) as sv:
+        load_scenario(sv, scn)
+        sv.simulate_diffusion_decay(0.01)
+        sv.simulate_diffusion_decay(0.05)  # coefficients still those of dt=0.01
+        stale = sv.get_densities()
+        sv.set_densities(scn.p0)
+        sv.reset_diffusion_setup()
+        sv.simulate_diffusion_decay(0.05)
+        fresh = sv.get_densities()
+    exp = O.oracle_run(scn, 2, 4)
+    assert np.all(rel_err(stale, exp) <= TOL64)
+    scn5 = W.mixed_small(shape=(10, 8, 6), S=2, n_agents=0, seed=45, dirichlet=False,
+                         bulk=False)
+    scn5.dt = 0.05
+    exp5 = O.oracle_run(scn5, 1, 4)
+    assert np.all(rel_err(fresh, exp5) <= TOL64)
+
+
+def test_plain_50_against_reference_golden():
+    """The 50^3 workload end to end (100 fused steps), checked against the
+    unmodified reference's output digest through the oracle."""
+    scn = W.plain_50()
+    p = run_gpu(scn, 100, 7)
+    g = load_golden("plain_50")
+    ref = O.oracle_run(scn, 100, 7)
+    assert sha(ref) == str(g["sha"])
+    assert np.all(rel_err(p, ref) <= TOL64)
+
+
+def test_fp32_sweeps_error_bound():
+    scn = W.lod_cube(48, 4, 2000, steps=20, seed=5, bulk_radius=150.0, name="lod_48")
+    ref = O.oracle_run(scn, 20, 7)
+    p32 = run_gpu(scn, 20, 7, precision=32)
+    err = rel_err(p32, ref)
+    assert np.all(err <= TOL32), err
+
+
+@pytest.mark.slow
+def test_lod_256_full_size_two_steps():
+    """The full 256^3 x 10 workload with 100k agents: two fused steps against
+    the oracle, then the exact per-substrate balance of a diffusion-only step."""
+    scn = W.lod_256(steps=2)
+    p = run_gpu(scn, 2, 7)
+    ref = O.oracle_run(scn, 2, 7)
+    err = rel_err(p, ref)
+    assert np.all(err <= TOL64), err
+    # balance: Neumann boundaries, no sources -> total / (1 + dt*decay/3)^3
+    with Solver(0) as sv:
+        load_scenario(sv, scn)
+        rng = np.random.default_rng(0)
+        p0 = rng.random((scn.num_voxels, scn.S))
+        sv.set_densities(p0)
+        sv.step(scn.dt, 1, STEP_DIFFUSION)
+        p1 = sv.get_densities()
+    c2 = scn.dt * scn.decay / 3.0
+    np.testing.assert_allclose(p1.sum(0), p0.sum(0) / (1 + c2) ** 3, rtol=1e-12)

@@ -224,7 +224,11 @@ def run_ours(args, world, rank, local):
     from biofvm_b200 import STEP_ALL, Solver, load_scenario
     from biofvm_b200 import workloads as W
 
-    scn = W.lod_256(steps=args.steps)
+    if args.size == 256 and args.substrates == 10 and args.agents == 100_000:
+        scn = W.lod_256(steps=args.steps)
+    else:
+        scn = W.lod_cube(args.size, args.substrates, args.agents, steps=args.steps,
+                         name=f"lod_{args.size}")
     N, S = scn.num_voxels, scn.S
     sv = Solver(local)
     load_scenario(sv, scn)
@@ -255,9 +259,10 @@ def run_ours(args, world, rank, local):
     ms_step = ms / args.steps
 
     # per-kernel device times on the solver's stream (CUDA events between sweeps)
-    kx, ky, kz = sv.profile_step(dt, max(3, min(args.steps, 10)), STEP_ALL)
-    per = {"x_sweep_fused": kx, "y_sweep": ky, "z_sweep": kz}
+    ks, kx, ky, kz = sv.profile_step(dt, max(3, min(args.steps, 10)), STEP_ALL)
+    per = {"x_sweep": kx, "y_sweep": ky, "z_sweep": kz}
     dom = max(per, key=per.get)
+    per["sources"] = ks
     hbm, peak_kind = peaks()
     achieved = BYTES_PER_VS_SWEEP * N * S / (per[dom] / 1e3) / 1e9
     traffic = ncu_traffic(dom)
@@ -303,8 +308,8 @@ def run_ours(args, world, rank, local):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded)",
-            "config": {"workload": "lod_256: 256^3 voxels x 10 substrates FP64, 100k agents, "
-                                   "bulk sphere r=500um, dt=0.01",
+            "config": {"workload": f"{scn.name}: {args.size}^3 voxels x {S} substrates FP64, "
+                                   f"{scn.num_agents} agents, bulk sphere r=500um, dt=0.01",
                        "voxels": N, "substrates": S, "agents": scn.num_agents,
                        "l2": "inputs (1.34 GB field) larger than L2; no flush",
                        "parallelism": f"instances x{world}" if world > 1 else "1 GPU"},
@@ -331,6 +336,9 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--size", type=int, default=256, help="cube edge in voxels (default 256)")
+    ap.add_argument("--substrates", type=int, default=10)
+    ap.add_argument("--agents", type=int, default=100_000)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     world, rank, local = dist_init(args)

@@ -26,6 +26,11 @@ STEP_CELLS = 2
 STEP_DIFFUSION = 4
 STEP_ALL = 7
 
+PATH_AUTO = 0
+PATH_GENERIC = 1
+PATH_TMA = 2
+PATH_DIRECT = 3
+
 FP64 = 64
 FP32 = 32
 
@@ -42,6 +47,7 @@ SIGNATURES = {
     "bfvm_destroy": (c_int, [_P]),
     "bfvm_resize_space": (c_int, [_P] + [c_double] * 9),
     "bfvm_resize_space_nodes": (c_int, [_P] + [c_double] * 6 + [c_int] * 3),
+    "bfvm_set_mesh": (c_int, [_P, _IP, _DP, c_int]),
     "bfvm_get_mesh": (c_int, [_P, _IP, _DP, _IP]),
     "bfvm_resize_densities": (c_int, [_P, c_int]),
     "bfvm_add_density": (c_int, [_P, c_double, c_double]),
@@ -64,10 +70,15 @@ SIGNATURES = {
     "bfvm_simulate_bulk_sources_and_sinks": (c_int, [_P, c_double]),
     "bfvm_simulate_cell_sources_and_sinks": (c_int, [_P, c_double]),
     "bfvm_simulate_diffusion_decay": (c_int, [_P, c_double]),
+    "bfvm_simulate_diffusion_decay_2d": (c_int, [_P, c_double]),
     "bfvm_apply_dirichlet_conditions": (c_int, [_P]),
     "bfvm_step": (c_int, [_P, c_double, c_int, c_int]),
     "bfvm_reset_diffusion_setup": (c_int, [_P]),
     "bfvm_set_precision": (c_int, [_P, c_int]),
+    "bfvm_set_sweep_config": (c_int, [_P, c_int, c_int, c_int, c_int]),
+    "bfvm_get_sweep_config": (c_int, [_P, c_int, _IP]),
+    "bfvm_set_kernel_path": (c_int, [_P, c_int]),
+    "bfvm_set_fuse_sources": (c_int, [_P, c_int]),
     "bfvm_synchronize": (c_int, [_P]),
     "bfvm_get_stream": (c_int, [_P, POINTER(c_void_p)]),
     "bfvm_get_launch_count": (c_int, [_P, _LP]),

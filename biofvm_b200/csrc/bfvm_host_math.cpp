@@ -14,7 +14,7 @@ int nodes_from_spacing(double start, double end, double d) {
 }
 
 void thomas_axis(int n, int S, double dx, double dt, const double* D, const double* decay,
-                 double* c1, double* denom, double* cx) {
+                 double* c1, double* denom, double* cx, int dims) {
   for (int s = 0; s < S; ++s) {
     // BioFVM_solvers.cpp:105-126: the constants are built by the same
     // sequence of elementwise operations.
@@ -26,7 +26,10 @@ void thomas_axis(int n, int S, double dx, double dt, const double* D, const doub
     k1a *= -1.0;
     double k2 = decay[s];
     k2 *= dt;
-    k2 /= 3.0;
+    if (dims == 2)
+      k2 *= 0.5;  // LOD_2D splits the decay over two sweeps (BioFVM_solvers.cpp:311-312)
+    else
+      k2 /= 3.0;
     double k3 = 1.0;
     k3 += k1;
     k3 += k1;
@@ -67,6 +70,45 @@ void bulk_coefficients(int S, const double* supply, const double* target, const 
     st[s] = t2;
     su[s] = t3;
   }
+}
+
+}  // namespace bfvm
+
+namespace bfvm {
+
+void chunk_tables(int n, int S, int ch, const double* c1, const double* denom, const double* cx,
+                  double* k1, double* kg, double* kc) {
+  const int nc = (n + ch - 1) / ch;
+  for (size_t i = 0; i < (size_t)nc * ch * S * 2; ++i) k1[i] = kg[i] = 0.0;
+  for (int s = 0; s < S; ++s) {
+    for (int c = 0; c < nc; ++c) {
+      const int k0 = c * ch, k1e = (k0 + ch < n) ? k0 + ch : n;
+      double P = 1.0;
+      for (int k = k0; k < k1e; ++k) {
+        const size_t q = (size_t)k * S + s;
+        const double a = -cx[q];  // == c1[s] / denom[q], see the header
+        P *= a;
+        k1[q * 2 + 0] = 1.0 / denom[q];
+        k1[q * 2 + 1] = a;
+        kg[q * 2 + 0] = P;  // P_k for now, turned into G_k below
+      }
+      double R = 1.0, G = 0.0;
+      for (int k = k1e - 1; k >= k0; --k) {
+        const size_t q = (size_t)k * S + s;
+        const double a = k1[q * 2 + 1];
+        G = kg[q * 2 + 0] + a * G;
+        R *= a;
+        kg[q * 2 + 0] = G;
+        kg[q * 2 + 1] = R;
+      }
+      double* t = kc + ((size_t)c * S + s) * 4;
+      t[0] = P;
+      t[1] = kg[((size_t)k0 * S + s) * 2 + 0];
+      t[2] = kg[((size_t)k0 * S + s) * 2 + 1];
+      t[3] = 0.0;
+    }
+  }
+  (void)c1;
 }
 
 }  // namespace bfvm

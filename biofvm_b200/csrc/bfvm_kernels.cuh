@@ -120,9 +120,11 @@ __device__ __forceinline__ void apply_dirichlet_seg(T (&v)[CH], const SegList& L
 // the plain sweeps free of the prologue's registers.
 enum : int { kSweepPlain = 0, kSweepDirEpi = 1, kSweepFull = 2 };
 
-template <typename T, int CH, int MODE>
-__global__ void __launch_bounds__(512) lod_sweep_kernel(const SweepArgs<T> a) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+// MINB = minimum resident blocks per SM requested from the compiler (1 or 2):
+// 2 caps registers at 64 per thread so two 512-thread blocks fit an SM.
+template <typename T, int CH, int MODE, int MINB>
+__global__ void __launch_bounds__(512, MINB) lod_sweep_kernel(const SweepArgs<T> a) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   const int TW = blockDim.x;
   const int NC = blockDim.y;
   T* sQ = reinterpret_cast<T*>(smem_raw);  // [NC][TW] forward chunk end values

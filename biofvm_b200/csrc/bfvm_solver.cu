@@ -15,6 +15,8 @@
 #include "bfvm.h"
 #include "bfvm_host_math.h"
 #include "bfvm_kernels.cuh"
+#include "bfvm_kernels_tma.cuh"
+#include <cudaTypedefs.h>
 
 namespace {
 
@@ -100,6 +102,8 @@ std::vector<int> segment_offsets(int64_t nlines, int nchunks, int ch,
 struct Axis {
   int ch = 16;  // points per thread
   int tw = 32;  // columns per block
+  int minb = 1; // resident blocks per SM the kernel is compiled for (1 or 2)
+  bool user = false;  // set through bfvm_set_sweep_config
 };
 
 }  // namespace
@@ -124,6 +128,11 @@ struct bfvm_solver {
   // Thomas coefficients (computed once, BioFVM_solvers.cpp:87,172)
   bool setup_done = false;
   DevBuf coef[3];  // per axis: inv_den, fwd, bwd [n*S] then c1 [S], in the sweep precision
+  std::vector<double> h_c1[3], h_den[3], h_cx[3];  // FP64 host copies per axis
+  DevBuf chunk[3];     // per axis: chunk tables k1, kg, kc by slot (sweep precision)
+  DevBuf chunk_slots[3];  // per axis: slot of every chunk
+  int chunk_ch[3] = {0, 0, 0};
+  int chunk_nslots[3] = {0, 0, 0};
   Axis axis[3];
 
   // bulk sources/sinks: non-identity voxels, ascending
@@ -149,6 +158,17 @@ struct bfvm_solver {
   DevBuf d_ag_vox_orig, d_group_vox, d_group_start, d_gather;
   DevSegList seg_cells;
 
+  // device status word: set to non-zero by a kernel whose bounded wait failed
+  DevBuf d_status;
+  int num_sms = 148;
+  int path = 0;  // BFVM_PATH_*
+  int fuse_sources = 0;  // bulk/cell updates in the x sweep's prologue
+  int lod_dims = 3;      // 2 while a LOD_2D step runs: sweeps of the z = 0 plane only
+  // cached tensor maps of the y and z sweeps (keyed by field pointer)
+  CUtensorMap maps[3];
+  const void* map_key[3] = {nullptr, nullptr, nullptr};
+  int map_w[3] = {0, 0, 0};
+
   int64_t N() const { return (int64_t)nx * ny * nz; }
   int64_t NS() const { return N() * S; }
   size_t elem() const { return precision == BFVM_FP64 ? sizeof(double) : sizeof(float); }
@@ -164,12 +184,18 @@ void check_launch(bfvm_solver* m) {
 }
 
 // Chunk length CH (points per thread) and block width TW (columns per block)
-// per axis; a block is TW x NC threads with NC = ceil(n/CH) <= 512/TW.
+// per axis; a block is TW x NC threads with NC = ceil(n/CH) <= 512/TW.  The y
+// and z sweeps of long lines take CH = 32 (fewer chunks to join per line), x
+// keeps CH = 16 for its register kernel.
 void choose_axes(bfvm_solver* m) {
   const int ns[3] = {m->nx, m->ny, m->nz};
   for (int a = 0; a < 3; ++a) {
     const int n = ns[a];
+    if (m->axis[a].user && (n + m->axis[a].ch - 1) / m->axis[a].ch * m->axis[a].tw <= 512)
+      continue;
+    m->axis[a].user = false;
     int ch = (n <= 64) ? 8 : 16;
+    if (a > 0 && n >= 128) ch = 32;
     while ((n + ch - 1) / ch > 16 && ch < 32) ch *= 2;
     int tw = 32;
     if ((n + ch - 1) / ch > 16) tw = 16;
@@ -195,11 +221,15 @@ void clear_state_after_resize(bfvm_solver* m) {
   m->ag_t1.clear();
   m->ag_t2.clear();
   m->ag_dirty = true;
+  for (auto& A : m->axis) A.user = false;
   choose_axes(m);
 }
 
 // ---- Thomas coefficients ---------------------------------------------------
 
+// The reference shares one set of Thomas coefficients between its 3-D and
+// 2-D LOD solvers (diffusion_solver_setup_done): whichever runs first fixes
+// them.
 void thomas_setup(bfvm_solver* m, double dt) {
   const int ns[3] = {m->nx, m->ny, m->nz};
   for (int a = 0; a < 3; ++a) {
@@ -207,7 +237,7 @@ void thomas_setup(bfvm_solver* m, double dt) {
     std::vector<double> c1(S), den((size_t)n * S), cx((size_t)n * S);
     // The reference uses mesh.dx for every axis (BioFVM_solvers.cpp:112-113).
     bfvm::thomas_axis(n, S, m->dx, dt, m->D.data(), m->decay.data(), c1.data(), den.data(),
-                      cx.data());
+                      cx.data(), m->lod_dims);
     std::vector<double> tab((size_t)3 * n * S + S);
     for (size_t i = 0; i < (size_t)n * S; ++i) {
       const int s = (int)(i % S);
@@ -222,8 +252,93 @@ void thomas_setup(bfvm_solver* m, double dt) {
       std::vector<float> tf(tab.begin(), tab.end());
       upload(m->coef[a], tf, m->stream);
     }
+    m->h_c1[a] = c1;
+    m->h_den[a] = den;
+    m->h_cx[a] = cx;
+    m->chunk_ch[a] = 0;
   }
   m->setup_done = true;
+}
+
+// Chunk tables of one axis for its current chunk length (rebuilt when the
+// chunk length or the Thomas coefficients change).  Chunks whose tables are
+// bit-identical share one slot: away from the two line ends the Thomas
+// denominators converge to a fixed point, so most interior chunks of a long
+// line are the same and the tables the kernels read stay small enough for L1.
+template <typename T>
+bfvm::ChunkCoef<T> chunk_view(bfvm_solver* m, int a) {
+  const int ns[3] = {m->nx, m->ny, m->nz};
+  const int n = ns[a], S = m->S, ch = m->axis[a].ch;
+  const int nc = (n + ch - 1) / ch;
+  auto up4 = [](size_t x) { return (x + 3) & ~(size_t)3; };
+  if (m->chunk_ch[a] != ch) {
+    const size_t fk = (size_t)S * n * 2;
+    std::vector<double> k1((size_t)nc * ch * S * 2, 0.0), kg((size_t)nc * ch * S * 2, 0.0),
+        kc((size_t)nc * S * 4);
+    bfvm::chunk_tables(n, S, ch, m->h_c1[a].data(), m->h_den[a].data(), m->h_cx[a].data(),
+                       k1.data(), kg.data(), kc.data());
+    (void)fk;
+    // slot per chunk: the first earlier full-length chunk with identical tables
+    const size_t cw = (size_t)ch * S * 2;  // elements of one chunk in k1 / kg
+    std::vector<int> slot_of(nc);
+    std::vector<int> slot_chunk;  // representative chunk of each slot
+    for (int c = 0; c < nc; ++c) {
+      const bool full = (c + 1) * ch <= n;
+      int found = -1;
+      if (full) {
+        for (size_t sl = 0; sl < slot_chunk.size() && found < 0; ++sl) {
+          const int r = slot_chunk[sl];
+          if ((r + 1) * ch > n) continue;
+          if (std::memcmp(&k1[r * cw], &k1[c * cw], cw * sizeof(double)) == 0 &&
+              std::memcmp(&kg[r * cw], &kg[c * cw], cw * sizeof(double)) == 0 &&
+              std::memcmp(&kc[(size_t)r * S * 4], &kc[(size_t)c * S * 4],
+                          (size_t)S * 4 * sizeof(double)) == 0)
+            found = (int)sl;
+        }
+      }
+      if (found < 0) {
+        found = (int)slot_chunk.size();
+        slot_chunk.push_back(c);
+      }
+      slot_of[c] = found;
+    }
+    const size_t ns_ = slot_chunk.size();
+    const size_t k1n = up4(ns_ * cw), kgn = up4(ns_ * cw), kcn = up4((size_t)nc * S * 4);
+    std::vector<double> tab(k1n + kgn + kcn, 0.0);
+    for (size_t sl = 0; sl < ns_; ++sl) {
+      const int r = slot_chunk[sl];
+      std::copy_n(&k1[r * cw], cw, &tab[sl * cw]);
+      std::copy_n(&kg[r * cw], cw, &tab[k1n + sl * cw]);
+    }
+    // transfer constants per chunk (not per slot): the fold reads every chunk
+    std::copy_n(kc.data(), (size_t)nc * S * 4, &tab[k1n + kgn]);
+    if (sizeof(T) == sizeof(double)) {
+      upload(m->chunk[a], tab, m->stream);
+    } else {
+      std::vector<float> tf(tab.begin(), tab.end());
+      upload(m->chunk[a], tf, m->stream);
+    }
+    upload(m->chunk_slots[a], slot_of, m->stream);
+    m->chunk_ch[a] = ch;
+    m->chunk_nslots[a] = (int)ns_;
+  }
+  const size_t cw = (size_t)ch * S * 2;
+  const size_t ns_ = (size_t)m->chunk_nslots[a];
+  const size_t k1n = up4(ns_ * cw), kgn = up4(ns_ * cw);
+  const T* base = m->chunk[a].as<T>();
+  bfvm::ChunkCoef<T> c;
+  c.k1 = base;
+  c.kg = base + k1n;
+  c.kc = base + k1n + kgn;
+  c.slot = m->chunk_slots[a].as<int>();
+  c.ch = ch;
+  c.nc = nc;
+  c.tab_elems = (int)(k1n + kgn + up4((size_t)nc * S * 4));
+  const T* vec_sections[3] = {c.k1, c.kg, c.kc};
+  for (const T* q : vec_sections)
+    require(reinterpret_cast<uintptr_t>(q) % (2 * sizeof(T)) == 0,
+            "chunk table not aligned for vector loads", BFVM_ERR_STATE);
+  return c;
 }
 
 template <typename T>
@@ -374,6 +489,7 @@ void build_agents(bfvm_solver* m) {
   }
   gstart.push_back((int)A);
   m->n_groups = (int64_t)gvox.size();
+
   const int ch = m->axis[0].ch, nc = (m->nx + ch - 1) / ch;
   upload(m->seg_cells.off, segment_offsets((int64_t)m->ny * m->nz, nc, ch, line, pos), st);
   upload(m->seg_cells.pos, pos, st);
@@ -394,15 +510,24 @@ void build_all(bfvm_solver* m) {
 
 // ---- launches ---------------------------------------------------------------
 
-template <typename T, int CH>
-void launch_sweep_ch(const bfvm::SweepArgs<T>& a, int mode, dim3 grid, dim3 block, size_t smem,
+template <typename T, int CH, int MINB>
+void launch_sweep_mb(const bfvm::SweepArgs<T>& a, int mode, dim3 grid, dim3 block, size_t smem,
                      cudaStream_t st) {
   if (mode == bfvm::kSweepFull)
-    bfvm::lod_sweep_kernel<T, CH, bfvm::kSweepFull><<<grid, block, smem, st>>>(a);
+    bfvm::lod_sweep_kernel<T, CH, bfvm::kSweepFull, MINB><<<grid, block, smem, st>>>(a);
   else if (mode == bfvm::kSweepDirEpi)
-    bfvm::lod_sweep_kernel<T, CH, bfvm::kSweepDirEpi><<<grid, block, smem, st>>>(a);
+    bfvm::lod_sweep_kernel<T, CH, bfvm::kSweepDirEpi, MINB><<<grid, block, smem, st>>>(a);
   else
-    bfvm::lod_sweep_kernel<T, CH, bfvm::kSweepPlain><<<grid, block, smem, st>>>(a);
+    bfvm::lod_sweep_kernel<T, CH, bfvm::kSweepPlain, MINB><<<grid, block, smem, st>>>(a);
+}
+
+template <typename T, int CH>
+void launch_sweep_ch(const bfvm::SweepArgs<T>& a, int mode, int minb, dim3 grid, dim3 block,
+                     size_t smem, cudaStream_t st) {
+  if (minb == 2)
+    launch_sweep_mb<T, CH, 2>(a, mode, grid, block, smem, st);
+  else
+    launch_sweep_mb<T, CH, 1>(a, mode, grid, block, smem, st);
 }
 
 template <typename T>
@@ -414,18 +539,19 @@ void launch_sweep(bfvm_solver* m, int ax, int fuse, double dt) {
   a.S = S;
   a.dt = dt;
   a.coef = coef_view<T>(m, ax);
+  const int64_t nzp = (m->lod_dims == 2) ? 1 : nz;  // planes swept
   if (ax == 0) {
     a.n = (int)nx;
     a.C = S;
     a.outer_stride = nx * S;
     a.line_stride = S;
-    a.ncols = ny * nz * S;
+    a.ncols = ny * nzp * S;
   } else if (ax == 1) {
     a.n = (int)ny;
     a.C = nx * S;
     a.outer_stride = nx * ny * S;
     a.line_stride = nx * S;
-    a.ncols = nz * nx * S;
+    a.ncols = nzp * nx * S;
   } else {
     a.n = (int)nz;
     a.C = nx * ny * S;
@@ -453,19 +579,433 @@ void launch_sweep(bfvm_solver* m, int ax, int fuse, double dt) {
   else if (fuse & bfvm::kFuseDirEpi)
     mode = bfvm::kSweepDirEpi;
   switch (A.ch) {
-    case 8: launch_sweep_ch<T, 8>(a, mode, grid, block, smem, m->stream); break;
-    case 16: launch_sweep_ch<T, 16>(a, mode, grid, block, smem, m->stream); break;
-    case 32: launch_sweep_ch<T, 32>(a, mode, grid, block, smem, m->stream); break;
+    case 8: launch_sweep_ch<T, 8>(a, mode, A.minb, grid, block, smem, m->stream); break;
+    case 16: launch_sweep_ch<T, 16>(a, mode, A.minb, grid, block, smem, m->stream); break;
+    case 32: launch_sweep_ch<T, 32>(a, mode, A.minb, grid, block, smem, m->stream); break;
     default: throw Error(BFVM_ERR_STATE, "unsupported chunk length");
   }
   check_launch(m);
 }
 
+// ---- TMA-fed persistent sweeps ---------------------------------------------
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* ptr = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    BFVM_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q));
+    require(q == cudaDriverEntryPointSuccess && ptr != nullptr,
+            "cuTensorMapEncodeTiled is not available from the driver", BFVM_ERR_CUDA);
+    fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(ptr);
+  }
+  return fn;
+}
+
+// Raises the dynamic shared-memory limit of a kernel once per device.
+void allow_smem(const void* kernel, int device, size_t bytes) {
+  static std::unordered_map<const void*, uint64_t> done;  // kernel -> device bitmask
+  uint64_t& mask = done[kernel];
+  if (mask & (1ull << device)) return;
+  BFVM_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 227 * 1024));
+  mask |= 1ull << device;
+  (void)bytes;
+}
+
+constexpr size_t kSmemBudget = 224 * 1024;  // of the 227 KB a block may use
+
+// Shared-memory bytes of an axis's chunk tables plus slot map (for staging
+// them per block); 0 if the tables are not built yet.
+size_t table_bytes(const bfvm_solver* m, int a) {
+  if (m->chunk_ch[a] != m->axis[a].ch || m->chunk_nslots[a] == 0) return 0;
+  auto up4 = [](size_t x) { return (x + 3) & ~(size_t)3; };
+  const int ns[3] = {m->nx, m->ny, m->nz};
+  const size_t ch = m->axis[a].ch, S = m->S, nsl = m->chunk_nslots[a];
+  const size_t nc = (ns[a] + ch - 1) / ch;
+  const size_t elems = up4(nsl * ch * S * 2) * 2 + up4(nc * S * 4);
+  return elems * m->elem() + nc * sizeof(int) + 16;
+}
+
+struct LinesPlan {
+  bool ok = false;
+  bool smem_tab = false;
+  int n = 0, ch = 0, nc = 0, w = 0, stages = 0, box_n = 0, nboxes = 0;
+  int64_t C = 0, nouter = 0, ls = 0, os = 0;
+  size_t smem = 0;
+};
+
+// y (ax = 1) or z (ax = 2) sweep as a 3-D tensor [outer][n][C].  Tiles are
+// 16 columns wide in FP64 and 32 in FP32 (128-byte rows); the ring gets as
+// many stages as keep two blocks per SM, else one block with more stages.
+LinesPlan plan_lines(const bfvm_solver* m, int ax) {
+  LinesPlan L;
+  const int64_t es = (int64_t)m->elem();
+  const int64_t nx = m->nx, ny = m->ny, nz = m->nz, S = m->S;
+  if (ax == 1) {
+    L.n = (int)ny; L.C = nx * S; L.nouter = (m->lod_dims == 2) ? 1 : nz; L.ls = nx * S;
+    L.os = nx * ny * S;
+  } else {
+    L.n = (int)nz; L.C = nx * ny * S; L.nouter = 1; L.ls = nx * ny * S; L.os = nx * ny * nz * S;
+  }
+  if ((L.ls * es) % 16 || (L.os * es) % 16 || L.n > 1024 || L.C >= ((int64_t)1 << 31)) return L;
+  // the chunk length of the axis: the (line, chunk) segment lists are built with it
+  L.ch = m->axis[ax].ch;
+  L.nc = (L.n + L.ch - 1) / L.ch;
+  L.w = (es == 8) ? 16 : 32;
+  if (L.nc > 16) return L;
+  L.box_n = std::min(L.n, 256);
+  L.nboxes = (L.n + L.box_n - 1) / L.box_n;
+  const int64_t ctiles = (L.C + L.w - 1) / L.w;
+  if (ctiles * L.nouter >= ((int64_t)1 << 31)) return L;
+  const size_t stage = (size_t)L.box_n * L.nboxes * L.w * es;
+  const size_t fold = 4 * (size_t)L.nc * L.w * es;  // two parities of (qe, x0) pairs
+  const size_t extra = 8 * 4 + 128;
+  const size_t tab = table_bytes(m, ax);
+  // preferred: the chunk tables staged in shared memory, two blocks per SM
+  // (about 113 KB each); else one block; else tables read through L1.
+  auto stages_for = [&](size_t budget, size_t t) -> int {
+    return budget > fold + extra + t ? (int)std::min<size_t>(4, (budget - fold - extra - t) / stage)
+                                     : 0;
+  };
+  L.smem_tab = tab > 0;
+  L.stages = L.smem_tab ? stages_for(113 * 1024, tab) : 0;
+  if (L.stages < 2 && L.smem_tab) L.stages = stages_for(kSmemBudget, tab);
+  if (L.stages < 2) {
+    L.smem_tab = false;
+    L.stages = stages_for(80 * 1024, 0);
+    if (L.stages < 2) L.stages = stages_for(kSmemBudget, 0);
+    if (L.stages < 2) return L;
+  }
+  L.smem = L.stages * stage + fold + extra + (L.smem_tab ? tab : 0);
+  L.ok = true;
+  return L;
+}
+
+struct RowsPlan {
+  bool ok = false;
+  bool smem_tab = false;
+  int ch = 0, nc = 0, R = 0, stages = 0;
+  int64_t pitch = 0;
+  size_t smem = 0;
+};
+
+// x sweep: tiles of R whole rows, one block per SM of R*S*NC <= 512 threads.
+// Rows sit in shared memory at a padded pitch (16-byte multiple, = S modulo
+// 16 elements where possible) so the column-major thread mapping is free of
+// bank conflicts.
+RowsPlan plan_rows(const bfvm_solver* m) {
+  RowsPlan P;
+  const int64_t es = (int64_t)m->elem();
+  const int64_t row_elems = (int64_t)m->nx * m->S;
+  const int64_t row_bytes = row_elems * es;
+  const int64_t rows = (int64_t)m->ny * (m->lod_dims == 2 ? 1 : m->nz);
+  if (row_bytes % 16 || m->nx > 1024) return P;
+  P.ch = m->axis[0].ch;
+  P.nc = (m->nx + P.ch - 1) / P.ch;
+  const int cols = m->S * P.nc;
+  if (cols > 512) return P;
+  P.R = (int)std::min<int64_t>(std::max(1, 512 / cols), rows);
+  // pitch: row_elems rounded up so that pitch == S (mod 16 elements of 8 B,
+  // 32 of 4 B) and pitch*es is a multiple of 16 bytes
+  const int64_t mod = (es == 8) ? 16 : 32, step = 16 / es;
+  int64_t pitch = row_elems;
+  for (int64_t k = 0; k < mod; k += step) {
+    if (((row_elems + k) - m->S) % mod == 0) {
+      pitch = row_elems + k;
+      break;
+    }
+  }
+  if (pitch == row_elems && (row_elems - m->S) % mod != 0)
+    pitch = (row_elems + step - 1) / step * step;
+  P.pitch = pitch;
+  const size_t extra = 8 * 4 + 16 + 128;
+  const size_t tab = table_bytes(m, 0);
+  // largest R whose ring (>= 3 stages) fits with the chunk tables staged in
+  // shared memory; else the largest without staging them
+  const int rmax = P.R;
+  for (int staged = 1; staged >= 0; --staged) {
+    if (staged && tab == 0) continue;
+    for (P.R = rmax; P.R >= 1; --P.R) {
+      const size_t stage = (size_t)(P.R * pitch * es);
+      const size_t fold = 4 * (size_t)P.nc * P.R * m->S * es;  // two parities of (qe, x0)
+      const size_t t = staged ? tab : 0;
+      if (kSmemBudget <= fold + extra + t) continue;
+      P.stages = (int)std::min<size_t>(4, (kSmemBudget - fold - extra - t) / stage);
+      if (P.stages >= 3) {
+        P.smem_tab = staged != 0;
+        P.smem = P.stages * stage + fold + extra + t;
+        P.ok = true;
+        return P;
+      }
+    }
+  }
+  return P;
+}
+
+template <typename T, int CH, int ST, bool DIR, bool TAB>
+void launch_lines_inst(const CUtensorMap& map, const bfvm::LinesArgs<T>& a, int ntiles,
+                       dim3 block, size_t smem, bfvm_solver* m) {
+  constexpr int W = sizeof(T) == 8 ? 16 : 32;
+  auto k = bfvm::lod_lines_tma_kernel<T, CH, W, ST, DIR, TAB>;
+  allow_smem((const void*)k, m->device, smem);
+  int per_sm = 0;
+  BFVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, block.x * block.y, smem));
+  require(per_sm > 0, "sweep kernel does not fit on an SM", BFVM_ERR_STATE);
+  dim3 grid((unsigned)std::min<int64_t>(ntiles, (int64_t)per_sm * m->num_sms));
+  k<<<grid, block, smem, m->stream>>>(map, a);
+}
+
+template <typename T, int CH, int ST, bool TAB>
+void launch_lines_dir(const CUtensorMap& map, const bfvm::LinesArgs<T>& a, bool dir, int ntiles,
+                      dim3 block, size_t smem, bfvm_solver* m) {
+  if (dir)
+    launch_lines_inst<T, CH, ST, true, TAB>(map, a, ntiles, block, smem, m);
+  else
+    launch_lines_inst<T, CH, ST, false, TAB>(map, a, ntiles, block, smem, m);
+}
+
+template <typename T, int CH, int ST>
+void launch_lines_tab(const CUtensorMap& map, const bfvm::LinesArgs<T>& a, bool dir, bool tab,
+                      int ntiles, dim3 block, size_t smem, bfvm_solver* m) {
+  if (tab)
+    launch_lines_dir<T, CH, ST, true>(map, a, dir, ntiles, block, smem, m);
+  else
+    launch_lines_dir<T, CH, ST, false>(map, a, dir, ntiles, block, smem, m);
+}
+
+template <typename T, int CH>
+void launch_lines_st(const CUtensorMap& map, const bfvm::LinesArgs<T>& a, int stages, bool dir,
+                     bool tab, int ntiles, dim3 block, size_t smem, bfvm_solver* m) {
+  switch (stages) {
+    case 2: launch_lines_tab<T, CH, 2>(map, a, dir, tab, ntiles, block, smem, m); break;
+    case 3: launch_lines_tab<T, CH, 3>(map, a, dir, tab, ntiles, block, smem, m); break;
+    default: launch_lines_tab<T, CH, 4>(map, a, dir, tab, ntiles, block, smem, m); break;
+  }
+}
+
+template <typename T>
+void launch_lines(bfvm_solver* m, int ax, const LinesPlan& L, bool dir) {
+  // (re)encode the tensor map when the field moved
+  if (m->map_key[ax] != m->p.ptr || m->map_w[ax] != L.w) {
+    const int64_t es = (int64_t)sizeof(T);
+    cuuint64_t dims[3] = {(cuuint64_t)L.C, (cuuint64_t)L.n, (cuuint64_t)L.nouter};
+    cuuint64_t strides[2] = {(cuuint64_t)(L.ls * es), (cuuint64_t)(L.os * es)};
+    cuuint32_t box[3] = {(cuuint32_t)L.w, (cuuint32_t)L.box_n, 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = tensor_map_encoder()(
+        &m->maps[ax], sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+        3, m->p.ptr, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    require(r == CUDA_SUCCESS, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")",
+            BFVM_ERR_CUDA);
+    m->map_key[ax] = m->p.ptr;
+    m->map_w[ax] = L.w;
+  }
+  bfvm::LinesArgs<T> a{};
+  a.p = m->p.as<T>();
+  a.C = L.C;
+  a.n = L.n;
+  a.ls = L.ls;
+  a.os = L.os;
+  a.S = m->S;
+  a.ctiles = (uint32_t)((L.C + L.w - 1) / L.w);
+  a.ntiles = (uint32_t)(a.ctiles * L.nouter);
+  a.box_n = L.box_n;
+  a.nboxes = L.nboxes;
+  a.nchunks = L.nc;
+  a.cc = chunk_view<T>(m, ax);
+  a.status = m->d_status.as<int>();
+  if (dir) a.dir_epi = m->seg_dir_y.view();
+  dim3 block(L.w, L.nc);
+  switch (L.ch) {
+    case 8: launch_lines_st<T, 8>(m->maps[ax], a, L.stages, dir, L.smem_tab, a.ntiles, block, L.smem, m); break;
+    case 16: launch_lines_st<T, 16>(m->maps[ax], a, L.stages, dir, L.smem_tab, a.ntiles, block, L.smem, m); break;
+    default: launch_lines_st<T, 32>(m->maps[ax], a, L.stages, dir, L.smem_tab, a.ntiles, block, L.smem, m); break;
+  }
+  check_launch(m);
+}
+
+template <typename T, int CH, int MODE>
+void launch_direct_inst(const bfvm::DirectArgs<T>& a, dim3 grid, dim3 block, bfvm_solver* m) {
+  constexpr int W = 32;
+  auto k = bfvm::lod_sweep_direct_kernel<T, CH, W, MODE>;
+  // fold pairs + per-chunk constants + slot map
+  const size_t smem = sizeof(T) * 2 * block.x * block.y + sizeof(T) * 4 * block.y * a.S +
+                      sizeof(int) * block.y + 16;
+  k<<<grid, block, smem, m->stream>>>(a);
+}
+
+template <typename T, int CH>
+void launch_direct_mode(const bfvm::DirectArgs<T>& a, int mode, dim3 grid, dim3 block,
+                        bfvm_solver* m) {
+  if (mode == bfvm::kSweepFull)
+    launch_direct_inst<T, CH, bfvm::kSweepFull>(a, grid, block, m);
+  else if (mode == bfvm::kSweepDirEpi)
+    launch_direct_inst<T, CH, bfvm::kSweepDirEpi>(a, grid, block, m);
+  else
+    launch_direct_inst<T, CH, bfvm::kSweepPlain>(a, grid, block, m);
+}
+
+// Any axis with direct loads: blocks of 32 columns x all chunks of a line.
+template <typename T>
+bool launch_direct(bfvm_solver* m, int ax, int fuse, double dt) {
+  const int64_t nx = m->nx, ny = m->ny, nz = m->nz, S = m->S;
+  bfvm::DirectArgs<T> a{};
+  const int64_t nzp = (m->lod_dims == 2) ? 1 : nz;  // planes swept
+  if (ax == 0) {
+    a.n = (int)nx; a.C = S; a.outer_stride = nx * S; a.line_stride = S; a.ncols = ny * nzp * S;
+  } else if (ax == 1) {
+    a.n = (int)ny; a.C = nx * S; a.outer_stride = nx * ny * S; a.line_stride = nx * S;
+    a.ncols = nzp * nx * S;
+  } else {
+    a.n = (int)nz; a.C = nx * ny * S; a.outer_stride = 0; a.line_stride = nx * ny * S;
+    a.ncols = nx * ny * S;
+  }
+  const int ch = m->axis[ax].ch;
+  const int nc = (a.n + ch - 1) / ch;
+  constexpr int W = 32;
+  const int64_t nblocks = (a.ncols + W - 1) / W;
+  if (W * nc > 512 || nblocks >= ((int64_t)1 << 31)) return false;
+  a.p = m->p.as<T>();
+  a.S = (int)S;
+  a.nchunks = nc;
+  a.cc = chunk_view<T>(m, ax);
+  a.dt = dt;
+  if ((fuse & bfvm::kFuseBulk) && !m->seg_bulk.present) fuse &= ~bfvm::kFuseBulk;
+  if ((fuse & bfvm::kFuseCells) && !m->seg_cells.present) fuse &= ~bfvm::kFuseCells;
+  const DevSegList& dseg = (ax == 0) ? m->seg_dir_x : m->seg_dir_y;
+  if (!dseg.present || ax == 2) fuse &= ~(bfvm::kFuseDirPro | bfvm::kFuseDirEpi);
+  a.fuse = fuse;
+  a.bulk = m->seg_bulk.view();
+  a.cells = m->seg_cells.view();
+  a.dir_pro = dseg.view();
+  a.dir_epi = dseg.view();
+  int mode = bfvm::kSweepPlain;
+  if (fuse & (bfvm::kFuseBulk | bfvm::kFuseCells | bfvm::kFuseDirPro))
+    mode = bfvm::kSweepFull;
+  else if (fuse & bfvm::kFuseDirEpi)
+    mode = bfvm::kSweepDirEpi;
+  dim3 block(W, nc);
+  dim3 grid((unsigned)nblocks);
+  switch (ch) {
+    case 8: launch_direct_mode<T, 8>(a, mode, grid, block, m); break;
+    case 16: launch_direct_mode<T, 16>(a, mode, grid, block, m); break;
+    default: launch_direct_mode<T, 32>(a, mode, grid, block, m); break;
+  }
+  check_launch(m);
+  return true;
+}
+
+template <typename T, int CH, int ST, bool TAB>
+void launch_rows_inst(const bfvm::RowsArgs<T>& a, dim3 block, size_t smem, bfvm_solver* m) {
+  auto k = bfvm::lod_rows_tma_kernel<T, CH, ST, TAB>;
+  allow_smem((const void*)k, m->device, smem);
+  int per_sm = 0;
+  BFVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, block.x * block.y, smem));
+  require(per_sm > 0, "sweep kernel does not fit on an SM", BFVM_ERR_STATE);
+  dim3 grid((unsigned)std::min<int64_t>(a.ntiles, (int64_t)per_sm * m->num_sms));
+  k<<<grid, block, smem, m->stream>>>(a);
+}
+
+template <typename T>
+void launch_rows(bfvm_solver* m, const RowsPlan& P, int fuse, double dt) {
+  bfvm::RowsArgs<T> a{};
+  a.p = m->p.as<T>();
+  a.rows = (int64_t)m->ny * (m->lod_dims == 2 ? 1 : m->nz);
+  a.n = m->nx;
+  a.S = m->S;
+  a.ntiles = (a.rows + P.R - 1) / P.R;
+  a.nchunks = P.nc;
+  a.R = P.R;
+  a.pitch = P.pitch;
+  a.cc = chunk_view<T>(m, 0);
+  a.dt = dt;
+  if ((fuse & bfvm::kFuseBulk) && !m->seg_bulk.present) fuse &= ~bfvm::kFuseBulk;
+  if ((fuse & bfvm::kFuseCells) && !m->seg_cells.present) fuse &= ~bfvm::kFuseCells;
+  if (!m->seg_dir_x.present) fuse &= ~(bfvm::kFuseDirPro | bfvm::kFuseDirEpi);
+  a.fuse = fuse;
+  a.bulk = m->seg_bulk.view();
+  a.cells = m->seg_cells.view();
+  a.dir = m->seg_dir_x.view();
+  a.status = m->d_status.as<int>();
+  // whole warps: threads past R*S*NC idle through the sweep
+  dim3 block((unsigned)((P.R * m->S * P.nc + 31) / 32 * 32));
+  const int key = (P.smem_tab ? 1000 : 0) + P.ch * 10 + P.stages;
+  switch (key) {
+    case 83: launch_rows_inst<T, 8, 3, false>(a, block, P.smem, m); break;
+    case 84: launch_rows_inst<T, 8, 4, false>(a, block, P.smem, m); break;
+    case 163: launch_rows_inst<T, 16, 3, false>(a, block, P.smem, m); break;
+    case 164: launch_rows_inst<T, 16, 4, false>(a, block, P.smem, m); break;
+    case 323: launch_rows_inst<T, 32, 3, false>(a, block, P.smem, m); break;
+    case 324: launch_rows_inst<T, 32, 4, false>(a, block, P.smem, m); break;
+    case 1083: launch_rows_inst<T, 8, 3, true>(a, block, P.smem, m); break;
+    case 1084: launch_rows_inst<T, 8, 4, true>(a, block, P.smem, m); break;
+    case 1163: launch_rows_inst<T, 16, 3, true>(a, block, P.smem, m); break;
+    case 1164: launch_rows_inst<T, 16, 4, true>(a, block, P.smem, m); break;
+    case 1323: launch_rows_inst<T, 32, 3, true>(a, block, P.smem, m); break;
+    default: launch_rows_inst<T, 32, 4, true>(a, block, P.smem, m); break;
+  }
+  check_launch(m);
+}
+
 void sweep(bfvm_solver* m, int ax, int fuse, double dt) {
-  if (m->precision == BFVM_FP64)
+  const bool fp64 = m->precision == BFVM_FP64;
+  const int path = m->path;
+  if (path != BFVM_PATH_GENERIC) {
+    // build the chunk tables first: the plans size shared memory from them
+    if (fp64)
+      chunk_view<double>(m, ax);
+    else
+      chunk_view<float>(m, ax);
+    // AUTO: the register kernel for x (measured fastest there), TMA tiles
+    // for y and z
+    if (path == BFVM_PATH_AUTO && ax == 0) {
+      if (fp64)
+        launch_sweep<double>(m, ax, fuse, dt);
+      else
+        launch_sweep<float>(m, ax, fuse, dt);
+      return;
+    }
+    const bool want_tma = (path == BFVM_PATH_TMA) || (path == BFVM_PATH_AUTO);
+    if (want_tma && ax == 0) {
+      const RowsPlan P = plan_rows(m);
+      if (P.ok) {
+        if (fp64)
+          launch_rows<double>(m, P, fuse, dt);
+        else
+          launch_rows<float>(m, P, fuse, dt);
+        return;
+      }
+    } else if (want_tma) {
+      const LinesPlan L = plan_lines(m, ax);
+      if (L.ok) {
+        const bool dir = (ax == 1) && (fuse & bfvm::kFuseDirEpi) && m->seg_dir_y.present;
+        if (fp64)
+          launch_lines<double>(m, ax, L, dir);
+        else
+          launch_lines<float>(m, ax, L, dir);
+        return;
+      }
+    }
+    if (fp64 ? launch_direct<double>(m, ax, fuse, dt) : launch_direct<float>(m, ax, fuse, dt))
+      return;
+  }
+  if (fp64)
     launch_sweep<double>(m, ax, fuse, dt);
   else
     launch_sweep<float>(m, ax, fuse, dt);
+}
+
+void check_status(bfvm_solver* m) {
+  int st = 0;
+  BFVM_CUDA(cudaMemcpyAsync(&st, m->d_status.ptr, sizeof(int), cudaMemcpyDeviceToHost, m->stream));
+  BFVM_CUDA(cudaStreamSynchronize(m->stream));
+  if (st != 0) {
+    BFVM_CUDA(cudaMemsetAsync(m->d_status.ptr, 0, sizeof(int), m->stream));
+    throw Error(BFVM_ERR_STATE, "a sweep kernel gave up waiting for its tile copies");
+  }
 }
 
 void check_lod_mesh(bfvm_solver* m) {
@@ -475,13 +1015,55 @@ void check_lod_mesh(bfvm_solver* m) {
           BFVM_ERR_MESH);
 }
 
-void diffusion(bfvm_solver* m, double dt, int fuse_x) {
+void bulk_any(bfvm_solver* m, double dt);
+void cells_any(bfvm_solver* m);
+
+// One step: bulk -> cells -> LOD_3D (BioFVM_solvers.cpp:175-273), the parts
+// selected by flags (diffusion always).  Bulk and cell updates run as their
+// own kernels over the sparse lists (they touch only the listed voxels) unless
+// fuse_sources folds them into the x sweep's prologue.  The Dirichlet
+// overwrites are fused into the sweeps.  ev (optional, 5 events) brackets
+// the source kernels, the x, y and z sweeps.
+void step_once(bfvm_solver* m, double dt, int flags, cudaEvent_t* ev) {
   check_lod_mesh(m);
   if (!m->setup_done) thomas_setup(m, dt);
   build_all(m);
-  sweep(m, 0, fuse_x | bfvm::kFuseDirPro | bfvm::kFuseDirEpi, dt);
+  if (ev) BFVM_CUDA(cudaEventRecord(ev[0], m->stream));
+  int fuse = 0;
+  if (m->fuse_sources) {
+    if (flags & BFVM_STEP_BULK) fuse |= bfvm::kFuseBulk;
+    if (flags & BFVM_STEP_CELLS) fuse |= bfvm::kFuseCells;
+  } else {
+    if (flags & BFVM_STEP_BULK) bulk_any(m, dt);
+    if (flags & BFVM_STEP_CELLS) cells_any(m);
+  }
+  if (ev) BFVM_CUDA(cudaEventRecord(ev[1], m->stream));
+  sweep(m, 0, fuse | bfvm::kFuseDirPro | bfvm::kFuseDirEpi, dt);
+  if (ev) BFVM_CUDA(cudaEventRecord(ev[2], m->stream));
   sweep(m, 1, bfvm::kFuseDirEpi, dt);
+  if (ev) BFVM_CUDA(cudaEventRecord(ev[3], m->stream));
   sweep(m, 2, 0, dt);
+  if (ev) BFVM_CUDA(cudaEventRecord(ev[4], m->stream));
+}
+
+void diffusion(bfvm_solver* m, double dt) { step_once(m, dt, BFVM_STEP_DIFFUSION, nullptr); }
+
+// diffusion_decay_solver__constant_coefficients_LOD_2D (BioFVM_solvers.cpp:278-427):
+// uniform mesh, Dirichlet then x-Thomas, Dirichlet then y-Thomas, on the
+// z = 0 plane.
+void diffusion_2d(bfvm_solver* m, double dt) {
+  require(m->uniform,
+          "Error: This algorithm is written for uniform Cartesian meshes. Try: something else.",
+          BFVM_ERR_MESH);
+  struct Restore {
+    bfvm_solver* m;
+    ~Restore() { m->lod_dims = 3; }
+  } restore{m};
+  m->lod_dims = 2;
+  if (!m->setup_done) thomas_setup(m, dt);
+  build_all(m);
+  sweep(m, 0, bfvm::kFuseDirPro | bfvm::kFuseDirEpi, dt);
+  sweep(m, 1, 0, dt);
 }
 
 template <typename T>
@@ -611,6 +1193,9 @@ int bfvm_create(bfvm_solver** out, int device) {
       delete m;
       throw Error(BFVM_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
     }
+    m->d_status.ensure(16);
+    BFVM_CUDA(cudaMemset(m->d_status.ptr, 0, 16));
+    BFVM_CUDA(cudaDeviceGetAttribute(&m->num_sms, cudaDevAttrMultiProcessorCount, device));
     // Microenvironment(): mesh.resize(1,1,1) (BioFVM_microenvironment.cpp:101)
     // = resize(-0.5, 0.5, ..., 1, 1, 1) (BioFVM_mesh.cpp:924-925), dx = 1.
     resize_common(m, 1, 1, 1);
@@ -638,6 +1223,9 @@ int bfvm_destroy(bfvm_solver* m) {
     m->d_group_start.release();
     m->d_gather.release();
     m->seg_cells.release();
+    m->d_status.release();
+    for (auto& c : m->chunk) c.release();
+    for (auto& c : m->chunk_slots) c.release();
     cudaStreamDestroy(m->stream);
     delete m;
   });
@@ -689,6 +1277,20 @@ int bfvm_resize_space_nodes(bfvm_solver* m, double x0, double x1, double y0, dou
     const double bb[6] = {x0, y0, z0, x1, y1, z1};
     std::copy(bb, bb + 6, m->bbox);
     resize_common(m, nx, ny, nz);
+  });
+}
+
+int bfvm_set_mesh(bfvm_solver* m, const int* nxyz, const double* geom, int uniform) {
+  return SOLVER_CALL(m, {
+    require(nxyz != nullptr && geom != nullptr, "null mesh description");
+    require(geom[0] > 0 && geom[1] > 0 && geom[2] > 0, "voxel spacing must be positive");
+    m->dx = geom[0];
+    m->dy = geom[1];
+    m->dz = geom[2];
+    m->dV = geom[0] * geom[1] * geom[2];
+    std::copy(geom + 4, geom + 10, m->bbox);
+    m->uniform = uniform != 0;
+    resize_common(m, nxyz[0], nxyz[1], nxyz[2]);
   });
 }
 
@@ -807,6 +1409,7 @@ int bfvm_set_densities(bfvm_solver* m, const double* host) {
 int bfvm_get_densities(bfvm_solver* m, double* host) {
   return SOLVER_CALL(m, {
     require(host != nullptr, "null host buffer");
+    check_status(m);
     const size_t NS = (size_t)m->NS();
     if (m->precision == BFVM_FP64) {
       BFVM_CUDA(cudaMemcpyAsync(host, m->p.ptr, NS * sizeof(double), cudaMemcpyDeviceToHost,
@@ -1036,7 +1639,11 @@ int bfvm_simulate_cell_sources_and_sinks(bfvm_solver* m, double dt) {
 }
 
 int bfvm_simulate_diffusion_decay(bfvm_solver* m, double dt) {
-  return SOLVER_CALL(m, diffusion(m, dt, 0));
+  return SOLVER_CALL(m, diffusion(m, dt));
+}
+
+int bfvm_simulate_diffusion_decay_2d(bfvm_solver* m, double dt) {
+  return SOLVER_CALL(m, diffusion_2d(m, dt));
 }
 
 int bfvm_apply_dirichlet_conditions(bfvm_solver* m) {
@@ -1063,10 +1670,7 @@ int bfvm_step(bfvm_solver* m, double dt, int nsteps, int flags) {
       }
       return;
     }
-    int fuse = 0;
-    if (flags & BFVM_STEP_BULK) fuse |= bfvm::kFuseBulk;
-    if (flags & BFVM_STEP_CELLS) fuse |= bfvm::kFuseCells;
-    for (int it = 0; it < nsteps; ++it) diffusion(m, dt, fuse);
+    for (int it = 0; it < nsteps; ++it) step_once(m, dt, flags, nullptr);
   });
 }
 
@@ -1102,8 +1706,50 @@ int bfvm_set_precision(bfvm_solver* m, int precision) {
   });
 }
 
+int bfvm_set_sweep_config(bfvm_solver* m, int axis, int chunk, int columns, int min_blocks) {
+  return SOLVER_CALL(m, {
+    require(axis >= 0 && axis < 3, "axis must be 0, 1 or 2");
+    require(chunk == 8 || chunk == 16 || chunk == 32, "chunk must be 8, 16 or 32");
+    require(columns == 8 || columns == 16 || columns == 32 || columns == 64,
+            "columns must be 8, 16, 32 or 64");
+    require(min_blocks == 1 || min_blocks == 2, "min_blocks must be 1 or 2");
+    const int ns[3] = {m->nx, m->ny, m->nz};
+    const int nc = (ns[axis] + chunk - 1) / chunk;
+    require(nc * columns <= 512, "chunks x columns exceeds 512 threads per block");
+    Axis& A = m->axis[axis];
+    if (A.ch != chunk) m->bulk_dirty = m->dir_dirty = m->ag_dirty = true;
+    A.ch = chunk;
+    A.tw = columns;
+    A.minb = min_blocks;
+    A.user = true;
+  });
+}
+
+int bfvm_get_sweep_config(bfvm_solver* m, int axis, int* config) {
+  return SOLVER_CALL(m, {
+    require(axis >= 0 && axis < 3 && config != nullptr, "bad arguments");
+    config[0] = m->axis[axis].ch;
+    config[1] = m->axis[axis].tw;
+    config[2] = m->axis[axis].minb;
+  });
+}
+
 int bfvm_synchronize(bfvm_solver* m) {
-  return SOLVER_CALL(m, BFVM_CUDA(cudaStreamSynchronize(m->stream)));
+  return SOLVER_CALL(m, {
+    BFVM_CUDA(cudaStreamSynchronize(m->stream));
+    check_status(m);
+  });
+}
+
+int bfvm_set_fuse_sources(bfvm_solver* m, int fuse) {
+  return SOLVER_CALL(m, { m->fuse_sources = fuse ? 1 : 0; });
+}
+
+int bfvm_set_kernel_path(bfvm_solver* m, int path) {
+  return SOLVER_CALL(m, {
+    require(path >= BFVM_PATH_AUTO && path <= BFVM_PATH_DIRECT, "unknown kernel path");
+    m->path = path;
+  });
 }
 
 int bfvm_get_stream(bfvm_solver* m, void** stream) {
@@ -1124,32 +1770,21 @@ int bfvm_profile_step(bfvm_solver* m, double dt, int nsteps, int flags, double* 
   return SOLVER_CALL(m, {
     require(ms != nullptr && nsteps > 0, "bad arguments");
     require(flags & BFVM_STEP_DIFFUSION, "profiling needs the diffusion sweeps");
-    check_lod_mesh(m);
-    if (!m->setup_done) thomas_setup(m, dt);
-    build_all(m);
-    int fuse = 0;
-    if (flags & BFVM_STEP_BULK) fuse |= bfvm::kFuseBulk;
-    if (flags & BFVM_STEP_CELLS) fuse |= bfvm::kFuseCells;
-    cudaEvent_t ev[4];
+    cudaEvent_t ev[5];
     for (auto& e : ev) BFVM_CUDA(cudaEventCreate(&e));
-    double acc[3] = {0, 0, 0};
+    double acc[4] = {0, 0, 0, 0};
     for (int it = 0; it < nsteps; ++it) {
-      BFVM_CUDA(cudaEventRecord(ev[0], m->stream));
-      sweep(m, 0, fuse | bfvm::kFuseDirPro | bfvm::kFuseDirEpi, dt);
-      BFVM_CUDA(cudaEventRecord(ev[1], m->stream));
-      sweep(m, 1, bfvm::kFuseDirEpi, dt);
-      BFVM_CUDA(cudaEventRecord(ev[2], m->stream));
-      sweep(m, 2, 0, dt);
-      BFVM_CUDA(cudaEventRecord(ev[3], m->stream));
-      BFVM_CUDA(cudaEventSynchronize(ev[3]));
-      for (int a = 0; a < 3; ++a) {
+      step_once(m, dt, flags, ev);
+      BFVM_CUDA(cudaEventSynchronize(ev[4]));
+      for (int a = 0; a < 4; ++a) {
         float t = 0;
         BFVM_CUDA(cudaEventElapsedTime(&t, ev[a], ev[a + 1]));
         acc[a] += t;
       }
     }
-    for (int a = 0; a < 3; ++a) ms[a] = acc[a] / nsteps;
+    for (int a = 0; a < 4; ++a) ms[a] = acc[a] / nsteps;
     for (auto& e : ev) cudaEventDestroy(e);
+    check_status(m);
   });
 }
 

@@ -172,6 +172,9 @@ class Solver:
     def simulate_diffusion_decay(self, dt: float) -> None:
         call("bfvm_simulate_diffusion_decay", self._h, dt)
 
+    def simulate_diffusion_decay_2d(self, dt: float) -> None:
+        call("bfvm_simulate_diffusion_decay_2d", self._h, dt)
+
     def apply_dirichlet_conditions(self) -> None:
         call("bfvm_apply_dirichlet_conditions", self._h)
 
@@ -183,6 +186,20 @@ class Solver:
 
     def set_precision(self, bits: int) -> None:
         call("bfvm_set_precision", self._h, bits)
+
+    def set_sweep_config(self, axis: int, chunk: int, columns: int, min_blocks: int = 1) -> None:
+        call("bfvm_set_sweep_config", self._h, axis, chunk, columns, min_blocks)
+
+    def get_sweep_config(self, axis: int):
+        cfg = (ctypes.c_int * 3)()
+        call("bfvm_get_sweep_config", self._h, axis, cfg)
+        return tuple(cfg)
+
+    def set_kernel_path(self, path: int) -> None:
+        call("bfvm_set_kernel_path", self._h, path)
+
+    def set_fuse_sources(self, fuse: bool) -> None:
+        call("bfvm_set_fuse_sources", self._h, 1 if fuse else 0)
 
     def synchronize(self) -> None:
         call("bfvm_synchronize", self._h)
@@ -200,7 +217,8 @@ class Solver:
         return n.value
 
     def profile_step(self, dt: float, nsteps: int, flags: int = _abi.STEP_ALL):
-        ms = (ctypes.c_double * 3)()
+        """(sources, x, y, z) milliseconds per step."""
+        ms = (ctypes.c_double * 4)()
         call("bfvm_profile_step", self._h, dt, nsteps, flags, ms)
         return tuple(ms)
 

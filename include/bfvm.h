@@ -66,6 +66,11 @@ BFVM_API int bfvm_resize_space(bfvm_solver* m, double x0, double x1, double y0, 
  * (BioFVM_microenvironment.cpp:246-265 -> BioFVM_mesh.cpp:663-794). */
 BFVM_API int bfvm_resize_space_nodes(bfvm_solver* m, double x0, double x1, double y0, double y1,
                             double z0, double z1, int nx, int ny, int nz);
+/* Restores a mesh exactly as bfvm_get_mesh describes it (nxyz[3], geom[10],
+ * uniform flag), e.g. for a copy of a Microenvironment or a restart; no
+ * counterpart call in the reference, whose Cartesian_Mesh members are public.
+ * Densities are reset to zero and the lists cleared, as by a resize. */
+BFVM_API int bfvm_set_mesh(bfvm_solver* m, const int* nxyz, const double* geom, int uniform);
 /* nxyz[3] node counts; geom[10] = dx, dy, dz, dV, bounding box
  * (xmin, ymin, zmin, xmax, ymax, zmax); flags[2] = uniform_mesh, S. */
 BFVM_API int bfvm_get_mesh(bfvm_solver* m, int* nxyz, double* geom, int* flags);
@@ -140,6 +145,11 @@ BFVM_API int bfvm_simulate_cell_sources_and_sinks(bfvm_solver* m, double dt);
  * dispatching to diffusion_decay_solver__constant_coefficients_LOD_3D
  * (BioFVM_solvers.cpp:77-276). */
 BFVM_API int bfvm_simulate_diffusion_decay(bfvm_solver* m, double dt);
+/* diffusion_decay_solver__constant_coefficients_LOD_2D
+ * (BioFVM_solvers.cpp:278-427): x and y sweeps of the z = 0 plane with the
+ * decay split in halves; it shares the Thomas set-up with the 3-D solver as
+ * the reference does. */
+BFVM_API int bfvm_simulate_diffusion_decay_2d(bfvm_solver* m, double dt);
 /* Microenvironment::apply_dirichlet_conditions (BioFVM_microenvironment.cpp:192-197). */
 BFVM_API int bfvm_apply_dirichlet_conditions(bfvm_solver* m);
 /* nsteps of the canonical step bulk -> cells -> diffusion
@@ -158,15 +168,42 @@ BFVM_API int bfvm_reset_diffusion_setup(bfvm_solver* m);
  * resident field. */
 BFVM_API int bfvm_set_precision(bfvm_solver* m, int precision);
 
+/* Launch shape of one axis's sweep kernel (no counterpart in the reference,
+ * whose OpenMP loops have no tunables): chunk = points per thread (8, 16,
+ * 32), columns = lines per block (8..64), min_blocks = resident blocks per SM
+ * the kernel is compiled for (1, 2).  Kept until the next resize.  The
+ * default is chosen from the axis length; the autotuner sets this. */
+BFVM_API int bfvm_set_sweep_config(bfvm_solver* m, int axis, int chunk, int columns,
+                                   int min_blocks);
+/* config[3] = chunk, columns, min_blocks */
+/* Which sweep kernels run (all compute the same sweep):
+ *   BFVM_PATH_AUTO    (default) the register kernel for x, the TMA-fed
+ *                     persistent kernel for y and z where the layout allows
+ *                     it (16-byte multiple row and plane strides), else
+ *                     direct loads;
+ *   BFVM_PATH_GENERIC the first, table-free register kernel on every axis;
+ *   BFVM_PATH_TMA     TMA-fed persistent kernels on every axis they fit;
+ *   BFVM_PATH_DIRECT  direct-load kernels on every axis. */
+#define BFVM_PATH_AUTO 0
+#define BFVM_PATH_GENERIC 1
+#define BFVM_PATH_TMA 2
+#define BFVM_PATH_DIRECT 3
+BFVM_API int bfvm_set_kernel_path(bfvm_solver* m, int path);
+/* bfvm_step: 0 (default) runs the bulk and cell updates as their own kernels
+ * over the stored voxel lists before the x sweep; 1 applies them inside the
+ * x sweep's prologue.  Same results either way. */
+BFVM_API int bfvm_set_fuse_sources(bfvm_solver* m, int fuse);
+BFVM_API int bfvm_get_sweep_config(bfvm_solver* m, int axis, int* config);
+
 BFVM_API int bfvm_synchronize(bfvm_solver* m);
 /* The solver's cudaStream_t, for events and interop. */
 BFVM_API int bfvm_get_stream(bfvm_solver* m, void** stream);
 /* Kernel launches enqueued by this solver since creation. */
 BFVM_API int bfvm_get_launch_count(bfvm_solver* m, int64_t* count);
 
-/* Times one fused step's three sweep kernels with CUDA events on the solver's
- * stream, averaged over nsteps steps: ms[3] = x (with bulk/cells/Dirichlet
- * prologue), y, z. */
+/* Times bfvm_step's kernels with CUDA events on the solver's stream, averaged
+ * over nsteps steps: ms[4] = source kernels (bulk + cells), x sweep (with its
+ * Dirichlet prologue/epilogue), y sweep, z sweep. */
 BFVM_API int bfvm_profile_step(bfvm_solver* m, double dt, int nsteps, int flags, double* ms);
 
 #ifdef __cplusplus

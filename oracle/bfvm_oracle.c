@@ -28,8 +28,9 @@ int64_t or_nearest_voxel(const double* box_min, double dx, double dy, double dz,
   return ((int64_t)k * ny + j) * nx + i;
 }
 
-void or_thomas_setup(int n, int S, double dx, double dt, const double* D, const double* decay,
-                     double* c1, double* denom, double* cx) {
+static void thomas_setup_split(int n, int S, double dx, double dt, const double* D,
+                               const double* decay, double* c1, double* denom, double* cx,
+                               int dims) {
   for (int s = 0; s < S; ++s) {
     /* BioFVM_solvers.cpp:105-126: each constant built by the same sequence
      * of elementwise vector operations. */
@@ -41,7 +42,10 @@ void or_thomas_setup(int n, int S, double dx, double dt, const double* D, const 
     k1a *= -1.0;
     double k2 = decay[s];
     k2 *= dt;
-    k2 /= 3.0;
+    if (dims == 2)
+      k2 *= 0.5; /* :311-312 */
+    else
+      k2 /= 3.0;
     double k3 = 1.0;
     k3 += k1;
     k3 += k1;
@@ -68,6 +72,16 @@ void or_thomas_setup(int n, int S, double dx, double dt, const double* D, const 
       cx[(size_t)i * S + s] /= denom[(size_t)i * S + s];
     }
   }
+}
+
+void or_thomas_setup(int n, int S, double dx, double dt, const double* D, const double* decay,
+                     double* c1, double* denom, double* cx) {
+  thomas_setup_split(n, S, dx, dt, D, decay, c1, denom, cx, 3);
+}
+
+void or_thomas_setup_2d(int n, int S, double dx, double dt, const double* D,
+                        const double* decay, double* c1, double* denom, double* cx) {
+  thomas_setup_split(n, S, dx, dt, D, decay, c1, denom, cx, 2);
 }
 
 void or_apply_dirichlet(int S, double* p, int ndir, const int64_t* idx, const double* val) {
@@ -113,6 +127,17 @@ void or_lod3d(int nx, int ny, int nz, int S, double* p, const double* c1, const 
   or_apply_dirichlet(S, p, ndir, dir_idx, dir_val);
   for (int j = 0; j < ny; ++j)
     for (int i = 0; i < nx; ++i) thomas_line(p, (int64_t)j * nx + i, kj, nz, S, c1, denz, cxz);
+}
+
+void or_lod2d(int nx, int ny, int S, double* p, const double* c1, const double* denx,
+              const double* cxx, const double* deny, const double* cxy, int ndir,
+              const int64_t* dir_idx, const double* dir_val) {
+  /* :367-392 x-diffusion of the rows of the z = 0 plane */
+  or_apply_dirichlet(S, p, ndir, dir_idx, dir_val);
+  for (int j = 0; j < ny; ++j) thomas_line(p, (int64_t)j * nx, 1, nx, S, c1, denx, cxx);
+  /* :394-425 y-diffusion */
+  or_apply_dirichlet(S, p, ndir, dir_idx, dir_val);
+  for (int i = 0; i < nx; ++i) thomas_line(p, i, nx, ny, S, c1, deny, cxy);
 }
 
 void or_bulk(int64_t N, int S, double* p, const double* supply, const double* target,

@@ -29,6 +29,18 @@ int or_nodes_from_spacing(double start, double end, double d);
 int64_t or_nearest_voxel(const double* box_min, double dx, double dy, double dz, int nx,
                          int ny, int nz, double x, double y, double z);
 
+/* Thomas coefficients of one axis for the 2-D LOD solver
+ * (BioFVM_solvers.cpp:293-336): as or_thomas_setup with the decay split in
+ * halves (constant2 *= 0.5). */
+void or_thomas_setup_2d(int n, int S, double dx, double dt, const double* D,
+                        const double* decay, double* c1, double* denom, double* cx);
+
+/* diffusion_decay_solver__constant_coefficients_LOD_2D (BioFVM_solvers.cpp:
+ * 339-426): Dirichlet, x-Thomas on the z = 0 plane, Dirichlet, y-Thomas. */
+void or_lod2d(int nx, int ny, int S, double* p, const double* c1, const double* denx,
+              const double* cxx, const double* deny, const double* cxy, int ndir,
+              const int64_t* dir_idx, const double* dir_val);
+
 /* Thomas coefficients of one axis (BioFVM_solvers.cpp:105-170).
  * c1[S] = dt*D/dx^2, denom[n*S], cx[n*S] ([point][substrate]).  The
  * reference uses mesh.dx for all three axes (BioFVM_solvers.cpp:112-113). */

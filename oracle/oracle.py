@@ -58,6 +58,12 @@ def load_oracle() -> ctypes.CDLL:
                                          c_double, c_double, c_double]
         lib.or_thomas_setup.restype = None
         lib.or_thomas_setup.argtypes = [c_int, c_int, c_double, c_double, _DP, _DP, _DP, _DP, _DP]
+        lib.or_thomas_setup_2d.restype = None
+        lib.or_thomas_setup_2d.argtypes = [c_int, c_int, c_double, c_double, _DP, _DP, _DP, _DP,
+                                           _DP]
+        lib.or_lod2d.restype = None
+        lib.or_lod2d.argtypes = [c_int, c_int, c_int, _DP, _DP, _DP, _DP, _DP, _DP, c_int, _LP,
+                                 _DP]
         lib.or_apply_dirichlet.restype = None
         lib.or_apply_dirichlet.argtypes = [c_int, _DP, c_int, _LP, _DP]
         lib.or_lod3d.restype = None
@@ -103,6 +109,7 @@ def load_reference(variant: str = "core2") -> ctypes.CDLL:
             "refh_add_dirichlet": (None, [V, c_int, _DP]),
             "refh_update_dirichlet": (None, [V, c_int, _DP]),
             "refh_add_agent": (c_int, [V] + [c_double] * 4 + [_DP, _DP, _DP, c_double]),
+            "refh_set_solver": (None, [V, c_int]),
             "refh_step_bulk": (None, [V, c_double]),
             "refh_step_cells": (None, [V, c_double]),
             "refh_step_diffusion": (None, [V, c_double]),
@@ -130,6 +137,30 @@ def oracle_thomas(n: int, S: int, dx: float, dt: float, D, decay):
     cx = np.empty((n, S))
     lib.or_thomas_setup(n, S, dx, dt, _d(D), _d(decay), _d(c1), _d(den), _d(cx))
     return c1, den, cx
+
+
+def oracle_lod2d_run(scn, steps: int) -> np.ndarray:
+    """steps of the 2-D LOD solver on the z = 0 plane (diffusion only)."""
+    lib = load_oracle()
+    m = scn.mesh
+    S = scn.S
+    p = np.ascontiguousarray(scn.initial_field(), np.float64).copy()
+    D = np.ascontiguousarray(scn.D, np.float64)
+    dec = np.ascontiguousarray(scn.decay, np.float64)
+    c1 = np.empty(S)
+    dnx, cxx = np.empty((m.nx, S)), np.empty((m.nx, S))
+    dny, cxy = np.empty((m.ny, S)), np.empty((m.ny, S))
+    lib.or_thomas_setup_2d(m.nx, S, m.dx, scn.dt, _d(D), _d(dec), _d(c1), _d(dnx), _d(cxx))
+    lib.or_thomas_setup_2d(m.ny, S, m.dx, scn.dt, _d(D), _d(dec), _d(c1), _d(dny), _d(cxy))
+    if scn.dirichlet_voxels is not None and len(scn.dirichlet_voxels):
+        dv = np.ascontiguousarray(scn.dirichlet_voxels, np.int64)
+        dval = np.ascontiguousarray(scn.dirichlet_values, np.float64)
+    else:
+        dv, dval = np.zeros(0, np.int64), np.zeros((0, S))
+    for _ in range(steps):
+        lib.or_lod2d(m.nx, m.ny, S, _d(p), _d(c1), _d(dnx), _d(cxx), _d(dny), _d(cxy), dv.size,
+                     _l(dv), _d(dval))
+    return p
 
 
 def oracle_agent_arrays(scn):
@@ -213,6 +244,9 @@ class Reference:
                 _d(np.ascontiguousarray(scn.agent_secretion[a], np.float64)),
                 _d(np.ascontiguousarray(scn.agent_saturation[a], np.float64)),
                 _d(np.ascontiguousarray(scn.agent_uptake[a], np.float64)), scn.dt)
+
+    def set_solver(self, dims: int):
+        self.lib.refh_set_solver(self.h, dims)
 
     def mesh_info(self):
         nxyz = (c_int * 5)()

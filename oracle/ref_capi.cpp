@@ -210,6 +210,14 @@ int refh_add_agent(void* hp, double x, double y, double z, double volume,
   return a->nearest_voxel_index();
 }
 
+// 3 = diffusion_decay_solver__constant_coefficients_LOD_3D (the default),
+// 2 = diffusion_decay_solver__constant_coefficients_LOD_2D.
+void refh_set_solver(void* hp, int dims) {
+  static_cast<RefHarness*>(hp)->M->diffusion_decay_solver =
+      dims == 2 ? diffusion_decay_solver__constant_coefficients_LOD_2D
+                : diffusion_decay_solver__constant_coefficients_LOD_3D;
+}
+
 void refh_step_bulk(void* hp, double dt) {
   RefHarness* h = static_cast<RefHarness*>(hp);
   g_active = h;

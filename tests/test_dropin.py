@@ -1,0 +1,91 @@
+"""The C++ drop-in: the reference's own example programs, unmodified, built
+against biofvm_b200's headers (biofvm_b200/shim) run on the GPU and write the
+same MATLAB files as the same programs built against the reference."""
+import glob
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
+SHIM_INCLUDE = os.path.join(ROOT, "biofvm_b200", "shim", "include")
+DROPIN = os.path.join(ROOT, "biofvm_b200", "shim", "_build", "dropin", "examples")
+REFBIN = os.path.join(ROOT, "oracle", "_ref", "examples")
+REFERENCE_EXAMPLES = "/root/reference/examples"
+
+# example -> command-line arguments (dt, t_max, dx where the example takes them)
+EXAMPLES = {
+    "convergence_test1": ["0.01", "0.5", "20"],
+    "convergence_test2": ["0.01", "1", "20"],
+    "tutorial2_BioFVM": [],
+    "tutorial3_BioFVM": [],
+}
+
+
+def read_mat4(path):
+    """MATLAB Level-4 full real double matrix -> array [rows, cols]."""
+    with open(path, "rb") as f:
+        typ, rows, cols, imag, nlen = np.frombuffer(f.read(20), dtype="<i4")
+        assert typ == 0 and imag == 0
+        f.read(int(nlen))
+        data = np.frombuffer(f.read(), dtype="<f8")
+    return data.reshape(int(cols), int(rows)).T
+
+
+@pytest.mark.skipif(not os.path.isdir(REFERENCE_EXAMPLES), reason="reference sources absent")
+def test_every_reference_driver_compiles_against_the_dropin_headers(tmp_path):
+    work = tmp_path / "examples"
+    work.mkdir()
+    os.symlink(os.path.join(SHIM_INCLUDE, "BioFVM.h"), tmp_path / "BioFVM.h")
+    sources = sorted(glob.glob(os.path.join(REFERENCE_EXAMPLES, "*.cpp")))
+    assert len(sources) >= 14
+    for src in sources:
+        with open(src, "rb") as f:
+            r = subprocess.run(["/usr/bin/g++", "-std=c++14", "-fopenmp", "-fsyntax-only",
+                                "-I", SHIM_INCLUDE, "-I", os.path.join(ROOT, "include"),
+                                "-x", "c++", "-"], stdin=f, cwd=work, capture_output=True,
+                               text=True)
+        assert r.returncode == 0, (src, r.stderr[-2000:])
+
+
+def test_dropin_library_exports_the_reference_api():
+    lib = os.path.join(ROOT, "biofvm_b200", "libbiofvm_b200.so")
+    out = subprocess.run(["nm", "-DC", "--defined-only", lib], capture_output=True, text=True,
+                         check=True).stdout
+    for sym in ["BioFVM::Microenvironment::simulate_diffusion_decay(double)",
+                "BioFVM::Microenvironment::simulate_bulk_sources_and_sinks(double)",
+                "BioFVM::Microenvironment::simulate_cell_sources_and_sinks(double)",
+                "BioFVM::Microenvironment::apply_dirichlet_conditions()",
+                "BioFVM::Microenvironment::resize_space_uniform(double, double, double, double, "
+                "double, double, double)",
+                "BioFVM::Basic_Agent::set_internal_uptake_constants(double)",
+                "BioFVM::create_basic_agent()",
+                "BioFVM::diffusion_decay_solver__constant_coefficients_LOD_3D("
+                "BioFVM::Microenvironment&, double)"]:
+        assert sym in out, sym
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(EXAMPLES))
+def test_reference_example_runs_unchanged_on_the_gpu(name, tmp_path):
+    dropin = os.path.join(DROPIN, name)
+    ref = os.path.join(REFBIN, name)
+    if not (os.path.exists(dropin) and os.path.exists(ref)):
+        pytest.skip("example binaries not built (they need the reference sources)")
+    outs = {}
+    for tag, exe in (("ref", ref), ("gpu", dropin)):
+        d = tmp_path / tag
+        d.mkdir()
+        r = subprocess.run([exe, *EXAMPLES[name]], cwd=d, capture_output=True, text=True,
+                           timeout=600)
+        assert r.returncode == 0, (tag, r.stdout[-2000:], r.stderr[-2000:])
+        outs[tag] = {os.path.basename(p): read_mat4(p) for p in glob.glob(str(d / "*.mat"))}
+    assert outs["ref"] and set(outs["ref"]) == set(outs["gpu"])
+    for fname, a in outs["ref"].items():
+        b = outs["gpu"][fname]
+        assert a.shape == b.shape, fname
+        assert np.array_equal(a[:4], b[:4]), fname  # voxel centres and volumes
+        den = np.maximum(np.abs(a[4:]).max(axis=1), 1e-300)
+        err = np.abs(a[4:] - b[4:]).max(axis=1) / den
+        assert np.all(err <= 1e-12), (fname, err)

@@ -91,3 +91,17 @@ def test_mass_balance_without_sources():
     p1 = O.oracle_run(scn, 1, 4)
     c2 = scn.dt * scn.decay / 3.0
     np.testing.assert_allclose(p1.sum(0), p0.sum(0) / (1 + c2) ** 3, rtol=1e-13)
+
+
+@pytest.mark.skipif(not REF, reason="compiled reference (oracle/_ref) not built")
+@pytest.mark.parametrize("shape", [(17, 13, 1), (9, 11, 3), (1, 6, 1)])
+def test_lod2d_oracle_matches_reference(shape):
+    """diffusion_decay_solver__constant_coefficients_LOD_2D: the z = 0 plane,
+    decay split in halves, Dirichlet before each sweep."""
+    scn = W.mixed_small(shape=shape, S=2, n_agents=0, seed=sum(shape), bulk=False)
+    a = O.oracle_lod2d_run(scn, 3)
+    with O.Reference(scn) as ref:
+        ref.set_solver(2)
+        ref.run(3, 4)
+        b = ref.densities()
+    assert np.array_equal(a, b)

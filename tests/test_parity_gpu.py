@@ -9,7 +9,7 @@ import pytest
 
 from biofvm_b200 import STEP_BULK, STEP_CELLS, STEP_DIFFUSION, Solver, load_scenario
 from biofvm_b200 import workloads as W
-from biofvm_b200._abi import BfvmError
+from biofvm_b200._abi import PATH_AUTO, PATH_DIRECT, PATH_GENERIC, PATH_TMA, BfvmError
 from cases import CASES, sha
 from conftest import load_golden
 from oracle import oracle as O
@@ -24,9 +24,10 @@ def rel_err(a, b):
     return O.max_rel_err(a, b)
 
 
-def run_gpu(scn, steps, flags, fused=True, precision=64):
+def run_gpu(scn, steps, flags, fused=True, precision=64, path=PATH_AUTO):
     with Solver(0) as sv:
         load_scenario(sv, scn)
+        sv.set_kernel_path(path)
         if precision != 64:
             sv.set_precision(precision)
         if fused:
@@ -42,13 +43,18 @@ def run_gpu(scn, steps, flags, fused=True, precision=64):
         return sv.get_densities()
 
 
+PATHS = [PATH_AUTO, PATH_TMA, PATH_DIRECT, PATH_GENERIC]
+PATH_IDS = ["auto", "tma", "direct", "generic"]
+
+
+@pytest.mark.parametrize("path", PATHS, ids=PATH_IDS)
 @pytest.mark.parametrize("fused", [True, False], ids=["fused", "per_call"])
 @pytest.mark.parametrize("name", list(CASES))
-def test_golden_cases(name, fused):
+def test_golden_cases(name, fused, path):
     build, flags, steps, _ = CASES[name]
     scn = build()
     g = load_golden(name)
-    p = run_gpu(scn, steps, flags, fused)
+    p = run_gpu(scn, steps, flags, fused, path=path)
     assert p.shape == tuple(g["shape"])
     if not flags & STEP_DIFFUSION:
         # per-voxel updates only: same IEEE operations in the same order
@@ -174,12 +180,32 @@ def test_plain_50_against_reference_golden():
     assert np.all(rel_err(p, ref) <= TOL64)
 
 
-def test_fp32_sweeps_error_bound():
+@pytest.mark.parametrize("path", PATHS, ids=PATH_IDS)
+def test_fp32_sweeps_error_bound(path):
     scn = W.lod_cube(48, 4, 2000, steps=20, seed=5, bulk_radius=150.0, name="lod_48")
     ref = O.oracle_run(scn, 20, 7)
-    p32 = run_gpu(scn, 20, 7, precision=32)
+    p32 = run_gpu(scn, 20, 7, precision=32, path=path)
     err = rel_err(p32, ref)
     assert np.all(err <= TOL32), err
+
+
+@pytest.mark.parametrize("shape,S", [((7, 5, 3), 1), ((13, 11, 9), 3), ((40, 33, 21), 2)])
+def test_layouts_without_tma_alignment(shape, S):
+    """Row or plane strides that are not 16-byte multiples fall back to the
+    register kernel for that axis; mixed paths in one step must agree."""
+    scn = W.mixed_small(shape=shape, S=S, n_agents=100, seed=sum(shape))
+    ref = O.oracle_run(scn, 3, 7)
+    p = run_gpu(scn, 3, 7)
+    assert np.all(rel_err(p, ref) <= TOL64)
+
+
+def test_long_lines_multiple_boxes():
+    """Lines longer than one 256-row tensor box (two boxes per tile)."""
+    scn = W.mixed_small(shape=(20, 300, 12), S=2, n_agents=200, seed=77)
+    ref = O.oracle_run(scn, 2, 7)
+    for path in PATHS:
+        p = run_gpu(scn, 2, 7, path=path)
+        assert np.all(rel_err(p, ref) <= TOL64), path
 
 
 @pytest.mark.slow
@@ -201,3 +227,54 @@ def test_lod_256_full_size_two_steps():
         p1 = sv.get_densities()
     c2 = scn.dt * scn.decay / 3.0
     np.testing.assert_allclose(p1.sum(0), p0.sum(0) / (1 + c2) ** 3, rtol=1e-12)
+
+
+@pytest.mark.parametrize("chunk", [8, 16, 32])
+@pytest.mark.parametrize("path", PATHS, ids=PATH_IDS)
+def test_chunk_lengths(chunk, path):
+    """Every chunk length on every path (the segment lists and the chunk
+    tables are rebuilt for it)."""
+    scn = W.mixed_small(shape=(40, 36, 30), S=3, n_agents=300, seed=91)
+    ref = O.oracle_run(scn, 2, 7)
+    with Solver(0) as sv:
+        load_scenario(sv, scn)
+        sv.set_kernel_path(path)
+        for ax in range(3):
+            sv.set_sweep_config(ax, chunk, 16 if chunk == 8 else 32)
+        sv.step(scn.dt, 2)
+        p = sv.get_densities()
+    assert np.all(rel_err(p, ref) <= TOL64)
+
+
+@pytest.mark.parametrize("path", PATHS, ids=PATH_IDS)
+@pytest.mark.parametrize("name", ["mixed_full", "mixed_odd", "plain_50"])
+def test_sources_fused_into_the_x_sweep(name, path):
+    """Bulk and cell updates in the x sweep's prologue give the same field as
+    the separate source kernels."""
+    build, flags, steps, _ = CASES[name]
+    scn = build()
+    steps = min(steps, 10)
+    ref = O.oracle_run(scn, steps, flags)
+    with Solver(0) as sv:
+        load_scenario(sv, scn)
+        sv.set_kernel_path(path)
+        sv.set_fuse_sources(True)
+        sv.step(scn.dt, steps, flags)
+        p = sv.get_densities()
+    assert np.all(rel_err(p, ref) <= TOL64)
+
+
+@pytest.mark.parametrize("path", PATHS, ids=PATH_IDS)
+@pytest.mark.parametrize("shape", [(17, 13, 1), (9, 11, 3), (64, 48, 1)])
+def test_lod2d(shape, path):
+    """diffusion_decay_solver__constant_coefficients_LOD_2D on the GPU: the
+    z = 0 plane only, decay split in halves, Dirichlet before each sweep."""
+    scn = W.mixed_small(shape=shape, S=2, n_agents=0, seed=sum(shape), bulk=False)
+    ref = O.oracle_lod2d_run(scn, 3)
+    with Solver(0) as sv:
+        load_scenario(sv, scn)
+        sv.set_kernel_path(path)
+        for _ in range(3):
+            sv.simulate_diffusion_decay_2d(scn.dt)
+        p = sv.get_densities()
+    assert np.all(rel_err(p, ref) <= TOL64)

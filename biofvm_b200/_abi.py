@@ -57,6 +57,7 @@ SIGNATURES = {
     "bfvm_get_densities": (c_int, [_P, _DP]),
     "bfvm_get_voxel_densities": (c_int, [_P, c_int64, _LP, _DP]),
     "bfvm_set_voxel_densities": (c_int, [_P, c_int64, _LP, _DP]),
+    "bfvm_get_voxel_densities_noalloc": (c_int, [_P, c_int64, _LP, _DP]),
     "bfvm_device_densities": (c_int, [_P, POINTER(c_void_p)]),
     "bfvm_set_bulk_rates": (c_int, [_P, _DP, _DP, _DP]),
     "bfvm_set_bulk_rates_sparse": (c_int, [_P, c_int64, _LP, _DP, _DP, _DP]),

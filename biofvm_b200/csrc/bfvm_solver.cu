@@ -17,6 +17,7 @@
 #include "bfvm_kernels.cuh"
 #include "bfvm_kernels_tma.cuh"
 #include <cudaTypedefs.h>
+#include <mutex>
 
 namespace {
 
@@ -1789,3 +1790,75 @@ int bfvm_profile_step(bfvm_solver* m, double dt, int nsteps, int flags, double* 
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Gather without allocation.
+//
+// bfvm_get_voxel_densities allocates two small device buffers per call (the
+// voxel list and the gathered values).  Some callers can't call cudaMalloc:
+// cudaMalloc and cudaFree can synchronise the whole device, which a host loop
+// that must not stall cannot afford, and in a process whose device memory is
+// held by another allocator (a framework's caching allocator) a fresh
+// cudaMalloc may fail.  bfvm_get_voxel_densities_noalloc does the same gather
+// through one file-scope device array of fixed size instead.  Every GPU that
+// loads the library holds the array until the process exits; every call (on
+// any solver of that device) reuses it and it keeps the last call's contents.
+// Nothing in it needs to start at zero: the voxel list and the values are
+// written before they are read.  Calls whose GPU work overlaps (from several
+// host threads, or on several solvers' streams at once) race on the array;
+// each call synchronises its solver's stream before returning, so calls made
+// one after another never overlap.
+
+namespace {
+
+constexpr size_t kGatherScratchBytes = (size_t)4 << 20;  // 4 MiB
+__device__ __align__(256) unsigned char g_gather_scratch[kGatherScratchBytes];
+
+std::mutex g_gather_scratch_mutex;
+void* g_gather_scratch_addr[64] = {};  // per device, set on first use
+
+// Device address of g_gather_scratch on the current device (the caller has
+// made m->device current).  In host code the array's name is only a host-side
+// stand-in, so the address is looked up once per device.
+void* gather_scratch(int device) {
+  require(device >= 0 && device < 64, "device index out of range for the static scratch");
+  std::lock_guard<std::mutex> g(g_gather_scratch_mutex);
+  if (g_gather_scratch_addr[device] == nullptr) {
+    void* ptr = nullptr;
+    BFVM_CUDA(cudaGetSymbolAddress(&ptr, g_gather_scratch));
+    require(ptr != nullptr, "cudaGetSymbolAddress returned no address", BFVM_ERR_CUDA);
+    g_gather_scratch_addr[device] = ptr;
+  }
+  return g_gather_scratch_addr[device];
+}
+
+}  // namespace
+
+extern "C" int bfvm_get_voxel_densities_noalloc(bfvm_solver* m, int64_t count,
+                                                const int64_t* voxels, double* values) {
+  return SOLVER_CALL(m, {
+    require(count >= 0 && (count == 0 || (voxels && values)), "bad arguments");
+    const size_t vox_bytes = ((size_t)count * sizeof(int64_t) + 255) & ~(size_t)255;
+    const size_t val_bytes = (size_t)count * m->S * sizeof(double);
+    require(vox_bytes + val_bytes <= kGatherScratchBytes,
+            "bfvm_get_voxel_densities_noalloc: " + std::to_string(count) + " voxels x " +
+                std::to_string(m->S) + " densities need " +
+                std::to_string(vox_bytes + val_bytes) + " bytes of the " +
+                std::to_string(kGatherScratchBytes) +
+                "-byte static scratch (at most count*(8 + 8*S) bytes, after rounding the "
+                "voxel list up to 256 bytes)");
+    validate_voxels(m, count, voxels);
+    if (count == 0) return;
+    unsigned char* base = static_cast<unsigned char*>(gather_scratch(m->device));
+    int64_t* d_vox = reinterpret_cast<int64_t*>(base);
+    double* d_out = reinterpret_cast<double*>(base + vox_bytes);
+    BFVM_CUDA(cudaMemcpyAsync(d_vox, voxels, (size_t)count * sizeof(int64_t),
+                              cudaMemcpyHostToDevice, m->stream));
+    if (m->precision == BFVM_FP64)
+      gather<double>(m, count, d_vox, d_out);
+    else
+      gather<float>(m, count, d_vox, d_out);
+    BFVM_CUDA(cudaMemcpyAsync(values, d_out, val_bytes, cudaMemcpyDeviceToHost, m->stream));
+    BFVM_CUDA(cudaStreamSynchronize(m->stream));
+  });
+}

@@ -99,6 +99,21 @@ BFVM_API int bfvm_get_voxel_densities(bfvm_solver* m, int64_t count, const int64
                              double* values);
 BFVM_API int bfvm_set_voxel_densities(bfvm_solver* m, int64_t count, const int64_t* voxels,
                              const double* values);
+/* The same gather as bfvm_get_voxel_densities, for callers that can't call
+ * cudaMalloc (no counterpart in the reference, which has no device).
+ * cudaMalloc and cudaFree can synchronise the whole device, which a host
+ * loop that must not stall cannot afford, and where another allocator holds
+ * the device's memory a fresh cudaMalloc may fail.  This entry point
+ * allocates nothing: it stages the voxel list and the values in one 4 MiB
+ * file-scope device array, so count*(8 + 8*S) bytes (the voxel list rounded
+ * up to 256) must fit, else BFVM_ERR_ARG.  Every GPU that loads the library
+ * holds that array until exit.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress); make that first call before
+ * any stream capture.  All calls share the array and it keeps the last
+ * call's contents; calls whose GPU work overlaps race on it (each call
+ * synchronises the solver's stream before returning). */
+BFVM_API int bfvm_get_voxel_densities_noalloc(bfvm_solver* m, int64_t count,
+                                              const int64_t* voxels, double* values);
 /* Device address of the density field ([N][S], double or float per the
  * precision); valid until the next resize or precision change. */
 BFVM_API int bfvm_device_densities(bfvm_solver* m, void** device_ptr);

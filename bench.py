@@ -48,60 +48,84 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons, sampled during the timed region."""
+    """SM clock and clock-event (throttle) reasons of this process's GPU,
+    sampled through NVML every 5 ms while the timed region runs (read only;
+    nothing is set).  Falls back to `nvidia-smi -lms 50` without NVML."""
 
-    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": "nvmlClocksEventReasonHwSlowdown",
+               "hw_thermal_slowdown": "nvmlClocksEventReasonHwThermalSlowdown",
+               "sw_thermal_slowdown": "nvmlClocksEventReasonSwThermalSlowdown",
+               "sw_power_cap": "nvmlClocksEventReasonSwPowerCap"}
 
     def __init__(self, gpu: int):
         self.gpu = gpu
+        self.samples: list[tuple[float, float, set]] = []
+        self.stop = threading.Event()
+        self.t = None
         self.proc = None
-        self.lines: list[str] = []
+
+    def _nvml_handle(self):
+        import pynvml
+
+        pynvml.nvmlInit()
+        try:
+            import torch
+
+            pr = torch.cuda.get_device_properties(self.gpu)
+            bus = f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
+
+    def _nvml_loop(self, nv, h):
+        mx = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+        masks = {k: getattr(nv, v) for k, v in self.REASONS.items()}
+        while not self.stop.is_set():
+            sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+            r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+            self.samples.append((sm, mx, {k for k, m in masks.items() if r & m}))
+            self.stop.wait(0.005)
+
+    def _smi_loop(self):
+        q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        self.proc = subprocess.Popen(
+            ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+             "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        for line in self.proc.stdout:
+            f = [x.strip() for x in line.split(",")]
+            try:
+                sm, mx = float(f[0]), float(f[1])
+            except (ValueError, IndexError):
+                continue
+            act = {k for k, v in zip(self.REASONS, f[2:6]) if v.lower() == "active"}
+            self.samples.append((sm, mx, act))
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
-        except (FileNotFoundError, OSError):
-            self.proc = None
+            nv, h = self._nvml_handle()
+            self.t = threading.Thread(target=self._nvml_loop, args=(nv, h), daemon=True)
+        except Exception:
+            self.t = threading.Thread(target=self._smi_loop, daemon=True)
+        self.t.start()
+        time.sleep(0.01)
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
-
     def __exit__(self, *exc):
+        self.stop.set()
         if self.proc is not None:
             self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
+        if self.t is not None:
+            self.t.join(timeout=5)
 
     def summary(self):
-        sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
-            f = [x.strip() for x in line.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                mx.append(float(f[2]))
-            except ValueError:
-                continue
-            for n, v in zip(names, f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
-        if not sm:
+        if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
-                "reasons": sorted(reasons), "samples": len(sm)}
+        reasons = set().union(*(r for _, _, r in self.samples))
+        return {"sm_mhz": statistics.median(s for s, _, _ in self.samples),
+                "sm_max_mhz": max(m for _, m, _ in self.samples),
+                "reasons": sorted(reasons), "samples": len(self.samples)}
 
 
 def ncu_traffic(kernel_key: str):
@@ -272,8 +296,21 @@ def run_ours(args, world, rank, local):
     # change rates each step) and reads back the densities at the agents.
     e2e = None
     if not args.no_e2e:
-        vox, t1, t2 = scn.agent_arrays()
-        out = np.empty((scn.num_agents, S))
+        # host buffers in page-locked memory, as a host loop that exchanges
+        # agent data with the solver every step would keep them
+        import torch
+
+        keep = []
+
+        def pinned(a):
+            t = torch.empty(a.shape, dtype=torch.from_numpy(a[:0]).dtype, pin_memory=True)
+            keep.append(t)
+            v = t.numpy()
+            v[...] = a
+            return v
+
+        vox, t1, t2 = (pinned(np.ascontiguousarray(a)) for a in scn.agent_arrays())
+        out = pinned(np.empty((scn.num_agents, S)))
         e_steps = max(1, min(args.steps, 20))
         sv.synchronize()
         barrier(world)
@@ -287,8 +324,8 @@ def run_ours(args, world, rank, local):
         e2e = {"value": N * S * e_steps * world / e_secs, "unit": UNIT,
                "h2d_bytes_per_step": int(vox.nbytes + t1.nbytes + t2.nbytes),
                "d2h_bytes_per_step": int(out.nbytes), "steps": e_steps,
-               "what": "per step: bfvm_set_agents (host voxel+temp1+temp2), bfvm_step, "
-                       "bfvm_get_agent_densities (host [A][S])"}
+               "what": "per step: bfvm_set_agents (pinned host voxel+temp1+temp2), bfvm_step, "
+                       "bfvm_get_agent_densities (pinned host [A][S]); wall clock"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -328,6 +365,172 @@ def run_ours(args, world, rank, local):
     sv.close()
 
 
+def run_batched(args, world, rank, local):
+    """The batched workload: 64 independent microenvironments (grids drawn
+    from 32^3 to 128^3, 1-8 substrates, 0-20k agents each; seeded), 200 steps,
+    advanced by one bfvm_batch_step call (one CUDA-graph replay) against the
+    same instances solved one after another with bfvm_step.  Both arms start
+    from the same fields and are timed by the wall clock around the call plus
+    a device synchronisation; the batched results must match the looped ones
+    within 1e-10 relative max-norm per substrate."""
+    import numpy as np
+
+    from biofvm_b200 import STEP_ALL, Batch, Solver, load_scenario
+    from biofvm_b200 import workloads as W
+
+    count = args.instances
+    scns = W.batched_instances(count=count, steps=args.steps)
+    sols = []
+    for scn in scns:
+        sv = Solver(local)
+        load_scenario(sv, scn)
+        sols.append(sv)
+    dt = scns[0].dt
+    vs_per_step = sum(s.num_voxels * s.S for s in scns)
+
+    def reset():
+        for sv, scn in zip(sols, scns):
+            sv.set_densities(scn.initial_field())
+        for sv in sols:
+            sv.synchronize()
+
+    # looped plain solves (first one warms every instance up: Thomas setup, lists)
+    for sv in sols:
+        sv.step(dt, 1, STEP_ALL)
+    reset()
+    barrier(world)
+    t0 = time.perf_counter()
+    for sv in sols:
+        sv.step(dt, args.steps, STEP_ALL)
+        sv.synchronize()
+    t_plain = max_over_ranks(time.perf_counter() - t0, world)
+    plain = [sv.get_densities() for sv in sols]
+
+    bt = Batch(local)
+    for sv in sols:
+        bt.add(sv)
+    reset()
+    t0 = time.perf_counter()
+    bt.tune(dt, STEP_ALL, 3)
+    t_tune = time.perf_counter() - t0
+    cfg = bt.get_config()
+    # first call captures the graph; the timed call replays it
+    reset()
+    t0 = time.perf_counter()
+    bt.step(dt, args.steps, STEP_ALL)
+    bt.synchronize()
+    t_first = time.perf_counter() - t0
+    reset()
+    with ClockSampler(local) as clocks:
+        barrier(world)
+        t0 = time.perf_counter()
+        bt.step(dt, args.steps, STEP_ALL)
+        bt.synchronize()
+        t_batch = max_over_ranks(time.perf_counter() - t0, world)
+    groups, kernels = bt.plan()
+    err = 0.0
+    for sv, ref in zip(sols, plain):
+        p = sv.get_densities()
+        den = np.maximum(np.abs(ref).max(axis=0), 1e-300)
+        err = max(err, float((np.abs(p - ref).max(axis=0) / den).max()))
+    bt.close()
+    for sv in sols:
+        sv.close()
+    if rank == 0:
+        line = {
+            "metric": METRIC + " (batched instances)", "value": vs_per_step * args.steps * world /
+            t_batch, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": 1,
+            "ms_per_step": 1e3 * t_batch / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": f"batched: {count} instances, grids 32^3..128^3, 1-8 "
+                                   f"substrates, 0-20k agents, {args.steps} steps",
+                       "voxel_substrates_per_step": vs_per_step,
+                       "field_bytes": vs_per_step * 8},
+            "looped_plain": {"value": vs_per_step * args.steps * world / t_plain,
+                             "seconds": t_plain},
+            "batched_seconds": t_batch, "speedup_vs_looped_plain": t_plain / t_batch,
+            "max_rel_err_vs_looped_plain": err,
+            "tuned": {"chunk": cfg[0], "threads": cfg[1], "group_bytes": cfg[2],
+                      "tune_seconds": t_tune},
+            "graph": {"groups": groups, "kernels_per_call": kernels,
+                      "first_call_seconds": t_first},
+            "gpu_launches": kernels,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+
+
+def run_fp32(args, world, rank, local):
+    """FP32 sweeps (FP64 Thomas coefficients rounded once to FP32, FP64
+    arithmetic in the bulk and cell updates) at 512^3 voxels x 8 substrates
+    with 1M agents, 50 steps, next to the FP64 path timed on the same
+    workload; reports the max relative error per substrate of the FP32 field
+    against the FP64 one after the run."""
+    import numpy as np
+    import torch
+
+    from biofvm_b200 import FP32, STEP_ALL, Solver, load_scenario
+    from biofvm_b200 import workloads as W
+
+    n = args.size if "--size" in sys.argv else 512
+    S = args.substrates if "--substrates" in sys.argv else 8
+    A = args.agents if "--agents" in sys.argv else 1_000_000
+    scn = W.lod_cube(n, S, A, steps=args.steps, name=f"lod_{n}")
+    N = scn.num_voxels
+    sv = Solver(local)
+    load_scenario(sv, scn)
+    dt = scn.dt
+    stream = torch.cuda.ExternalStream(sv.stream, device=torch.device("cuda", local))
+    p0 = scn.initial_field()
+
+    def timed(clocks=None):
+        sv.step(dt, args.warmup, STEP_ALL)
+        sv.set_densities(p0)
+        sv.synchronize()
+        barrier(world)
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        sv.step(dt, args.steps, STEP_ALL)
+        ev1.record(stream)
+        ev1.synchronize()
+        return max_over_ranks(ev0.elapsed_time(ev1), world)
+
+    ms64 = timed()
+    ref = sv.get_densities()
+    sv.set_precision(FP32)
+    sv.set_densities(p0)
+    with ClockSampler(local) as clocks:
+        ms32 = timed()
+    got = sv.get_densities()
+    den = np.maximum(np.abs(ref).max(axis=0), 1e-300)
+    err = (np.abs(got - ref).max(axis=0) / den).tolist()
+    sv.close()
+    if rank == 0:
+        hbm, peak_kind = peaks()
+        bytes32 = 3 * 8 * N * S * args.steps
+        line = {
+            "metric": METRIC + " (FP32 sweeps)", "value": N * S * args.steps * world / (ms32 / 1e3),
+            "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms32 / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": f"lod_{n}: {n}^3 voxels x {S} substrates, {A} agents, "
+                                   f"{args.steps} steps, FP32 sweeps / FP64 coefficients and "
+                                   f"source arithmetic", "voxels": N, "substrates": S,
+                       "agents": A, "l2": "inputs larger than L2; no flush"},
+            "hbm_gbs_step": bytes32 / (ms32 / 1e3) / 1e9,
+            "roofline": {"bound": "hbm", "kernel": "whole step (3 sweeps, 24 B/VS)",
+                         "achieved": bytes32 / (ms32 / 1e3) / 1e9, "peak": hbm,
+                         "peak_kind": peak_kind, "unit": "GB/s",
+                         "frac": bytes32 / (ms32 / 1e3) / 1e9 / hbm, "traffic": None},
+            "fp64_same_workload": {"value": N * S * args.steps * world / (ms64 / 1e3),
+                                   "ms_per_step": ms64 / args.steps},
+            "max_rel_err_vs_fp64_per_substrate": err,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -339,12 +542,25 @@ def main():
     ap.add_argument("--size", type=int, default=256, help="cube edge in voxels (default 256)")
     ap.add_argument("--substrates", type=int, default=10)
     ap.add_argument("--agents", type=int, default=100_000)
+    ap.add_argument("--workload", choices=["lod256", "batched", "fp32"], default="lod256",
+                    help="lod256: the headline line (default); batched: 64 independent "
+                         "instances vs looped plain solves; fp32: FP32 sweeps at 512^3 x 8 "
+                         "with 1M agents against FP64")
+    ap.add_argument("--instances", type=int, default=64)
     args = ap.parse_args()
+    if args.workload == "batched" and "--steps" not in sys.argv:
+        args.steps = 200
+    if args.workload == "fp32" and "--steps" not in sys.argv:
+        args.steps = 50
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     world, rank, local = dist_init(args)
     try:
         if args.impl == "reference":
             run_reference_arm(args, world, rank)
+        elif args.workload == "batched":
+            run_batched(args, world, rank, local)
+        elif args.workload == "fp32":
+            run_fp32(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:

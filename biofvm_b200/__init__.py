@@ -7,7 +7,8 @@ built library, importing the solver raises.
 """
 from . import mesh, workloads
 from ._abi import BfvmError, FP32, FP64, STEP_ALL, STEP_BULK, STEP_CELLS, STEP_DIFFUSION
+from .batch import Batch
 from .solver import Solver, load_scenario
 
-__all__ = ["Solver", "load_scenario", "mesh", "workloads", "BfvmError", "FP32", "FP64",
+__all__ = ["Batch", "Solver", "load_scenario", "mesh", "workloads", "BfvmError", "FP32", "FP64",
            "STEP_ALL", "STEP_BULK", "STEP_CELLS", "STEP_DIFFUSION"]

@@ -84,6 +84,17 @@ SIGNATURES = {
     "bfvm_get_stream": (c_int, [_P, POINTER(c_void_p)]),
     "bfvm_get_launch_count": (c_int, [_P, _LP]),
     "bfvm_profile_step": (c_int, [_P, c_double, c_int, c_int, _DP]),
+    "bfvm_batch_create": (c_int, [POINTER(c_void_p), c_int]),
+    "bfvm_batch_destroy": (c_int, [_P]),
+    "bfvm_batch_add": (c_int, [_P, _P]),
+    "bfvm_batch_clear": (c_int, [_P]),
+    "bfvm_batch_size": (c_int, [_P, _IP]),
+    "bfvm_batch_step": (c_int, [_P, c_double, c_int, c_int]),
+    "bfvm_batch_tune": (c_int, [_P, c_double, c_int, c_int]),
+    "bfvm_batch_set_config": (c_int, [_P, _IP, _IP, c_int64]),
+    "bfvm_batch_get_config": (c_int, [_P, _IP, _IP, _LP]),
+    "bfvm_batch_get_plan": (c_int, [_P, _IP, _LP]),
+    "bfvm_batch_synchronize": (c_int, [_P]),
 }
 
 _lib = None

@@ -1,0 +1,82 @@
+"""Many independent microenvironments advanced together, over the C ABI
+(``bfvm_batch_*`` in include/bfvm.h).
+
+``Batch.step(dt, n, flags)`` has the effect of ``Solver.step(dt, n, flags)``
+on every member; the members are packed into L2-sized groups and the whole
+run is one CUDA-graph replay.  The reference has no such object: its drivers
+loop over Microenvironment instances one by one.
+"""
+from __future__ import annotations
+
+import ctypes
+
+from . import _abi
+from ._abi import call
+from .solver import Solver
+
+
+class Batch:
+    def __init__(self, device: int = 0):
+        _abi.load_library()
+        h = ctypes.c_void_p()
+        call("bfvm_batch_create", ctypes.byref(h), device)
+        self._h = h
+        self.members: list[Solver] = []
+
+    def close(self) -> None:
+        if self._h is not None:
+            call("bfvm_batch_destroy", self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add(self, sv: Solver) -> None:
+        call("bfvm_batch_add", self._h, sv.handle)
+        self.members.append(sv)  # keeps the member alive while it is in the batch
+
+    def clear(self) -> None:
+        call("bfvm_batch_clear", self._h)
+        self.members.clear()
+
+    def __len__(self) -> int:
+        n = ctypes.c_int()
+        call("bfvm_batch_size", self._h, ctypes.byref(n))
+        return n.value
+
+    def step(self, dt: float, nsteps: int = 1, flags: int = _abi.STEP_ALL) -> None:
+        call("bfvm_batch_step", self._h, dt, nsteps, flags)
+
+    def tune(self, dt: float, flags: int = _abi.STEP_ALL, trial_steps: int = 5) -> None:
+        call("bfvm_batch_tune", self._h, dt, flags, trial_steps)
+
+    def set_config(self, chunk=(0, 0, 0), threads=(0, 0, 0), group_bytes: int = -1) -> None:
+        ch = (ctypes.c_int * 3)(*chunk)
+        th = (ctypes.c_int * 3)(*threads)
+        call("bfvm_batch_set_config", self._h, ch, th, group_bytes)
+
+    def get_config(self):
+        ch = (ctypes.c_int * 3)()
+        th = (ctypes.c_int * 3)()
+        gb = ctypes.c_int64()
+        call("bfvm_batch_get_config", self._h, ch, th, ctypes.byref(gb))
+        return tuple(ch), tuple(th), gb.value
+
+    def plan(self):
+        """(groups of the last plan, kernel launches per step() call)."""
+        g = ctypes.c_int()
+        k = ctypes.c_int64()
+        call("bfvm_batch_get_plan", self._h, ctypes.byref(g), ctypes.byref(k))
+        return g.value, k.value
+
+    def synchronize(self) -> None:
+        call("bfvm_batch_synchronize", self._h)

@@ -1,0 +1,614 @@
+// Many independent microenvironments advanced together (libbfvm.so).
+//
+// A bfvm_batch holds non-owning references to bfvm_solver instances of one
+// device and one precision.  bfvm_batch_step(b, dt, n, flags) has the effect
+// of bfvm_step(m, dt, n, flags) on every instance: per instance the Thomas
+// setup is done once from its first dt (BioFVM_solvers.cpp:87,172), and a
+// step is bulk -> cells -> Dirichlet, x sweep, Dirichlet, y sweep,
+// Dirichlet, z sweep (BioFVM_solvers.cpp:175-273).
+//
+// Scheduling.  The instances are packed, in the order they were added, into
+// groups whose density fields together stay within a byte budget (by
+// default a fraction of the L2 cache), and all n steps of one group run
+// before the next group starts: a group small enough for L2 keeps its fields
+// on chip across the three sweeps of a step and from step to step.  Within a
+// group every phase of a step is one launch over all of the group's
+// instances (the kernels of bfvm_batch_kernels.cuh).  The whole sequence --
+// groups x steps x phases -- is captured once into a CUDA graph and replayed
+// by one graph launch per call; the graph is rebuilt only when the plan
+// changes (instances, their lists or device buffers, dt, n, flags, tuning).
+//
+// The tuner (bfvm_batch_tune) picks, per axis, the chunk length (points per
+// thread) and threads per block, then the group budget, by timing short
+// graph runs on the instances' own fields, which it saves before and
+// restores after.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "bfvm.h"
+#include "bfvm_batch_kernels.cuh"
+#include "bfvm_state.h"
+
+namespace bfvm_rt {
+namespace {
+
+struct BatchConfig {
+  int ch[3] = {0, 0, 0};       // 0 = choose from the longest line
+  int threads[3] = {0, 0, 0};  // 0 = choose
+  int64_t group_bytes = -1;    // -1 = default (half of L2), 0 = one group
+};
+
+// Device descriptors of one group, all in one buffer.
+struct GroupPlan {
+  int64_t field_bytes = 0;
+  size_t off_sweep[3] = {0, 0, 0}, off_bulk = 0, off_cells = 0, off_dir = 0;
+  int n_sweep[3] = {0, 0, 0}, n_bulk = 0, n_cells = 0, n_dir = 0;
+  int64_t items[3] = {0, 0, 0};
+  int64_t work_bulk = 0, work_cells = 0, work_dir = 0;
+};
+
+}  // namespace
+}  // namespace bfvm_rt
+
+struct bfvm_batch {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev = nullptr;
+  std::vector<bfvm_solver*> inst;
+  bfvm_rt::BatchConfig cfg;
+  int l2_bytes = 0;
+  // current plan
+  std::vector<unsigned char> host_desc;  // descriptor bytes of every group
+  std::vector<bfvm_rt::GroupPlan> groups;
+  int ch[3] = {16, 16, 16}, threads[3] = {256, 256, 256};
+  bfvm_rt::DevBuf d_desc;
+  // cached graph and what it was captured for
+  cudaGraphExec_t exec = nullptr;
+  std::string key;
+  int64_t graph_kernels = 0;
+};
+
+namespace bfvm_rt {
+namespace {
+
+using namespace bfvm;
+
+template <typename T>
+void append(std::vector<unsigned char>& buf, const T& v) {
+  const size_t o = buf.size();
+  buf.resize(o + sizeof(T));
+  std::memcpy(buf.data() + o, &v, sizeof(T));
+}
+
+void align_to(std::vector<unsigned char>& buf, size_t a) {
+  buf.resize((buf.size() + a - 1) / a * a, 0);
+}
+
+int axis_len(const bfvm_solver* m, int a) { return a == 0 ? m->nx : (a == 1 ? m->ny : m->nz); }
+
+// Chunk length and threads per block valid for every instance: a work item
+// holds all chunks of its lines, at least 32 columns wide.
+bool config_fits(const bfvm_batch* b, int a, int ch, int threads) {
+  if (threads > batch_max_threads(ch)) return false;
+  for (const bfvm_solver* m : b->inst) {
+    const int nc = (axis_len(m, a) + ch - 1) / ch;
+    if (nc * 32 > threads) return false;
+  }
+  return true;
+}
+
+void choose_shapes(bfvm_batch* b) {
+  for (int a = 0; a < 3; ++a) {
+    int ch = b->cfg.ch[a], th = b->cfg.threads[a];
+    if (ch && th) {
+      require(config_fits(b, a, ch, th),
+              "batch config: chunk " + std::to_string(ch) + " x " + std::to_string(th) +
+                  " threads cannot hold the longest line of axis " + std::to_string(a));
+    } else {
+      ch = 0;
+      for (int c : {16, 32, 8})
+        for (int t : {256, 512})
+          if (!ch && config_fits(b, a, c, t)) ch = c, th = t;
+      require(ch != 0, "batch: an axis is longer than 512 x 32 points");
+    }
+    b->ch[a] = ch;
+    b->threads[a] = th;
+  }
+}
+
+template <typename T>
+BatchSweep<T> sweep_desc(const bfvm_solver* m, int a, int ch, int threads, int64_t first) {
+  BatchSweep<T> d;
+  std::memset(&d, 0, sizeof d);  // the bytes also key the graph cache
+  const int64_t nx = m->nx, ny = m->ny, nz = m->nz, S = m->S;
+  d.p = m->p.as<T>();
+  d.coef = coef_view<T>(m, a);
+  d.S = m->S;
+  if (a == 0) {
+    d.n = (int)nx;
+    d.C = S;
+    d.outer_stride = nx * S;
+    d.line_stride = S;
+    d.ncols = ny * nz * S;
+  } else if (a == 1) {
+    d.n = (int)ny;
+    d.C = nx * S;
+    d.outer_stride = nx * ny * S;
+    d.line_stride = nx * S;
+    d.ncols = nz * nx * S;
+  } else {
+    d.n = (int)nz;
+    d.C = nx * ny * S;
+    d.outer_stride = 0;
+    d.line_stride = nx * ny * S;
+    d.ncols = nx * ny * S;
+  }
+  d.nchunks = (d.n + ch - 1) / ch;
+  d.tw = std::max(32, threads / d.nchunks / 32 * 32);
+  d.first = first;
+  return d;
+}
+
+// Instances packed in order into groups of at most `budget` field bytes (a
+// single instance larger than the budget is a group of its own).
+std::vector<std::vector<bfvm_solver*>> make_groups(const bfvm_batch* b, int64_t budget) {
+  std::vector<std::vector<bfvm_solver*>> g;
+  int64_t cur = 0;
+  for (bfvm_solver* m : b->inst) {
+    const int64_t bytes = (int64_t)(m->NS() * m->elem());
+    if (g.empty() || (budget > 0 && cur + bytes > budget)) {
+      g.emplace_back();
+      cur = 0;
+    }
+    g.back().push_back(m);
+    cur += bytes;
+  }
+  return g;
+}
+
+template <typename T>
+void build_plan(bfvm_batch* b) {
+  const int64_t budget = b->cfg.group_bytes < 0 ? (int64_t)b->l2_bytes / 2 : b->cfg.group_bytes;
+  auto groups = make_groups(b, budget);
+  std::vector<unsigned char>& buf = b->host_desc;
+  buf.clear();
+  b->groups.clear();
+  for (auto& members : groups) {
+    GroupPlan G;
+    std::memset(&G, 0, sizeof G);
+    for (bfvm_solver* m : members) G.field_bytes += (int64_t)(m->NS() * m->elem());
+    for (int a = 0; a < 3; ++a) {
+      align_to(buf, 64);
+      G.off_sweep[a] = buf.size();
+      int64_t first = 0;
+      for (bfvm_solver* m : members) {
+        BatchSweep<T> d = sweep_desc<T>(m, a, b->ch[a], b->threads[a], first);
+        if (d.ncols == 0) continue;
+        first += (d.ncols + d.tw - 1) / d.tw;
+        append(buf, d);
+        G.n_sweep[a]++;
+      }
+      G.items[a] = first;
+    }
+    auto lists = [&](size_t& off, int& n, int64_t& work, auto fill) {
+      align_to(buf, 64);
+      off = buf.size();
+      for (bfvm_solver* m : members) {
+        BatchList<T> L;
+        std::memset(&L, 0, sizeof L);
+        L.p = m->p.as<T>();
+        L.S = m->S;
+        if (!fill(m, L) || L.count == 0) continue;
+        L.first = work;
+        work += L.count * m->S;
+        append(buf, L);
+        n++;
+      }
+    };
+    lists(G.off_bulk, G.n_bulk, G.work_bulk, [](bfvm_solver* m, BatchList<T>& L) {
+      L.count = (int64_t)m->bulk_vox.size();
+      L.vox = m->d_bulk_vox.as<int64_t>();
+      L.a = m->d_bulk_st.as<double>();
+      L.b = m->d_bulk_su.as<double>();
+      return true;
+    });
+    lists(G.off_cells, G.n_cells, G.work_cells, [](bfvm_solver* m, BatchList<T>& L) {
+      L.count = m->n_agents;
+      L.key = m->d_ag_key.as<uint64_t>();
+      L.idx = m->d_ag_idx.as<int>();
+      L.a = m->d_ag_t1.as<double>();
+      L.b = m->d_ag_t2.as<double>();
+      return true;
+    });
+    lists(G.off_dir, G.n_dir, G.work_dir, [](bfvm_solver* m, BatchList<T>& L) {
+      L.count = m->dir_unique;
+      L.vox = m->d_dir_vox.as<int64_t>();
+      L.a = m->d_dir_val.as<double>();
+      return true;
+    });
+    b->groups.push_back(G);
+  }
+  align_to(buf, 64);
+}
+
+template <typename T>
+void launch_sweep_group(bfvm_batch* b, const GroupPlan& G, int a, int64_t* kernels) {
+  if (G.items[a] == 0) return;
+  const auto* sw = reinterpret_cast<const BatchSweep<T>*>(b->d_desc.as<unsigned char>() +
+                                                          G.off_sweep[a]);
+  const int th = b->threads[a];
+  const size_t smem = 4 * sizeof(T) * (size_t)th;
+  const dim3 grid((unsigned)G.items[a]);
+  switch (b->ch[a]) {
+    case 8: lod_batch_sweep_kernel<T, 8><<<grid, th, smem, b->stream>>>(sw, G.n_sweep[a]); break;
+    case 16: lod_batch_sweep_kernel<T, 16><<<grid, th, smem, b->stream>>>(sw, G.n_sweep[a]); break;
+    case 32: lod_batch_sweep_kernel<T, 32><<<grid, th, smem, b->stream>>>(sw, G.n_sweep[a]); break;
+    default: throw Error(BFVM_ERR_STATE, "unsupported batch chunk length");
+  }
+  BFVM_CUDA(cudaGetLastError());
+  ++*kernels;
+}
+
+template <typename T>
+void launch_dirichlet_group(bfvm_batch* b, const GroupPlan& G, int64_t* kernels) {
+  if (G.work_dir == 0) return;
+  const auto* L =
+      reinterpret_cast<const BatchList<T>*>(b->d_desc.as<unsigned char>() + G.off_dir);
+  batch_dirichlet_kernel<T><<<(unsigned)blocks_for(G.work_dir, 256), 256, 0, b->stream>>>(
+      L, G.n_dir, G.work_dir);
+  BFVM_CUDA(cudaGetLastError());
+  ++*kernels;
+}
+
+// One step of one group; `axes` limits the sweeps (the tuner times one axis).
+template <typename T>
+void enqueue_group_step(bfvm_batch* b, const GroupPlan& G, double dt, int flags, int axes,
+                        int64_t* kernels) {
+  unsigned char* base = b->d_desc.as<unsigned char>();
+  if ((flags & BFVM_STEP_BULK) && G.work_bulk) {
+    const auto* L = reinterpret_cast<const BatchList<T>*>(base + G.off_bulk);
+    batch_bulk_kernel<T><<<(unsigned)blocks_for(G.work_bulk, 256), 256, 0, b->stream>>>(
+        L, G.n_bulk, G.work_bulk, dt);
+    BFVM_CUDA(cudaGetLastError());
+    ++*kernels;
+  }
+  if ((flags & BFVM_STEP_CELLS) && G.work_cells) {
+    const auto* L = reinterpret_cast<const BatchList<T>*>(base + G.off_cells);
+    batch_cells_kernel<T><<<(unsigned)blocks_for(G.work_cells, 256), 256, 0, b->stream>>>(
+        L, G.n_cells, G.work_cells);
+    BFVM_CUDA(cudaGetLastError());
+    ++*kernels;
+  }
+  if (!(flags & BFVM_STEP_DIFFUSION)) return;
+  for (int a = 0; a < 3; ++a) {
+    if (!(axes & (1 << a))) continue;
+    launch_dirichlet_group<T>(b, G, kernels);
+    launch_sweep_group<T>(b, G, a, kernels);
+  }
+}
+
+// Makes every instance ready for a step (Thomas setup from this dt when not
+// yet done, lists on the device) and orders the batch stream after the work
+// already queued on the instances' own streams.
+void prepare_instances(bfvm_batch* b, double dt) {
+  for (bfvm_solver* m : b->inst) {
+    DeviceGuard dg(m->device);
+    check_lod_mesh(m);
+    require(m->lod_dims == 3, "batch: instance is inside a LOD_2D step", BFVM_ERR_STATE);
+    if (!m->setup_done) thomas_setup(m, dt);
+    build_all(m);
+    BFVM_CUDA(cudaEventRecord(b->ev, m->stream));
+    BFVM_CUDA(cudaStreamWaitEvent(b->stream, b->ev, 0));
+  }
+}
+
+// Later work on the instances' streams waits for the batch.
+void release_instances(bfvm_batch* b) {
+  BFVM_CUDA(cudaEventRecord(b->ev, b->stream));
+  for (bfvm_solver* m : b->inst) BFVM_CUDA(cudaStreamWaitEvent(m->stream, b->ev, 0));
+}
+
+bool fp64(const bfvm_batch* b) { return b->inst.empty() || b->inst[0]->precision == BFVM_FP64; }
+
+void plan(bfvm_batch* b) {
+  choose_shapes(b);
+  if (fp64(b))
+    build_plan<double>(b);
+  else
+    build_plan<float>(b);
+  b->d_desc.ensure(std::max<size_t>(b->host_desc.size(), 64));
+  BFVM_CUDA(cudaMemcpyAsync(b->d_desc.ptr, b->host_desc.data(), b->host_desc.size(),
+                            cudaMemcpyHostToDevice, b->stream));
+}
+
+void drop_graph(bfvm_batch* b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  b->exec = nullptr;
+  b->key.clear();
+}
+
+// Captures groups x nsteps x phases into one graph executable.
+cudaGraphExec_t capture(bfvm_batch* b, double dt, int nsteps, int flags, int axes,
+                        int64_t* kernels) {
+  *kernels = 0;
+  cudaGraph_t graph = nullptr;
+  BFVM_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+  try {
+    for (const GroupPlan& G : b->groups)
+      for (int it = 0; it < nsteps; ++it) {
+        if (fp64(b))
+          enqueue_group_step<double>(b, G, dt, flags, axes, kernels);
+        else
+          enqueue_group_step<float>(b, G, dt, flags, axes, kernels);
+      }
+  } catch (...) {
+    cudaStreamEndCapture(b->stream, &graph);
+    if (graph) cudaGraphDestroy(graph);
+    throw;
+  }
+  BFVM_CUDA(cudaStreamEndCapture(b->stream, &graph));
+  cudaGraphExec_t exec = nullptr;
+  const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  BFVM_CUDA(e);
+  return exec;
+}
+
+std::string plan_key(const bfvm_batch* b, double dt, int nsteps, int flags) {
+  std::string k(reinterpret_cast<const char*>(b->host_desc.data()), b->host_desc.size());
+  k.append(reinterpret_cast<const char*>(&dt), sizeof dt);
+  k.append(reinterpret_cast<const char*>(&nsteps), sizeof nsteps);
+  k.append(reinterpret_cast<const char*>(&flags), sizeof flags);
+  k.append(reinterpret_cast<const char*>(b->ch), sizeof b->ch);
+  k.append(reinterpret_cast<const char*>(b->threads), sizeof b->threads);
+  for (const GroupPlan& G : b->groups) k.append(reinterpret_cast<const char*>(&G), sizeof G);
+  return k;
+}
+
+void batch_step(bfvm_batch* b, double dt, int nsteps, int flags) {
+  require(nsteps >= 0, "negative step count");
+  require((flags & ~BFVM_STEP_ALL) == 0, "unknown step flags");
+  if (b->inst.empty() || nsteps == 0) return;
+  prepare_instances(b, dt);
+  plan(b);
+  const std::string key = plan_key(b, dt, nsteps, flags);
+  if (!b->exec || key != b->key) {
+    drop_graph(b);
+    b->exec = capture(b, dt, nsteps, flags, 7, &b->graph_kernels);
+    b->key = key;
+  }
+  BFVM_CUDA(cudaGraphLaunch(b->exec, b->stream));
+  release_instances(b);
+}
+
+// Times `reps` replays of a graph of `steps` steps (or one axis's sweeps),
+// returning the best milliseconds per replay.
+float time_graph(bfvm_batch* b, double dt, int steps, int flags, int axes) {
+  int64_t k = 0;
+  cudaGraphExec_t exec = capture(b, dt, steps, flags, axes, &k);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  float best = 1e30f;
+  try {
+    BFVM_CUDA(cudaEventCreate(&e0));
+    BFVM_CUDA(cudaEventCreate(&e1));
+    BFVM_CUDA(cudaGraphLaunch(exec, b->stream));  // warm-up
+    for (int r = 0; r < 3; ++r) {
+      BFVM_CUDA(cudaEventRecord(e0, b->stream));
+      BFVM_CUDA(cudaGraphLaunch(exec, b->stream));
+      BFVM_CUDA(cudaEventRecord(e1, b->stream));
+      BFVM_CUDA(cudaEventSynchronize(e1));
+      float ms = 0;
+      BFVM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      best = std::min(best, ms);
+    }
+  } catch (...) {
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaGraphExecDestroy(exec);
+    throw;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaGraphExecDestroy(exec);
+  return best;
+}
+
+void batch_tune(bfvm_batch* b, double dt, int flags, int trial_steps) {
+  require(trial_steps >= 1 && trial_steps <= 1000, "trial_steps must be in [1, 1000]");
+  if (b->inst.empty()) return;
+  prepare_instances(b, dt);
+  // save the fields; the trial runs advance them
+  size_t total = 0;
+  for (bfvm_solver* m : b->inst) total += (m->NS() * m->elem() + 255) / 256 * 256;
+  DevBuf save;
+  save.ensure(std::max<size_t>(total, 16));
+  auto copy_fields = [&](bool to_save) {
+    size_t o = 0;
+    for (bfvm_solver* m : b->inst) {
+      const size_t bytes = m->NS() * m->elem();
+      unsigned char* s = save.as<unsigned char>() + o;
+      BFVM_CUDA(cudaMemcpyAsync(to_save ? s : m->p.ptr, to_save ? m->p.ptr : s, bytes,
+                                cudaMemcpyDeviceToDevice, b->stream));
+      o += (bytes + 255) / 256 * 256;
+    }
+  };
+  copy_fields(true);
+  const BatchConfig user = b->cfg;
+  drop_graph(b);
+  try {
+    // 1. per axis: chunk length x threads, sweeps alone, every instance in one group
+    BatchConfig best = user;
+    best.group_bytes = 0;
+    for (int a = 0; a < 3; ++a) {
+      float best_ms = 1e30f;
+      for (int ch : {8, 16, 32})
+        for (int th : {128, 256, 512}) {
+          if (!config_fits(b, a, ch, th)) continue;
+          b->cfg = best;
+          b->cfg.ch[a] = ch;
+          b->cfg.threads[a] = th;
+          plan(b);
+          const float ms = time_graph(b, dt, trial_steps, BFVM_STEP_DIFFUSION, 1 << a);
+          if (ms < best_ms) {
+            best_ms = ms;
+            best.ch[a] = ch;
+            best.threads[a] = th;
+          }
+        }
+    }
+    // 2. the group budget, whole steps
+    float best_ms = 1e30f;
+    int64_t best_budget = 0;
+    for (int64_t budget : {(int64_t)0, (int64_t)b->l2_bytes, (int64_t)b->l2_bytes / 2,
+                           (int64_t)b->l2_bytes / 4, (int64_t)b->l2_bytes / 8}) {
+      b->cfg = best;
+      b->cfg.group_bytes = budget;
+      plan(b);
+      const float ms = time_graph(b, dt, trial_steps, flags, 7);
+      if (ms < best_ms) {
+        best_ms = ms;
+        best_budget = budget;
+      }
+    }
+    best.group_bytes = best_budget;
+    b->cfg = best;
+  } catch (...) {
+    b->cfg = user;
+    copy_fields(false);
+    cudaStreamSynchronize(b->stream);
+    throw;
+  }
+  copy_fields(false);
+  BFVM_CUDA(cudaStreamSynchronize(b->stream));
+  release_instances(b);
+}
+
+#define BATCH_CALL(b, ...)                           \
+  guarded([&] {                                      \
+    require((b) != nullptr, "null batch handle");    \
+    DeviceGuard dg_((b)->device);                    \
+    __VA_ARGS__;                                     \
+  })
+
+}  // namespace
+}  // namespace bfvm_rt
+
+using namespace bfvm_rt;
+
+extern "C" {
+
+int bfvm_batch_create(bfvm_batch** out, int device) {
+  return guarded([&] {
+    require(out != nullptr, "null output pointer");
+    int ndev = 0;
+    BFVM_CUDA(cudaGetDeviceCount(&ndev));
+    require(device >= 0 && device < ndev, "no CUDA device " + std::to_string(device));
+    DeviceGuard dg(device);
+    bfvm_batch* b = new bfvm_batch;
+    b->device = device;
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->ev, cudaEventDisableTiming) != cudaSuccess) {
+      if (b->stream) cudaStreamDestroy(b->stream);
+      delete b;
+      throw Error(BFVM_ERR_CUDA, "batch stream/event creation failed");
+    }
+    cudaDeviceGetAttribute(&b->l2_bytes, cudaDevAttrL2CacheSize, device);
+    *out = b;
+  });
+}
+
+int bfvm_batch_destroy(bfvm_batch* b) {
+  if (!b) return BFVM_OK;
+  return BATCH_CALL(b, {
+    cudaStreamSynchronize(b->stream);
+    drop_graph(b);
+    b->d_desc.release();
+    cudaEventDestroy(b->ev);
+    cudaStreamDestroy(b->stream);
+    delete b;
+  });
+}
+
+int bfvm_batch_add(bfvm_batch* b, bfvm_solver* m) {
+  return BATCH_CALL(b, {
+    require(m != nullptr, "null solver handle");
+    require(m->device == b->device, "instance lives on another device");
+    require(b->inst.empty() || m->precision == b->inst[0]->precision,
+            "instances of one batch must share the precision");
+    require(std::find(b->inst.begin(), b->inst.end(), m) == b->inst.end(),
+            "instance already in the batch");
+    b->inst.push_back(m);
+  });
+}
+
+int bfvm_batch_clear(bfvm_batch* b) {
+  return BATCH_CALL(b, {
+    cudaStreamSynchronize(b->stream);
+    b->inst.clear();
+    drop_graph(b);
+  });
+}
+
+int bfvm_batch_size(bfvm_batch* b, int* count) {
+  return BATCH_CALL(b, {
+    require(count != nullptr, "null output pointer");
+    *count = (int)b->inst.size();
+  });
+}
+
+int bfvm_batch_step(bfvm_batch* b, double dt, int nsteps, int flags) {
+  return BATCH_CALL(b, batch_step(b, dt, nsteps, flags));
+}
+
+int bfvm_batch_tune(bfvm_batch* b, double dt, int flags, int trial_steps) {
+  return BATCH_CALL(b, batch_tune(b, dt, flags, trial_steps));
+}
+
+int bfvm_batch_set_config(bfvm_batch* b, const int* chunk, const int* threads,
+                          int64_t group_bytes) {
+  return BATCH_CALL(b, {
+    require(group_bytes >= -1, "group_bytes must be -1 (default), 0 (one group) or positive");
+    BatchConfig c;
+    for (int a = 0; a < 3; ++a) {
+      c.ch[a] = chunk ? chunk[a] : 0;
+      c.threads[a] = threads ? threads[a] : 0;
+      require(c.ch[a] == 0 || c.ch[a] == 8 || c.ch[a] == 16 || c.ch[a] == 32,
+              "chunk must be 0, 8, 16 or 32");
+      require(c.threads[a] == 0 || c.threads[a] == 128 || c.threads[a] == 256 ||
+                  c.threads[a] == 512,
+              "threads must be 0, 128, 256 or 512");
+      require((c.ch[a] == 0) == (c.threads[a] == 0), "chunk and threads are set together");
+    }
+    c.group_bytes = group_bytes;
+    b->cfg = c;
+  });
+}
+
+int bfvm_batch_get_config(bfvm_batch* b, int* chunk, int* threads, int64_t* group_bytes) {
+  return BATCH_CALL(b, {
+    if (!b->inst.empty()) choose_shapes(b);
+    for (int a = 0; a < 3; ++a) {
+      if (chunk) chunk[a] = b->ch[a];
+      if (threads) threads[a] = b->threads[a];
+    }
+    if (group_bytes)
+      *group_bytes = b->cfg.group_bytes < 0 ? (int64_t)b->l2_bytes / 2 : b->cfg.group_bytes;
+  });
+}
+
+int bfvm_batch_get_plan(bfvm_batch* b, int* groups, int64_t* kernels_per_call) {
+  return BATCH_CALL(b, {
+    if (groups) *groups = (int)b->groups.size();
+    if (kernels_per_call) *kernels_per_call = b->exec ? b->graph_kernels : 0;
+  });
+}
+
+int bfvm_batch_synchronize(bfvm_batch* b) {
+  return BATCH_CALL(b, BFVM_CUDA(cudaStreamSynchronize(b->stream)));
+}
+
+}  // extern "C"

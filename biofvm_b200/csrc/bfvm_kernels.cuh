@@ -272,21 +272,40 @@ __global__ void bulk_kernel(T* __restrict__ p, int S, int64_t E, const int64_t* 
   p[q] = (T)bulk_update((double)p[q], st[t], su[t], dt);
 }
 
-// simulate_cell_sources_and_sinks: one thread per (voxel group, substrate);
-// the agents of a group are applied in list order.
+// simulate_cell_sources_and_sinks over the agents sorted by voxel (key[r] =
+// voxel of the r-th sorted agent, idx[r] = its position in the agent list;
+// the sort is stable).  One thread per (sorted agent, substrate): the thread
+// of the first agent of each voxel applies all agents of that voxel in list
+// order, the others return.  t1/t2 are [A][S] in list order.
 template <typename T>
-__global__ void cells_kernel(T* __restrict__ p, int S, int64_t G, const int64_t* __restrict__ gvoxel,
-                             const int* __restrict__ gstart, const double* __restrict__ t1,
+__global__ void cells_kernel(T* __restrict__ p, int S, int64_t A, const uint64_t* __restrict__ key,
+                             const int* __restrict__ idx, const double* __restrict__ t1,
                              const double* __restrict__ t2) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= G * S) return;
-  const int64_t g = t / S;
-  const int s = (int)(t - g * S);
-  const int64_t q = gvoxel[g] * S + s;
+  if (t >= A * S) return;
+  const int64_t r = t / S;
+  const int s = (int)(t - r * S);
+  const uint64_t v = key[r];
+  if (r > 0 && key[r - 1] == v) return;
+  const int64_t q = (int64_t)v * S + s;
   double x = (double)p[q];
-  for (int e = gstart[g]; e < gstart[g + 1]; ++e)
-    x = cell_update(x, t1[(int64_t)e * S + s], t2[(int64_t)e * S + s]);
+  for (int64_t e = r; e < A && key[e] == v; ++e) {
+    const int64_t a = idx[e];
+    x = cell_update(x, t1[a * S + s], t2[a * S + s]);
+  }
   p[q] = (T)x;
+}
+
+static __global__ void iota_kernel(int* __restrict__ out, int64_t n) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) out[t] = (int)t;
+}
+
+// a[r][col] = v for r < rows (row pitch `pitch` elements)
+static __global__ void fill_column_kernel(double* __restrict__ a, int64_t rows, int pitch, int col,
+                                   double v) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < rows) a[t * pitch + col] = v;
 }
 
 // apply_dirichlet_conditions over the de-duplicated node list.

@@ -16,79 +16,15 @@
 #include "bfvm_host_math.h"
 #include "bfvm_kernels.cuh"
 #include "bfvm_kernels_tma.cuh"
+#include <cub/device/device_radix_sort.cuh>
 #include <cudaTypedefs.h>
 #include <mutex>
 
-namespace {
+#include "bfvm_state.h"
+
+namespace bfvm_rt {
 
 thread_local std::string g_last_error;
-
-struct Error : std::runtime_error {
-  int code;
-  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
-};
-
-#define BFVM_CUDA(call)                                                                   \
-  do {                                                                                    \
-    cudaError_t e_ = (call);                                                              \
-    if (e_ != cudaSuccess)                                                                \
-      throw Error(e_ == cudaErrorMemoryAllocation ? BFVM_ERR_NOMEM : BFVM_ERR_CUDA,       \
-                  std::string(#call) + ": " + cudaGetErrorString(e_));                    \
-  } while (0)
-
-void require(bool ok, const std::string& msg, int code = BFVM_ERR_ARG) {
-  if (!ok) throw Error(code, msg);
-}
-
-// A growable device allocation.
-struct DevBuf {
-  void* ptr = nullptr;
-  size_t bytes = 0;
-  void ensure(size_t nbytes) {
-    if (nbytes <= bytes && ptr) return;
-    release();
-    if (nbytes == 0) return;
-    BFVM_CUDA(cudaMalloc(&ptr, nbytes));
-    bytes = nbytes;
-  }
-  void release() {
-    if (ptr) cudaFree(ptr);
-    ptr = nullptr;
-    bytes = 0;
-  }
-  template <typename T>
-  T* as() const {
-    return static_cast<T*>(ptr);
-  }
-};
-
-template <typename T>
-void upload(DevBuf& b, const std::vector<T>& v, cudaStream_t st) {
-  b.ensure(std::max<size_t>(v.size() * sizeof(T), 16));
-  if (!v.empty())
-    BFVM_CUDA(cudaMemcpyAsync(b.ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
-}
-
-// Device copy of a segment list (see SegList in bfvm_kernels.cuh).
-struct DevSegList {
-  DevBuf off, pos, a, b;
-  bool present = false;
-  bfvm::SegList view() const {
-    bfvm::SegList L;
-    L.off = off.as<int>();
-    L.pos = pos.as<int>();
-    L.a = a.as<double>();
-    L.b = b.as<double>();
-    return L;
-  }
-  void release() {
-    off.release();
-    pos.release();
-    a.release();
-    b.release();
-    present = false;
-  }
-};
 
 // Groups entries (already in non-decreasing (line, pos) order) by
 // (line, chunk) segment.
@@ -98,90 +34,6 @@ std::vector<int> segment_offsets(int64_t nlines, int nchunks, int ch,
   for (size_t e = 0; e < line.size(); ++e) off[(size_t)(line[e] * nchunks + pos[e] / ch) + 1]++;
   for (size_t i = 1; i < off.size(); ++i) off[i] += off[i - 1];
   return off;
-}
-
-struct Axis {
-  int ch = 16;  // points per thread
-  int tw = 32;  // columns per block
-  int minb = 1; // resident blocks per SM the kernel is compiled for (1 or 2)
-  bool user = false;  // set through bfvm_set_sweep_config
-};
-
-}  // namespace
-
-struct bfvm_solver {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  int64_t launches = 0;
-
-  // mesh (Cartesian_Mesh, BioFVM_mesh.h:146-188)
-  int nx = 1, ny = 1, nz = 1;
-  double dx = 1, dy = 1, dz = 1, dV = 1;
-  double bbox[6] = {-0.5, -0.5, -0.5, 0.5, 0.5, 0.5};
-  bool uniform = true;
-
-  // densities
-  int S = 1;
-  std::vector<double> D{0.0}, decay{0.0};
-  int precision = BFVM_FP64;
-  DevBuf p;
-
-  // Thomas coefficients (computed once, BioFVM_solvers.cpp:87,172)
-  bool setup_done = false;
-  DevBuf coef[3];  // per axis: inv_den, fwd, bwd [n*S] then c1 [S], in the sweep precision
-  std::vector<double> h_c1[3], h_den[3], h_cx[3];  // FP64 host copies per axis
-  DevBuf chunk[3];     // per axis: chunk tables k1, kg, kc by slot (sweep precision)
-  DevBuf chunk_slots[3];  // per axis: slot of every chunk
-  int chunk_ch[3] = {0, 0, 0};
-  int chunk_nslots[3] = {0, 0, 0};
-  Axis axis[3];
-
-  // bulk sources/sinks: non-identity voxels, ascending
-  std::vector<int64_t> bulk_vox;
-  std::vector<double> bulk_st, bulk_su;
-  bool bulk_dirty = true;
-  DevBuf d_bulk_vox, d_bulk_st, d_bulk_su;
-  DevSegList seg_bulk;
-
-  // Dirichlet nodes in insertion order (BioFVM_microenvironment.h:102-103)
-  std::vector<int64_t> dir_vox;
-  std::vector<double> dir_val;
-  bool dir_dirty = true;
-  int64_t dir_unique = 0;
-  DevBuf d_dir_vox, d_dir_val;
-  DevSegList seg_dir_x, seg_dir_y;
-
-  // agents in list order
-  std::vector<int64_t> ag_vox;
-  std::vector<double> ag_t1, ag_t2;
-  bool ag_dirty = true;
-  int64_t n_groups = 0;
-  DevBuf d_ag_vox_orig, d_group_vox, d_group_start, d_gather;
-  DevSegList seg_cells;
-
-  // device status word: set to non-zero by a kernel whose bounded wait failed
-  DevBuf d_status;
-  int num_sms = 148;
-  int path = 0;  // BFVM_PATH_*
-  int fuse_sources = 0;  // bulk/cell updates in the x sweep's prologue
-  int lod_dims = 3;      // 2 while a LOD_2D step runs: sweeps of the z = 0 plane only
-  // cached tensor maps of the y and z sweeps (keyed by field pointer)
-  CUtensorMap maps[3];
-  const void* map_key[3] = {nullptr, nullptr, nullptr};
-  int map_w[3] = {0, 0, 0};
-
-  int64_t N() const { return (int64_t)nx * ny * nz; }
-  int64_t NS() const { return N() * S; }
-  size_t elem() const { return precision == BFVM_FP64 ? sizeof(double) : sizeof(float); }
-};
-
-namespace {
-
-int64_t blocks_for(int64_t work, int threads) { return (work + threads - 1) / threads; }
-
-void check_launch(bfvm_solver* m) {
-  m->launches++;
-  BFVM_CUDA(cudaGetLastError());
 }
 
 // Chunk length CH (points per thread) and block width TW (columns per block)
@@ -218,10 +70,8 @@ void clear_state_after_resize(bfvm_solver* m) {
   m->dir_vox.clear();
   m->dir_val.clear();
   m->dir_dirty = true;
-  m->ag_vox.clear();
-  m->ag_t1.clear();
-  m->ag_t2.clear();
-  m->ag_dirty = true;
+  m->n_agents = 0;
+  m->ag_dirty = m->ag_seg_dirty = true;
   for (auto& A : m->axis) A.user = false;
   choose_axes(m);
 }
@@ -342,18 +192,6 @@ bfvm::ChunkCoef<T> chunk_view(bfvm_solver* m, int a) {
   return c;
 }
 
-template <typename T>
-bfvm::AxisCoef<T> coef_view(const bfvm_solver* m, int a) {
-  const int ns[3] = {m->nx, m->ny, m->nz};
-  const size_t nS = (size_t)ns[a] * m->S;
-  const T* base = m->coef[a].as<T>();
-  bfvm::AxisCoef<T> c;
-  c.inv_den = base;
-  c.fwd = base + nS;
-  c.bwd = base + 2 * nS;
-  c.c1 = base + 3 * nS;
-  return c;
-}
 
 // ---- host lists -> device ---------------------------------------------------
 
@@ -455,58 +293,107 @@ void build_dirichlet(bfvm_solver* m) {
   m->dir_dirty = false;
 }
 
+// Agents stably sorted by voxel on the device (radix sort of (voxel, list
+// position) pairs; a radix sort is stable, so agents of one voxel keep their
+// list order, BioFVM_microenvironment.cpp:626-633).
 void build_agents(bfvm_solver* m) {
   if (!m->ag_dirty) return;
+  const int64_t A = m->n_agents;
+  m->ag_dirty = false;
+  if (A == 0) return;
   cudaStream_t st = m->stream;
+  m->d_ag_key.ensure(A * sizeof(uint64_t));
+  m->d_ag_idx_in.ensure(A * sizeof(int));
+  m->d_ag_idx.ensure(A * sizeof(int));
+  bfvm::iota_kernel<<<(unsigned)blocks_for(A, 256), 256, 0, st>>>(m->d_ag_idx_in.as<int>(), A);
+  check_launch(m);
+  int end_bit = 1;
+  while (end_bit < 63 && ((int64_t)1 << end_bit) < m->N()) ++end_bit;
+  // voxel indices were checked to lie in [0, N): as unsigned keys they sort
+  // like the signed values
+  const uint64_t* keys_in = m->d_ag_vox_orig.as<uint64_t>();
+  size_t tmp = 0;
+  BFVM_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, keys_in, m->d_ag_key.as<uint64_t>(),
+                                            m->d_ag_idx_in.as<int>(), m->d_ag_idx.as<int>(),
+                                            (int)A, 0, end_bit, st));
+  m->d_sort_tmp.ensure(std::max<size_t>(tmp, 16));
+  BFVM_CUDA(cub::DeviceRadixSort::SortPairs(m->d_sort_tmp.ptr, tmp, keys_in,
+                                            m->d_ag_key.as<uint64_t>(), m->d_ag_idx_in.as<int>(),
+                                            m->d_ag_idx.as<int>(), (int)A, 0, end_bit, st));
+}
+
+// Segment lists of the agents for the fused x-sweep prologue: entries grouped
+// by (x line, chunk), each group in sorted (voxel, list) order.  Built on the
+// host from the device copy; only the fused-sources path uses them.
+void build_agent_segments(bfvm_solver* m) {
+  if (!m->ag_seg_dirty) return;
   const int S = m->S;
-  const int64_t A = (int64_t)m->ag_vox.size();
+  const int64_t A = m->n_agents;
+  m->ag_seg_dirty = false;
   if (A == 0) {
     m->seg_cells.present = false;
-    m->n_groups = 0;
-    m->ag_dirty = false;
     return;
   }
-  // Stable order by voxel keeps list order among agents of one voxel.
-  std::vector<int64_t> order(A);
-  std::iota(order.begin(), order.end(), 0);
-  std::stable_sort(order.begin(), order.end(),
-                   [&](int64_t a, int64_t b) { return m->ag_vox[a] < m->ag_vox[b]; });
+  build_agents(m);
+  cudaStream_t st = m->stream;
+  std::vector<uint64_t> key(A);
+  std::vector<int> idx(A);
+  std::vector<double> t1_in((size_t)A * S), t2_in((size_t)A * S);
+  BFVM_CUDA(cudaMemcpyAsync(key.data(), m->d_ag_key.ptr, A * sizeof(uint64_t),
+                            cudaMemcpyDeviceToHost, st));
+  BFVM_CUDA(cudaMemcpyAsync(idx.data(), m->d_ag_idx.ptr, A * sizeof(int), cudaMemcpyDeviceToHost,
+                            st));
+  BFVM_CUDA(cudaMemcpyAsync(t1_in.data(), m->d_ag_t1.ptr, t1_in.size() * sizeof(double),
+                            cudaMemcpyDeviceToHost, st));
+  BFVM_CUDA(cudaMemcpyAsync(t2_in.data(), m->d_ag_t2.ptr, t2_in.size() * sizeof(double),
+                            cudaMemcpyDeviceToHost, st));
+  BFVM_CUDA(cudaStreamSynchronize(st));
   std::vector<int64_t> line(A);
   std::vector<int> pos(A);
   std::vector<double> t1((size_t)A * S), t2((size_t)A * S);
-  std::vector<int64_t> gvox;
-  std::vector<int> gstart;
   for (int64_t r = 0; r < A; ++r) {
-    const int64_t e = order[r];
-    const int64_t v = m->ag_vox[e];
+    const int64_t v = (int64_t)key[r], e = idx[r];
     line[r] = v / m->nx;
     pos[r] = (int)(v % m->nx);
-    std::copy_n(&m->ag_t1[(size_t)e * S], S, &t1[(size_t)r * S]);
-    std::copy_n(&m->ag_t2[(size_t)e * S], S, &t2[(size_t)r * S]);
-    if (r == 0 || v != gvox.back()) {
-      gvox.push_back(v);
-      gstart.push_back((int)r);
-    }
+    std::copy_n(&t1_in[(size_t)e * S], S, &t1[(size_t)r * S]);
+    std::copy_n(&t2_in[(size_t)e * S], S, &t2[(size_t)r * S]);
   }
-  gstart.push_back((int)A);
-  m->n_groups = (int64_t)gvox.size();
-
   const int ch = m->axis[0].ch, nc = (m->nx + ch - 1) / ch;
   upload(m->seg_cells.off, segment_offsets((int64_t)m->ny * m->nz, nc, ch, line, pos), st);
   upload(m->seg_cells.pos, pos, st);
   upload(m->seg_cells.a, t1, st);
   upload(m->seg_cells.b, t2, st);
   m->seg_cells.present = true;
-  upload(m->d_group_vox, gvox, st);
-  upload(m->d_group_start, gstart, st);
-  upload(m->d_ag_vox_orig, m->ag_vox, st);
-  m->ag_dirty = false;
+}
+
+// add_density on the agents: temp1/temp2 get one more column, 0 and 1 (the
+// identity update) for the new density.
+void widen_agents(bfvm_solver* m, int S0) {
+  const int64_t A = m->n_agents;
+  if (A == 0) return;
+  const int S1 = S0 + 1;
+  auto widen = [&](DevBuf& b, double fill) {
+    DevBuf w;
+    w.ensure((size_t)A * S1 * sizeof(double));
+    BFVM_CUDA(cudaMemcpy2DAsync(w.ptr, S1 * sizeof(double), b.ptr, S0 * sizeof(double),
+                                S0 * sizeof(double), A, cudaMemcpyDeviceToDevice, m->stream));
+    bfvm::fill_column_kernel<<<(unsigned)blocks_for(A, 256), 256, 0, m->stream>>>(
+        w.as<double>(), A, S1, S0, fill);
+    check_launch(m);
+    BFVM_CUDA(cudaStreamSynchronize(m->stream));
+    b.release();
+    b = w;
+    w.ptr = nullptr;
+  };
+  widen(m->d_ag_t1, 0.0);
+  widen(m->d_ag_t2, 1.0);
 }
 
 void build_all(bfvm_solver* m) {
   build_bulk(m);
   build_dirichlet(m);
   build_agents(m);
+  if (m->fuse_sources) build_agent_segments(m);
 }
 
 // ---- launches ---------------------------------------------------------------
@@ -1052,6 +939,9 @@ void diffusion(bfvm_solver* m, double dt) { step_once(m, dt, BFVM_STEP_DIFFUSION
 // diffusion_decay_solver__constant_coefficients_LOD_2D (BioFVM_solvers.cpp:278-427):
 // uniform mesh, Dirichlet then x-Thomas, Dirichlet then y-Thomas, on the
 // z = 0 plane.
+template <typename T>
+void dirichlet_standalone(bfvm_solver* m);
+
 void diffusion_2d(bfvm_solver* m, double dt) {
   require(m->uniform,
           "Error: This algorithm is written for uniform Cartesian meshes. Try: something else.",
@@ -1063,6 +953,15 @@ void diffusion_2d(bfvm_solver* m, double dt) {
   m->lod_dims = 2;
   if (!m->setup_done) thomas_setup(m, dt);
   build_all(m);
+  // apply_dirichlet_conditions covers every node, also those off the z = 0
+  // plane that the sweeps never touch (:367, :394); the fused overwrites
+  // below cover the swept plane.
+  if (m->nz > 1 && m->dir_unique > 0) {
+    if (m->precision == BFVM_FP64)
+      dirichlet_standalone<double>(m);
+    else
+      dirichlet_standalone<float>(m);
+  }
   sweep(m, 0, bfvm::kFuseDirPro | bfvm::kFuseDirEpi, dt);
   sweep(m, 1, 0, dt);
 }
@@ -1080,11 +979,12 @@ void bulk_standalone(bfvm_solver* m, double dt) {
 
 template <typename T>
 void cells_standalone(bfvm_solver* m) {
-  if (m->n_groups == 0) return;
-  const int64_t work = m->n_groups * m->S;
+  const int64_t A = m->n_agents;
+  if (A == 0) return;
+  const int64_t work = A * m->S;
   bfvm::cells_kernel<T><<<(unsigned)blocks_for(work, 256), 256, 0, m->stream>>>(
-      m->p.as<T>(), m->S, m->n_groups, m->d_group_vox.as<int64_t>(), m->d_group_start.as<int>(),
-      m->seg_cells.a.as<double>(), m->seg_cells.b.as<double>());
+      m->p.as<T>(), m->S, A, m->d_ag_key.as<uint64_t>(), m->d_ag_idx.as<int>(),
+      m->d_ag_t1.as<double>(), m->d_ag_t2.as<double>());
   check_launch(m);
 }
 
@@ -1123,8 +1023,9 @@ void cells_any(bfvm_solver* m) {
 void validate_voxels(const bfvm_solver* m, int64_t count, const int64_t* vox) {
   const int64_t N = m->N();
   for (int64_t e = 0; e < count; ++e)
-    require(vox[e] >= 0 && vox[e] < N,
-            "voxel index " + std::to_string(vox[e]) + " outside [0, " + std::to_string(N) + ")");
+    if (vox[e] < 0 || vox[e] >= N)  // the message is built only on failure
+      throw Error(BFVM_ERR_ARG, "voxel index " + std::to_string(vox[e]) + " outside [0, " +
+                                    std::to_string(N) + ")");
 }
 
 void resize_common(bfvm_solver* m, int nx, int ny, int nz) {
@@ -1136,44 +1037,10 @@ void resize_common(bfvm_solver* m, int nx, int ny, int nz) {
   clear_state_after_resize(m);
 }
 
-template <typename F>
-int guarded(F&& f) {
-  try {
-    f();
-    return BFVM_OK;
-  } catch (const Error& e) {
-    g_last_error = e.what();
-    return e.code;
-  } catch (const std::bad_alloc&) {
-    g_last_error = "host allocation failed";
-    return BFVM_ERR_NOMEM;
-  } catch (const std::exception& e) {
-    g_last_error = e.what();
-    return BFVM_ERR_STATE;
-  }
-}
 
-struct DeviceGuard {
-  int prev = -1;
-  explicit DeviceGuard(int dev) {
-    cudaGetDevice(&prev);
-    if (prev != dev) BFVM_CUDA(cudaSetDevice(dev));
-  }
-  ~DeviceGuard() {
-    int cur = -1;
-    cudaGetDevice(&cur);
-    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
-  }
-};
+}  // namespace bfvm_rt
 
-#define SOLVER_CALL(m, ...)                                     \
-  guarded([&] {                                                 \
-    require((m) != nullptr, "null solver handle");              \
-    DeviceGuard dg_((m)->device);                               \
-    __VA_ARGS__;                                                \
-  })
-
-}  // namespace
+using namespace bfvm_rt;
 
 extern "C" {
 
@@ -1220,8 +1087,12 @@ int bfvm_destroy(bfvm_solver* m) {
     m->seg_dir_x.release();
     m->seg_dir_y.release();
     m->d_ag_vox_orig.release();
-    m->d_group_vox.release();
-    m->d_group_start.release();
+    m->d_ag_t1.release();
+    m->d_ag_t2.release();
+    m->d_ag_key.release();
+    m->d_ag_idx_in.release();
+    m->d_ag_idx.release();
+    m->d_sort_tmp.release();
     m->d_gather.release();
     m->seg_cells.release();
     m->d_status.release();
@@ -1333,10 +1204,8 @@ int bfvm_resize_densities(bfvm_solver* m, int num_densities) {
     m->bulk_st.clear();
     m->bulk_su.clear();
     m->bulk_dirty = true;
-    m->ag_vox.clear();
-    m->ag_t1.clear();
-    m->ag_t2.clear();
-    m->ag_dirty = true;
+    m->n_agents = 0;
+    m->ag_dirty = m->ag_seg_dirty = true;
   });
 }
 
@@ -1369,9 +1238,9 @@ int bfvm_add_density(bfvm_solver* m, double diffusion_coefficient, double decay_
     widen(m->dir_val, 0.0);
     widen(m->bulk_st, 0.0);
     widen(m->bulk_su, 0.0);
-    widen(m->ag_t1, 0.0);
-    widen(m->ag_t2, 1.0);
-    m->dir_dirty = m->bulk_dirty = m->ag_dirty = true;
+    widen_agents(m, S0);
+    m->dir_dirty = m->bulk_dirty = true;
+    m->ag_dirty = m->ag_seg_dirty = true;
   });
 }
 
@@ -1600,19 +1469,30 @@ int bfvm_set_agents(bfvm_solver* m, int64_t count, const int64_t* voxel, const d
     require(count >= 0 && (count == 0 || (voxel && temp1 && temp2)), "bad arguments");
     require(count < ((int64_t)1 << 31), "too many agents");
     validate_voxels(m, count, voxel);
-    m->ag_vox.assign(voxel, voxel + count);
-    m->ag_t1.assign(temp1, temp1 + count * m->S);
-    m->ag_t2.assign(temp2, temp2 + count * m->S);
-    m->ag_dirty = true;
+    cudaStream_t st = m->stream;
+    const size_t tbytes = (size_t)count * m->S * sizeof(double);
+    m->n_agents = 0;
+    m->ag_dirty = m->ag_seg_dirty = true;
+    if (count > 0) {
+      m->d_ag_vox_orig.ensure(count * sizeof(int64_t));
+      m->d_ag_t1.ensure(tbytes);
+      m->d_ag_t2.ensure(tbytes);
+      BFVM_CUDA(cudaMemcpyAsync(m->d_ag_vox_orig.ptr, voxel, count * sizeof(int64_t),
+                                cudaMemcpyHostToDevice, st));
+      BFVM_CUDA(cudaMemcpyAsync(m->d_ag_t1.ptr, temp1, tbytes, cudaMemcpyHostToDevice, st));
+      BFVM_CUDA(cudaMemcpyAsync(m->d_ag_t2.ptr, temp2, tbytes, cudaMemcpyHostToDevice, st));
+      // the caller may reuse its arrays once this call returns
+      BFVM_CUDA(cudaStreamSynchronize(st));
+    }
+    m->n_agents = count;
   });
 }
 
 int bfvm_get_agent_densities(bfvm_solver* m, double* values) {
   return SOLVER_CALL(m, {
-    const int64_t A = (int64_t)m->ag_vox.size();
+    const int64_t A = m->n_agents;
     if (A == 0) return;
     require(values != nullptr, "null output buffer");
-    build_agents(m);
     m->d_gather.ensure(A * m->S * sizeof(double));
     if (m->precision == BFVM_FP64)
       gather<double>(m, A, m->d_ag_vox_orig.as<int64_t>(), m->d_gather.as<double>());
@@ -1703,7 +1583,7 @@ int bfvm_set_precision(bfvm_solver* m, int precision) {
     m->setup_done = false;  // coefficient tables are kept in the sweep precision
     choose_axes(m);
     // segment lists depend on the chunk lengths
-    m->bulk_dirty = m->dir_dirty = m->ag_dirty = true;
+    m->bulk_dirty = m->dir_dirty = m->ag_seg_dirty = true;
   });
 }
 
@@ -1718,7 +1598,7 @@ int bfvm_set_sweep_config(bfvm_solver* m, int axis, int chunk, int columns, int 
     const int nc = (ns[axis] + chunk - 1) / chunk;
     require(nc * columns <= 512, "chunks x columns exceeds 512 threads per block");
     Axis& A = m->axis[axis];
-    if (A.ch != chunk) m->bulk_dirty = m->dir_dirty = m->ag_dirty = true;
+    if (A.ch != chunk) m->bulk_dirty = m->dir_dirty = m->ag_seg_dirty = true;
     A.ch = chunk;
     A.tw = columns;
     A.minb = min_blocks;

@@ -5,10 +5,11 @@
 // nearest_density_vector() hand out references into a host mirror that is
 // refreshed from the device on first access after a step, and that is sent
 // back before the next simulate_* call (the mirror is assumed modified once a
-// reference has been handed out).  Bulk supply/target/uptake callbacks are
-// evaluated for every voxel at the first simulate_bulk_sources_and_sinks and
-// again after update_rates() or when a callback pointer changes; callbacks
-// whose rates change over time call update_rates() each step.
+// reference has been handed out).  Bulk supply/target/uptake callbacks run on
+// the host for every voxel at every simulate_bulk_sources_and_sinks, into
+// per-voxel vectors that persist between steps and are modified in place
+// exactly as the reference modifies its own (:595-610); the voxels whose
+// update is not the identity go to the device.
 #ifndef __BioFVM_microenvironment_h__
 #define __BioFVM_microenvironment_h__
 
@@ -44,7 +45,11 @@ class Microenvironment {
   // coefficient and bulk-rate state last sent to the device
   std::vector<double> sent_D_, sent_decay_;
   bool rates_dirty_;
-  void* sent_callbacks_[3];
+  // the reference's bulk_source_sink_solver_temp1/2/3: per-voxel vectors
+  // handed to the callbacks and modified in place after them
+  std::vector<std::vector<double> > bulk_temp1_, bulk_temp2_, bulk_temp3_;
+  std::vector<int64_t> sent_bulk_vox_;
+  std::vector<double> sent_bulk_rates_;
   uint64_t sent_agent_epoch_;
   const void* sent_agent_list_;
   std::vector<int> dirichlet_indices;
@@ -54,9 +59,9 @@ class Microenvironment {
   void copy_state(const Microenvironment& o);
   void sync_to_host();
   void sync_to_device();
-  void prepare_step(bool bulk, bool cells, std::vector<Basic_Agent*>* list);
+  void prepare_step(bool bulk, bool cells, std::vector<Basic_Agent*>* list, double dt = 0.0);
   void upload_agents(std::vector<Basic_Agent*>& list);
-  void upload_bulk_rates();
+  void upload_bulk_rates(double dt);
   void after_resize();
   std::vector<double>& mirror(int n);
 

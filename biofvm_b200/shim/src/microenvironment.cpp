@@ -25,10 +25,6 @@ int device_index() {
   return d ? std::atoi(d) : 0;
 }
 
-void* fn_key(void (*f)(Microenvironment*, int, std::vector<double>*)) {
-  return reinterpret_cast<void*>(f);
-}
-
 }  // namespace
 
 Microenvironment* get_default_microenvironment(void) { return g_default; }
@@ -54,7 +50,6 @@ Microenvironment::Microenvironment()
       host_valid_(false),
       host_dirty_(false),
       rates_dirty_(true),
-      sent_callbacks_{nullptr, nullptr, nullptr},
       sent_agent_epoch_(~0ull),
       sent_agent_list_(nullptr) {
   check(bfvm_create(&solver_, device_index()), "bfvm_create");
@@ -122,7 +117,11 @@ void Microenvironment::copy_state(const Microenvironment& o) {
   sent_decay_.clear();
   sent_agent_epoch_ = ~0ull;
   sent_agent_list_ = nullptr;
-  for (auto& c : sent_callbacks_) c = nullptr;
+  bulk_temp1_ = o.bulk_temp1_;
+  bulk_temp2_ = o.bulk_temp2_;
+  bulk_temp3_ = o.bulk_temp3_;
+  sent_bulk_vox_.clear();
+  sent_bulk_rates_.clear();
 }
 
 Microenvironment::Microenvironment(const Microenvironment& o)
@@ -202,37 +201,81 @@ void Microenvironment::after_resize() {
   sent_decay_.clear();
   dirichlet_indices.clear();
   dirichlet_value_vectors.clear();
+  bulk_temp1_.clear();
+  bulk_temp2_.clear();
+  bulk_temp3_.clear();
+  sent_bulk_vox_.clear();
+  sent_bulk_rates_.clear();
 }
 
 // ---- before every device step ---------------------------------------------
 
-void Microenvironment::upload_bulk_rates() {
-  // The three callbacks (BioFVM_microenvironment.h:130-132) for every voxel,
-  // as simulate_bulk_sources_and_sinks evaluates them (:598-600); voxels with
-  // zero supply and uptake are identities of the update and are not sent.
+void Microenvironment::upload_bulk_rates(double dt) {
+  // simulate_bulk_sources_and_sinks (BioFVM_microenvironment.cpp:584-613):
+  // the three callbacks (BioFVM_microenvironment.h:130-132) write into
+  // per-voxel vectors allocated once with zeros (:586-593).  After the
+  // update the reference leaves temp2 = S*T and temp3 = 1 + dt*(U+S) in those
+  // vectors (:603-607), so a callback that skips a voxel finds these values
+  // there at the next step; the same vectors and the same in-place
+  // operations are kept here.  The device receives (S, T, U) as the
+  // callbacks left them for every voxel whose update is not the identity.
   const int S = number_of_densities();
   const int N = number_of_voxels();
-  std::vector<double> sv(S), tv(S), uv(S);
-  std::vector<int64_t> vox;
-  std::vector<double> sup, tar, upt;
-  for (int n = 0; n < N; ++n) {
-    bulk_supply_rate_function(this, n, &sv);
-    bulk_supply_target_densities_function(this, n, &tv);
-    bulk_uptake_rate_function(this, n, &uv);
-    bool identity = true;
-    for (int s = 0; s < S; ++s) identity = identity && tv[s] * sv[s] == 0.0 && uv[s] + sv[s] == 0.0;
-    if (identity) continue;
-    vox.push_back(n);
-    sup.insert(sup.end(), sv.begin(), sv.end());
-    tar.insert(tar.end(), tv.begin(), tv.end());
-    upt.insert(upt.end(), uv.begin(), uv.end());
+  if ((int)bulk_temp1_.size() != N) {
+    const std::vector<double> zero(S, 0.0);
+    bulk_temp1_.assign(N, zero);
+    bulk_temp2_.assign(N, zero);
+    bulk_temp3_.assign(N, zero);
   }
-  check(bfvm_set_bulk_rates_sparse(solver_, (int64_t)vox.size(), vox.data(), sup.data(),
-                                   tar.data(), upt.data()),
+  std::vector<char> keep(N, 0);
+  std::vector<double> rates((size_t)N * 3 * S);
+#pragma omp parallel for schedule(static)
+  for (int n = 0; n < N; ++n) {
+    std::vector<double>& t1 = bulk_temp1_[n];
+    std::vector<double>& t2 = bulk_temp2_[n];
+    std::vector<double>& t3 = bulk_temp3_[n];
+    bulk_supply_rate_function(this, n, &t1);
+    bulk_supply_target_densities_function(this, n, &t2);
+    bulk_uptake_rate_function(this, n, &t3);
+    bool identity = true;
+    double* r = &rates[(size_t)n * 3 * S];
+    for (int s = 0; s < S; ++s) {
+      const double sv = t1[s], tv = t2[s], uv = t3[s];
+      identity = identity && tv * sv == 0.0 && uv + sv == 0.0;
+      r[s] = sv;
+      r[S + s] = tv;
+      r[2 * S + s] = uv;
+    }
+    keep[n] = !identity;
+    // the reference's in-place updates of its temporaries (:602-607)
+    for (int s = 0; s < S; ++s) {
+      t2[s] *= t1[s];
+      t3[s] += t1[s];
+      t3[s] *= dt;
+      t3[s] += 1.0;
+    }
+  }
+  std::vector<int64_t> vox;
+  for (int n = 0; n < N; ++n)
+    if (keep[n]) vox.push_back(n);
+  const size_t E = vox.size();
+  std::vector<double> sup(E * S), tar(E * S), upt(E * S), packed;
+  for (size_t e = 0; e < E; ++e) {
+    const double* r = &rates[(size_t)vox[e] * 3 * S];
+    std::copy_n(r, S, &sup[e * S]);
+    std::copy_n(r + S, S, &tar[e * S]);
+    std::copy_n(r + 2 * S, S, &upt[e * S]);
+  }
+  packed.reserve(3 * E * S);
+  packed.insert(packed.end(), sup.begin(), sup.end());
+  packed.insert(packed.end(), tar.begin(), tar.end());
+  packed.insert(packed.end(), upt.begin(), upt.end());
+  if (vox == sent_bulk_vox_ && packed == sent_bulk_rates_ && !rates_dirty_) return;
+  check(bfvm_set_bulk_rates_sparse(solver_, (int64_t)E, vox.data(), sup.data(), tar.data(),
+                                   upt.data()),
         "bfvm_set_bulk_rates_sparse");
-  sent_callbacks_[0] = fn_key(bulk_supply_rate_function);
-  sent_callbacks_[1] = fn_key(bulk_supply_target_densities_function);
-  sent_callbacks_[2] = fn_key(bulk_uptake_rate_function);
+  sent_bulk_vox_.swap(vox);
+  sent_bulk_rates_.swap(packed);
   rates_dirty_ = false;
 }
 
@@ -257,7 +300,8 @@ void Microenvironment::upload_agents(std::vector<Basic_Agent*>& list) {
   sent_agent_list_ = &list;
 }
 
-void Microenvironment::prepare_step(bool bulk, bool cells, std::vector<Basic_Agent*>* list) {
+void Microenvironment::prepare_step(bool bulk, bool cells, std::vector<Basic_Agent*>* list,
+                                    double dt) {
   sync_to_device();
   if (sent_D_ != diffusion_coefficients || sent_decay_ != decay_rates) {
     for (int s = 0; s < number_of_densities(); ++s)
@@ -266,10 +310,7 @@ void Microenvironment::prepare_step(bool bulk, bool cells, std::vector<Basic_Age
     sent_D_ = diffusion_coefficients;
     sent_decay_ = decay_rates;
   }
-  if (bulk && (rates_dirty_ || sent_callbacks_[0] != fn_key(bulk_supply_rate_function) ||
-               sent_callbacks_[1] != fn_key(bulk_supply_target_densities_function) ||
-               sent_callbacks_[2] != fn_key(bulk_uptake_rate_function)))
-    upload_bulk_rates();
+  if (bulk) upload_bulk_rates(dt);
   if (cells) {
     std::vector<Basic_Agent*>& l = list ? *list : all_basic_agents;
     if (sent_agent_epoch_ != basic_agent_epoch() || sent_agent_list_ != &l) upload_agents(l);
@@ -412,7 +453,7 @@ void Microenvironment::simulate_diffusion_decay(double dt) {
 }
 
 void Microenvironment::simulate_bulk_sources_and_sinks(double dt) {
-  prepare_step(true, false, nullptr);
+  prepare_step(true, false, nullptr, dt);
   check(bfvm_simulate_bulk_sources_and_sinks(solver_, dt), "bfvm_simulate_bulk_sources_and_sinks");
   host_valid_.store(false);
 }
@@ -431,7 +472,7 @@ void Microenvironment::simulate_cell_sources_and_sinks(double dt) {
 }
 
 void Microenvironment::simulate_step(double dt, bool bulk, bool cells) {
-  prepare_step(bulk, cells, nullptr);
+  prepare_step(bulk, cells, nullptr, dt);
   const int flags = BFVM_STEP_DIFFUSION | (bulk ? BFVM_STEP_BULK : 0) | (cells ? BFVM_STEP_CELLS : 0);
   const int rc = bfvm_step(solver_, dt, 1, flags);
   if (rc == BFVM_ERR_MESH) {

@@ -221,6 +221,39 @@ BFVM_API int bfvm_get_launch_count(bfvm_solver* m, int64_t* count);
  * Dirichlet prologue/epilogue), y sweep, z sweep. */
 BFVM_API int bfvm_profile_step(bfvm_solver* m, double dt, int nsteps, int flags, double* ms);
 
+/* ---- many independent microenvironments (no counterpart in the reference,
+ * whose drivers loop over Microenvironment objects one by one) ----------
+ *
+ * A batch refers to solvers (not owned; they must outlive their batch
+ * membership) of one device and one precision.  bfvm_batch_step(b, dt, n,
+ * flags) has the effect of bfvm_step(m, dt, n, flags) on every member: the
+ * instances are packed into groups whose fields fit a byte budget (default
+ * half the L2 cache) and every phase of a step is one launch over a group;
+ * the groups x steps x phases sequence is captured into a CUDA graph and
+ * replayed by one graph launch (the graph is kept while the plan is
+ * unchanged).  Work already queued on a member's stream runs first; later
+ * calls on a member wait for the batch. */
+typedef struct bfvm_batch bfvm_batch;
+BFVM_API int bfvm_batch_create(bfvm_batch** out, int device);
+BFVM_API int bfvm_batch_destroy(bfvm_batch* b);
+BFVM_API int bfvm_batch_add(bfvm_batch* b, bfvm_solver* m);
+BFVM_API int bfvm_batch_clear(bfvm_batch* b);
+BFVM_API int bfvm_batch_size(bfvm_batch* b, int* count);
+BFVM_API int bfvm_batch_step(bfvm_batch* b, double dt, int nsteps, int flags);
+/* Autotuner: times short graph runs (trial_steps steps) of candidate chunk
+ * lengths x threads per block for each axis, then candidate group budgets,
+ * and keeps the fastest.  The members' fields are saved before and restored
+ * after, so tuning does not advance the simulation. */
+BFVM_API int bfvm_batch_tune(bfvm_batch* b, double dt, int flags, int trial_steps);
+/* chunk[3] in {8,16,32} with threads[3] in {128,256,512} per axis, or 0/0 to
+ * choose; group_bytes -1 = default, 0 = all members in one group. */
+BFVM_API int bfvm_batch_set_config(bfvm_batch* b, const int* chunk, const int* threads,
+                                   int64_t group_bytes);
+BFVM_API int bfvm_batch_get_config(bfvm_batch* b, int* chunk, int* threads, int64_t* group_bytes);
+/* Groups of the last plan and kernel launches in its graph. */
+BFVM_API int bfvm_batch_get_plan(bfvm_batch* b, int* groups, int64_t* kernels_per_call);
+BFVM_API int bfvm_batch_synchronize(bfvm_batch* b);
+
 #ifdef __cplusplus
 }
 #endif

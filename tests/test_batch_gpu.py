@@ -1,0 +1,169 @@
+"""Many microenvironments in one batch (bfvm_batch_*): each member must end
+where stepping it alone ends.  Against the oracle: FP64 relative max-norm per
+substrate <= 1e-12 (the same bar as one instance); batched vs the plain
+single-instance path: <= 1e-10."""
+import numpy as np
+import pytest
+
+from biofvm_b200 import STEP_ALL, STEP_CELLS, STEP_DIFFUSION, Batch, BfvmError, Solver, load_scenario
+from biofvm_b200 import workloads as W
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12
+TOL_BATCH_VS_PLAIN = 1e-10
+
+
+def members(seed=71, count=6):
+    """Uneven shapes (1 to 40 points per axis), 1-4 substrates, agents with
+    shared voxels, bulk and Dirichlet on some members."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for b in range(count):
+        shape = tuple(int(v) for v in rng.integers(1, 41, 3))
+        out.append(W.mixed_small(shape=shape, S=int(rng.integers(1, 5)),
+                                 n_agents=int(rng.integers(0, 300)), seed=seed * 10 + b,
+                                 dirichlet=bool(b % 2), bulk=bool(b % 3)))
+    return out
+
+
+def run_batch(scns, steps, flags=STEP_ALL, config=None, tune=False, calls=1):
+    sols = [Solver(0) for _ in scns]
+    for sv, scn in zip(sols, scns):
+        load_scenario(sv, scn)
+    with Batch(0) as bt:
+        for sv in sols:
+            bt.add(sv)
+        if config:
+            bt.set_config(*config)
+        if tune:
+            bt.tune(scns[0].dt, flags, 2)
+        for _ in range(calls):
+            bt.step(scns[0].dt, steps, flags)
+        bt.synchronize()
+        plan = bt.plan()
+        out = [sv.get_densities() for sv in sols]
+    for sv in sols:
+        sv.close()
+    return out, plan
+
+
+def test_batch_matches_oracle_per_member():
+    scns = members()
+    got, (groups, kernels) = run_batch(scns, 3)
+    assert kernels > 0
+    for scn, p in zip(scns, got):
+        ref = O.oracle_run(scn, 3, 7)
+        assert np.all(O.max_rel_err(p, ref) <= TOL64), scn.shape
+
+
+def test_batch_matches_plain_solves():
+    scns = members(seed=72, count=5)
+    got, _ = run_batch(scns, 4)
+    for scn, p in zip(scns, got):
+        with Solver(0) as sv:
+            load_scenario(sv, scn)
+            sv.step(scn.dt, 4)
+            plain = sv.get_densities()
+        assert np.all(O.max_rel_err(p, plain) <= TOL_BATCH_VS_PLAIN), scn.shape
+
+
+@pytest.mark.parametrize("config", [
+    ((8, 8, 8), (512, 512, 512), 0),
+    ((16, 16, 16), (256, 256, 256), 0),
+    ((32, 32, 32), (128, 128, 128), 0),
+    ((16, 32, 8), (512, 256, 512), 1),      # every member its own group
+    ((0, 0, 0), (0, 0, 0), 200_000),       # small groups
+], ids=["ch8", "ch16", "ch32", "mixed-own-groups", "auto-small-groups"])
+def test_batch_configs_agree(config):
+    scns = members(seed=73, count=5)
+    got, (groups, _) = run_batch(scns, 2, config=config)
+    if config[2] == 1:
+        assert groups == len(scns)
+    for scn, p in zip(scns, got):
+        ref = O.oracle_run(scn, 2, 7)
+        assert np.all(O.max_rel_err(p, ref) <= TOL64), (config, scn.shape)
+
+
+def test_graph_replay_over_several_calls():
+    """The captured graph is replayed by later calls with the same plan."""
+    scns = members(seed=74, count=4)
+    got, _ = run_batch(scns, 2, calls=3)
+    for scn, p in zip(scns, got):
+        ref = O.oracle_run(scn, 6, 7)
+        assert np.all(O.max_rel_err(p, ref) <= TOL64), scn.shape
+
+
+def test_tuning_leaves_fields_unchanged():
+    scns = members(seed=75, count=4)
+    got, _ = run_batch(scns, 2, tune=True)
+    for scn, p in zip(scns, got):
+        ref = O.oracle_run(scn, 2, 7)
+        assert np.all(O.max_rel_err(p, ref) <= TOL64), scn.shape
+
+
+def test_member_changes_between_calls_are_seen():
+    """set_agents on a member between batch calls: the plan is rebuilt."""
+    a = W.mixed_small(shape=(10, 9, 8), S=2, n_agents=100, seed=76)
+    b = W.mixed_small(shape=(10, 9, 8), S=2, n_agents=40, seed=77)
+    c = W.mixed_small(shape=(7, 12, 5), S=3, n_agents=60, seed=78)
+    s1, s2 = Solver(0), Solver(0)
+    load_scenario(s1, a)
+    load_scenario(s2, c)
+    with Batch(0) as bt:
+        bt.add(s1)
+        bt.add(s2)
+        bt.step(a.dt, 1, STEP_CELLS)
+        s1.set_agents(*b.agent_arrays())
+        bt.step(a.dt, 1, STEP_CELLS)
+        bt.synchronize()
+    got = s1.get_densities()
+    lib = O.load_oracle()
+    exp = a.initial_field()
+    for scn in (a, b):
+        v, t1, t2 = (np.ascontiguousarray(x) for x in scn.agent_arrays())
+        lib.or_cells(v.size, a.S, O._d(exp), O._l(v), O._d(t1), O._d(t2))
+    assert np.array_equal(got, exp)
+    s1.close()
+    s2.close()
+
+
+def test_batch_diffusion_only_and_sources_only():
+    scns = members(seed=79, count=3)
+    for flags in (STEP_DIFFUSION, STEP_CELLS | 1):
+        got, _ = run_batch(scns, 2, flags=flags)
+        for scn, p in zip(scns, got):
+            ref = O.oracle_run(scn, 2, flags)
+            assert np.all(O.max_rel_err(p, ref) <= TOL64), (flags, scn.shape)
+
+
+def test_batch_rejects_mixed_precision_and_non_uniform_mesh():
+    with Solver(0) as a, Solver(0) as b, Batch(0) as bt:
+        a.resize_space(0, 100, 0, 100, 0, 100, 10)
+        b.resize_space(0, 100, 0, 100, 0, 100, 10)
+        b.set_precision(32)
+        bt.add(a)
+        with pytest.raises(BfvmError):
+            bt.add(b)
+        c = Solver(0)
+        c.resize_space(0, 100, 0, 100, 0, 100, 10, 20, 10)
+        bt.add(c)
+        with pytest.raises(BfvmError) as e:
+            bt.step(0.01, 1)
+        assert "uniform Cartesian" in str(e.value)
+        bt.clear()
+        c.close()
+
+
+def test_batched_workload_small_sample_matches_plain():
+    """Members drawn like the 64-instance batched workload (4 of them, 200
+    steps would be slow for the oracle: 5 steps against plain solves)."""
+    scns = W.batched_instances(count=4, seed=80, n_min=16, n_max=48, max_agents=3000)
+    got, _ = run_batch(scns, 5)
+    for scn, p in zip(scns, got):
+        with Solver(0) as sv:
+            load_scenario(sv, scn)
+            sv.step(scn.dt, 5)
+            plain = sv.get_densities()
+        assert np.all(O.max_rel_err(p, plain) <= TOL_BATCH_VS_PLAIN), scn.shape

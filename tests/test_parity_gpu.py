@@ -278,3 +278,49 @@ def test_lod2d(shape, path):
             sv.simulate_diffusion_decay_2d(scn.dt)
         p = sv.get_densities()
     assert np.all(rel_err(p, ref) <= TOL64)
+
+
+def test_agents_sharing_voxels_keep_list_order():
+    """Hundreds of agents in a handful of voxels: the implicit per-agent update
+    does not commute, so only the reference's list order reproduces it
+    (bit-exact, cells step alone)."""
+    scn = W.mixed_small(shape=(3, 2, 2), S=3, n_agents=700, seed=61, dirichlet=False,
+                        bulk=False)
+    ref = O.oracle_run(scn, 2, STEP_CELLS)
+    for fused in (True, False):
+        assert np.array_equal(run_gpu(scn, 2, STEP_CELLS, fused=fused), ref)
+
+
+def test_agents_replaced_between_steps():
+    """set_agents replaces the whole list (more, fewer, none)."""
+    a = W.mixed_small(shape=(12, 9, 7), S=2, n_agents=400, seed=62)
+    b = W.mixed_small(shape=(12, 9, 7), S=2, n_agents=90, seed=63)
+    with Solver(0) as sv:
+        load_scenario(sv, a)
+        sv.step(a.dt, 1, STEP_CELLS)
+        sv.set_agents(*b.agent_arrays())
+        sv.step(a.dt, 1, STEP_CELLS)
+        sv.set_agents(np.zeros(0, np.int64), np.zeros((0, 2)), np.zeros((0, 2)))
+        sv.step(a.dt, 1, STEP_CELLS)
+        got = sv.get_densities()
+    lib = O.load_oracle()
+    exp = a.initial_field()
+    for scn in (a, b):
+        v, t1, t2 = (np.ascontiguousarray(x) for x in scn.agent_arrays())
+        lib.or_cells(v.size, a.S, O._d(exp), O._l(v), O._d(t1), O._d(t2))
+    assert np.array_equal(got, exp)
+
+
+def test_add_density_after_agents_gives_identity_update():
+    """add_density widens every agent's constants with temp1 = 0, temp2 = 1
+    (secretion and uptake of a new density start at zero)."""
+    scn = W.mixed_small(shape=(8, 6, 5), S=2, n_agents=120, seed=64, dirichlet=False,
+                        bulk=False)
+    with Solver(0) as sv:
+        load_scenario(sv, scn)
+        sv.add_density(1e3, 0.1)
+        sv.set_voxel_densities(np.arange(scn.num_voxels), np.c_[scn.p0, np.full(scn.num_voxels, 2.5)])
+        sv.step(scn.dt, 2, STEP_CELLS)
+        got = sv.get_densities()
+    ref = O.oracle_run(scn, 2, STEP_CELLS)
+    assert np.array_equal(got[:, :2], ref) and np.all(got[:, 2] == 2.5)

@@ -531,6 +531,81 @@ def run_fp32(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_adjoint(args, world, rank, local):
+    """The adjoint workload: 128^3 voxels x 4 substrates FP64, 20k agents,
+    200 steps with checkpoints every 20.  Loss = 1/2 |p_T - target|^2, the
+    target made by the forward run with every parameter scaled by
+    (1 + 0.01 N(0,1)) (seeded).  Reports the forward (with checkpoints) and
+    backward device times, their ratio, and the agreement of the gradient
+    with central finite differences (h = 1e-6 relative) along random
+    directions."""
+    import numpy as np
+
+    from biofvm_b200 import workloads as W
+    from biofvm_b200.adjoint import AdjointProblem
+
+    n = args.size if "--size" in sys.argv else 128
+    S = args.substrates if "--substrates" in sys.argv else 4
+    A = args.agents if "--agents" in sys.argv else 20_000
+    k = 20
+    scn = W.lod_cube(n, S, A, steps=args.steps, name=f"lod_{n}")
+    th = [np.array(scn.agent_secretion, float), np.array(scn.agent_uptake, float),
+          np.array(scn.D, float), np.array(scn.decay, float)]
+    rng = np.random.default_rng(12349)
+    prob = AdjointProblem(scn, args.steps, checkpoint_every=k, device=local)
+    target = prob.run(*[x * (1 + 0.01 * rng.standard_normal(x.shape)) for x in th])
+    prob.forward(*th)  # warm-up of both passes
+    prob.backward(np.zeros((scn.num_voxels, S)))
+    from biofvm_b200._abi import call
+
+    sv = prob.solver
+    with ClockSampler(local) as clocks:
+        prob.set_parameters(*th)
+        sv.synchronize()
+        barrier(world)
+        t0 = time.perf_counter()
+        call("bfvm_adjoint_forward", sv.handle, scn.dt, args.steps, prob.flags, k)
+        sv.synchronize()
+        t_fwd = time.perf_counter() - t0
+        seed = sv.get_densities() - target
+        t0 = time.perf_counter()
+        g = prob.backward(seed)  # includes the seed upload and the gradient reads
+        t_bwd = time.perf_counter() - t0
+    prob.set_parameters(*th)
+    sv.synchronize()
+    t_plain = time.perf_counter()
+    sv.step(scn.dt, args.steps)
+    sv.synchronize()
+    t_plain = time.perf_counter() - t_plain
+    checks = []
+    for d in range(2):
+        v = [x * rng.standard_normal(x.shape) for x in th]
+        h = 1e-6
+        lp = 0.5 * np.sum((prob.run(*[a + h * b for a, b in zip(th, v)]) - target) ** 2)
+        lm = 0.5 * np.sum((prob.run(*[a - h * b for a, b in zip(th, v)]) - target) ** 2)
+        fd = (lp - lm) / (2 * h)
+        adj = (np.sum(g["secretion"] * v[0]) + np.sum(g["uptake"] * v[1]) +
+               np.sum(g["D"] * v[2]) + np.sum(g["decay"] * v[3]))
+        checks.append({"fd": fd, "adjoint": adj, "rel_diff": abs(adj - fd) / abs(fd)})
+    prob.close()
+    if rank == 0:
+        vs = scn.num_voxels * S * args.steps
+        line = {
+            "metric": METRIC + " (adjoint: forward with checkpoints + backward)",
+            "value": vs * world / (t_fwd + t_bwd), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": 1, "ms_per_step": 1e3 * (t_fwd + t_bwd) / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)",
+            "config": {"workload": f"adjoint: {n}^3 x {S} FP64, {A} agents, {args.steps} steps, "
+                                   f"checkpoints every {k}", "loss": "1/2 |p_T - target|^2"},
+            "forward_seconds": t_fwd, "backward_seconds": t_bwd,
+            "plain_forward_seconds": t_plain, "backward_over_forward": t_bwd / t_plain,
+            "gradient_vs_central_differences": checks,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -542,16 +617,20 @@ def main():
     ap.add_argument("--size", type=int, default=256, help="cube edge in voxels (default 256)")
     ap.add_argument("--substrates", type=int, default=10)
     ap.add_argument("--agents", type=int, default=100_000)
-    ap.add_argument("--workload", choices=["lod256", "batched", "fp32"], default="lod256",
+    ap.add_argument("--workload", choices=["lod256", "batched", "fp32", "adjoint"],
+                    default="lod256",
                     help="lod256: the headline line (default); batched: 64 independent "
                          "instances vs looped plain solves; fp32: FP32 sweeps at 512^3 x 8 "
-                         "with 1M agents against FP64")
+                         "with 1M agents against FP64; adjoint: gradients at 128^3 x 4, 200 "
+                         "steps")
     ap.add_argument("--instances", type=int, default=64)
     args = ap.parse_args()
     if args.workload == "batched" and "--steps" not in sys.argv:
         args.steps = 200
     if args.workload == "fp32" and "--steps" not in sys.argv:
         args.steps = 50
+    if args.workload == "adjoint" and "--steps" not in sys.argv:
+        args.steps = 200
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     world, rank, local = dist_init(args)
     try:
@@ -561,6 +640,8 @@ def main():
             run_batched(args, world, rank, local)
         elif args.workload == "fp32":
             run_fp32(args, world, rank, local)
+        elif args.workload == "adjoint":
+            run_adjoint(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:

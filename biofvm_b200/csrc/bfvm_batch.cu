@@ -440,9 +440,9 @@ void batch_tune(bfvm_batch* b, double dt, int flags, int trial_steps) {
   const BatchConfig user = b->cfg;
   drop_graph(b);
   try {
-    // 1. per axis: chunk length x threads, sweeps alone, every instance in one group
+    // 1. per axis: chunk length x threads, sweeps alone, default groups
     BatchConfig best = user;
-    best.group_bytes = 0;
+    best.group_bytes = -1;
     for (int a = 0; a < 3; ++a) {
       float best_ms = 1e30f;
       for (int ch : {8, 16, 32})

@@ -1038,6 +1038,8 @@ void resize_common(bfvm_solver* m, int nx, int ny, int nz) {
 }
 
 
+template void dirichlet_standalone<double>(bfvm_solver* m);
+
 }  // namespace bfvm_rt
 
 using namespace bfvm_rt;
@@ -1096,6 +1098,7 @@ int bfvm_destroy(bfvm_solver* m) {
     m->d_gather.release();
     m->seg_cells.release();
     m->d_status.release();
+    adjoint_release(m);
     for (auto& c : m->chunk) c.release();
     for (auto& c : m->chunk_slots) c.release();
     cudaStreamDestroy(m->stream);

@@ -128,6 +128,10 @@ inline int64_t blocks_for(int64_t work, int threads) { return (work + threads - 
 
 }  // namespace bfvm_rt
 
+namespace bfvm_rt {
+struct AdjointTape;
+}
+
 struct bfvm_solver {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -192,6 +196,9 @@ struct bfvm_solver {
   const void* map_key[3] = {nullptr, nullptr, nullptr};
   int map_w[3] = {0, 0, 0};
 
+  // checkpoints and buffers of the adjoint (bfvm_adjoint.cu), when used
+  bfvm_rt::AdjointTape* adj = nullptr;
+
   int64_t N() const { return (int64_t)nx * ny * nz; }
   int64_t NS() const { return N() * S; }
   size_t elem() const { return precision == BFVM_FP64 ? sizeof(double) : sizeof(float); }
@@ -221,6 +228,15 @@ bfvm::AxisCoef<T> coef_view(const bfvm_solver* m, int a) {
 void thomas_setup(bfvm_solver* m, double dt);
 void build_all(bfvm_solver* m);
 void check_lod_mesh(bfvm_solver* m);
+void check_status(bfvm_solver* m);
+void step_once(bfvm_solver* m, double dt, int flags, cudaEvent_t* ev);
+void sweep(bfvm_solver* m, int ax, int fuse, double dt);
+void bulk_any(bfvm_solver* m, double dt);
+void cells_any(bfvm_solver* m);
+template <typename T>
+void dirichlet_standalone(bfvm_solver* m);
+// Defined in bfvm_adjoint.cu.
+void adjoint_release(bfvm_solver* m);
 
 }  // namespace bfvm_rt
 

@@ -221,6 +221,29 @@ BFVM_API int bfvm_get_launch_count(bfvm_solver* m, int64_t* count);
  * Dirichlet prologue/epilogue), y sweep, z sweep. */
 BFVM_API int bfvm_profile_step(bfvm_solver* m, double dt, int nsteps, int flags, double* ms);
 
+/* ---- derivatives (no counterpart in the reference) ----------------------
+ *
+ * bfvm_adjoint_forward runs nsteps steps exactly like bfvm_step(m, dt,
+ * nsteps, flags) (FP64 only) and keeps the field every checkpoint_every
+ * steps.  bfvm_adjoint_backward then takes seed = dLoss/d(final field)
+ * ([N][S] FP64; host memory, or device memory when seed_on_device != 0) and
+ * returns, in host arrays (each may be NULL):
+ *   grad_D[S], grad_decay[S]       dLoss/d(diffusion coefficient, decay rate)
+ *   grad_temp1[A*S], grad_temp2[A*S]  dLoss/d(agent temp1, temp2), agents in
+ *       list order (Basic_Agent::cell_source_sink_solver_temp1/2,
+ *       BioFVM_basic_agent.cpp:139-147)
+ *   grad_p0[N*S]                   dLoss/d(field before the first step)
+ * It recomputes each checkpoint segment (3 fields kept per step of a
+ * segment) and applies the adjoint step by step in reverse.  The solver must
+ * not change between the two calls; the field keeps the forward result. */
+BFVM_API int bfvm_adjoint_forward(bfvm_solver* m, double dt, int nsteps, int flags,
+                                  int checkpoint_every);
+BFVM_API int bfvm_adjoint_backward(bfvm_solver* m, const double* seed, int seed_on_device,
+                                   double* grad_D, double* grad_decay, double* grad_temp1,
+                                   double* grad_temp2, double* grad_p0);
+/* Frees the checkpoints and buffers of the adjoint. */
+BFVM_API int bfvm_adjoint_release(bfvm_solver* m);
+
 /* ---- many independent microenvironments (no counterpart in the reference,
  * whose drivers loop over Microenvironment objects one by one) ----------
  *

@@ -542,7 +542,7 @@ def run_adjoint(args, world, rank, local):
     import numpy as np
 
     from biofvm_b200 import workloads as W
-    from biofvm_b200.adjoint import AdjointProblem
+    from biofvm_b200.adjoint import AdjointProblem, loss_difference
 
     n = args.size if "--size" in sys.argv else 128
     S = args.substrates if "--substrates" in sys.argv else 4
@@ -581,9 +581,9 @@ def run_adjoint(args, world, rank, local):
     for d in range(2):
         v = [x * rng.standard_normal(x.shape) for x in th]
         h = 1e-6
-        lp = 0.5 * np.sum((prob.run(*[a + h * b for a, b in zip(th, v)]) - target) ** 2)
-        lm = 0.5 * np.sum((prob.run(*[a - h * b for a, b in zip(th, v)]) - target) ** 2)
-        fd = (lp - lm) / (2 * h)
+        pp = prob.run(*[a + h * b for a, b in zip(th, v)])
+        pm = prob.run(*[a - h * b for a, b in zip(th, v)])
+        fd = loss_difference(pp, pm, target) / (2 * h)
         adj = (np.sum(g["secretion"] * v[0]) + np.sum(g["uptake"] * v[1]) +
                np.sum(g["D"] * v[2]) + np.sum(g["decay"] * v[3]))
         checks.append({"fd": fd, "adjoint": adj, "rel_diff": abs(adj - fd) / abs(fd)})

@@ -84,6 +84,9 @@ SIGNATURES = {
     "bfvm_get_stream": (c_int, [_P, POINTER(c_void_p)]),
     "bfvm_get_launch_count": (c_int, [_P, _LP]),
     "bfvm_profile_step": (c_int, [_P, c_double, c_int, c_int, _DP]),
+    "bfvm_compute_all_gradient_vectors": (c_int, [_P]),
+    "bfvm_get_gradient_vectors": (c_int, [_P, _DP]),
+    "bfvm_device_gradients": (c_int, [_P, POINTER(c_void_p)]),
     "bfvm_adjoint_forward": (c_int, [_P, c_double, c_int, c_int, c_int]),
     "bfvm_adjoint_backward": (c_int, [_P, c_void_p, c_int, _DP, _DP, _DP, _DP, _DP]),
     "bfvm_adjoint_release": (c_int, [_P]),

@@ -36,12 +36,15 @@ class AdjointProblem:
         self.solver = Solver(device)
         load_scenario(self.solver, scn)
         self.p0 = scn.initial_field()
-        self.vox, _, _ = scn.agent_arrays()
-        vol = np.asarray(scn.agent_volume, np.float64).reshape(-1, 1) if scn.num_agents else \
-            np.zeros((0, 1))
+        if scn.num_agents:
+            self.vox, _, _ = scn.agent_arrays()
+            vol = np.asarray(scn.agent_volume, np.float64).reshape(-1, 1)
+            self.saturation = np.asarray(scn.agent_saturation, np.float64)
+        else:
+            self.vox = np.zeros(0, np.int64)
+            vol = np.zeros((0, 1))
+            self.saturation = np.zeros((0, scn.S))
         self.c = scn.dt * vol / scn.mesh.dV
-        self.saturation = np.asarray(scn.agent_saturation, np.float64) if scn.num_agents else \
-            np.zeros((0, scn.S))
 
     def close(self) -> None:
         self.solver.close()
@@ -88,6 +91,13 @@ class AdjointProblem:
         if want_p0:
             out["p0"] = gp0
         return out
+
+
+def loss_difference(p_plus: np.ndarray, p_minus: np.ndarray, target: np.ndarray) -> float:
+    """L(p+) - L(p-) for L(p) = 1/2 |p - target|^2, summed as
+    1/2 sum((p+ - p-)(p+ + p- - 2 target)): the two losses are never formed,
+    so the difference keeps its digits (central finite differences)."""
+    return 0.5 * float(np.sum((p_plus - p_minus) * (p_plus + p_minus - 2.0 * target)))
 
 
 def transport(problem: AdjointProblem, secretion, uptake, D, decay):

@@ -341,6 +341,32 @@ __global__ void scatter_kernel(T* __restrict__ p, int S, int64_t E, const int64_
   p[voxel[e] * S + s] = (T)in[t];
 }
 
+// Microenvironment::compute_all_gradient_vectors (BioFVM_microenvironment.cpp:
+// 702-787): central differences along each axis at the points with a
+// neighbour on both sides, g = (p[n + jump] - p[n - jump]) / (2 d); the
+// components of points at an axis end are left as they are.  g is
+// [N][S][3] FP64.
+template <typename T>
+__global__ void gradient_kernel(const T* __restrict__ p, int nx, int ny, int nz, int S,
+                                double two_dx, double two_dy, double two_dz,
+                                double* __restrict__ g) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t NS = (int64_t)nx * ny * nz * S;
+  if (t >= NS) return;
+  const int64_t n = t / S;
+  const int i = (int)(n % nx);
+  const int j = (int)((n / nx) % ny);
+  const int k = (int)(n / ((int64_t)nx * ny));
+  const int64_t jx = S, jy = (int64_t)nx * S, jz = (int64_t)nx * ny * S;
+  double* out = g + 3 * t;
+  if (i > 0 && i < nx - 1)
+    out[0] = __ddiv_rn(__dsub_rn((double)p[t + jx], (double)p[t - jx]), two_dx);
+  if (j > 0 && j < ny - 1)
+    out[1] = __ddiv_rn(__dsub_rn((double)p[t + jy], (double)p[t - jy]), two_dy);
+  if (k > 0 && k < nz - 1)
+    out[2] = __ddiv_rn(__dsub_rn((double)p[t + jz], (double)p[t - jz]), two_dz);
+}
+
 template <typename Dst, typename Src>
 __global__ void convert_kernel(Dst* __restrict__ dst, const Src* __restrict__ src, int64_t count) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;

@@ -72,6 +72,7 @@ void clear_state_after_resize(bfvm_solver* m) {
   m->dir_dirty = true;
   m->n_agents = 0;
   m->ag_dirty = m->ag_seg_dirty = true;
+  m->d_grad.release();
   for (auto& A : m->axis) A.user = false;
   choose_axes(m);
 }
@@ -1098,6 +1099,7 @@ int bfvm_destroy(bfvm_solver* m) {
     m->d_gather.release();
     m->seg_cells.release();
     m->d_status.release();
+    m->d_grad.release();
     adjoint_release(m);
     for (auto& c : m->chunk) c.release();
     for (auto& c : m->chunk_slots) c.release();
@@ -1196,6 +1198,7 @@ int bfvm_resize_densities(bfvm_solver* m, int num_densities) {
     m->S = num_densities;
     m->D.assign(num_densities, 0.0);
     m->decay.assign(num_densities, 0.0);
+    m->d_grad.release();
     m->p.ensure(std::max<size_t>(m->NS() * m->elem(), 16));
     BFVM_CUDA(cudaMemsetAsync(m->p.ptr, 0, m->NS() * m->elem(), m->stream));
     // resize_densities keeps the Dirichlet list but its value vectors no
@@ -1242,6 +1245,18 @@ int bfvm_add_density(bfvm_solver* m, double diffusion_coefficient, double decay_
     widen(m->bulk_st, 0.0);
     widen(m->bulk_su, 0.0);
     widen_agents(m, S0);
+    if (m->d_grad.ptr) {  // gradient vectors keep their values, zeros for the new density
+      DevBuf g;
+      g.ensure((size_t)N * S1 * 3 * sizeof(double));
+      BFVM_CUDA(cudaMemsetAsync(g.ptr, 0, (size_t)N * S1 * 3 * sizeof(double), m->stream));
+      BFVM_CUDA(cudaMemcpy2DAsync(g.ptr, S1 * 3 * sizeof(double), m->d_grad.ptr,
+                                  S0 * 3 * sizeof(double), S0 * 3 * sizeof(double), N,
+                                  cudaMemcpyDeviceToDevice, m->stream));
+      BFVM_CUDA(cudaStreamSynchronize(m->stream));
+      m->d_grad.release();
+      m->d_grad = g;
+      g.ptr = nullptr;
+    }
     m->dir_dirty = m->bulk_dirty = true;
     m->ag_dirty = m->ag_seg_dirty = true;
   });
@@ -1555,6 +1570,49 @@ int bfvm_step(bfvm_solver* m, double dt, int nsteps, int flags) {
       return;
     }
     for (int it = 0; it < nsteps; ++it) step_once(m, dt, flags, nullptr);
+  });
+}
+
+void ensure_gradients(bfvm_solver* m) {
+  const size_t bytes = (size_t)m->NS() * 3 * sizeof(double);
+  if (m->d_grad.ptr && m->d_grad.bytes >= bytes) return;
+  m->d_grad.ensure(std::max<size_t>(bytes, 16));
+  BFVM_CUDA(cudaMemsetAsync(m->d_grad.ptr, 0, bytes, m->stream));
+}
+
+int bfvm_compute_all_gradient_vectors(bfvm_solver* m) {
+  return SOLVER_CALL(m, {
+    ensure_gradients(m);
+    // the reference divides by 2*dx, 2*dy, 2*dz (:704-713)
+    const double two_dx = m->dx * 2.0, two_dy = m->dy * 2.0, two_dz = m->dz * 2.0;
+    const int64_t work = m->NS();
+    if (m->precision == BFVM_FP64)
+      bfvm::gradient_kernel<double><<<(unsigned)blocks_for(work, 256), 256, 0, m->stream>>>(
+          m->p.as<double>(), m->nx, m->ny, m->nz, m->S, two_dx, two_dy, two_dz,
+          m->d_grad.as<double>());
+    else
+      bfvm::gradient_kernel<float><<<(unsigned)blocks_for(work, 256), 256, 0, m->stream>>>(
+          m->p.as<float>(), m->nx, m->ny, m->nz, m->S, two_dx, two_dy, two_dz,
+          m->d_grad.as<double>());
+    check_launch(m);
+  });
+}
+
+int bfvm_get_gradient_vectors(bfvm_solver* m, double* out) {
+  return SOLVER_CALL(m, {
+    require(out != nullptr, "null output buffer");
+    ensure_gradients(m);
+    BFVM_CUDA(cudaMemcpyAsync(out, m->d_grad.ptr, (size_t)m->NS() * 3 * sizeof(double),
+                              cudaMemcpyDeviceToHost, m->stream));
+    BFVM_CUDA(cudaStreamSynchronize(m->stream));
+  });
+}
+
+int bfvm_device_gradients(bfvm_solver* m, void** ptr) {
+  return SOLVER_CALL(m, {
+    require(ptr != nullptr, "null output pointer");
+    ensure_gradients(m);
+    *ptr = m->d_grad.ptr;
   });
 }
 

@@ -196,6 +196,9 @@ struct bfvm_solver {
   const void* map_key[3] = {nullptr, nullptr, nullptr};
   int map_w[3] = {0, 0, 0};
 
+  // gradient vectors [N][S][3] FP64 (allocated and zeroed on first use)
+  bfvm_rt::DevBuf d_grad;
+
   // checkpoints and buffers of the adjoint (bfvm_adjoint.cu), when used
   bfvm_rt::AdjointTape* adj = nullptr;
 

@@ -54,6 +54,10 @@ class Microenvironment {
   const void* sent_agent_list_;
   std::vector<int> dirichlet_indices;
   std::vector<std::vector<double> > dirichlet_value_vectors;
+  // gradient vectors [voxel][substrate][3] (BioFVM_microenvironment.h:65-66)
+  std::vector<std::vector<gradient> > gradient_vectors;
+  std::vector<bool> gradient_vector_computed;
+  void size_gradient_vectors();
 
   void ensure_solver();
   void copy_state(const Microenvironment& o);
@@ -138,6 +142,15 @@ class Microenvironment {
   std::vector<double>& operator()(int i, int j, int k);
   std::vector<double>& operator()(int i, int j);
   std::vector<double>& operator()(int n);
+
+  // gradients (BioFVM_microenvironment.h:176-184)
+  std::vector<gradient>& gradient_vector(int i, int j, int k);
+  std::vector<gradient>& gradient_vector(int i, int j);
+  std::vector<gradient>& gradient_vector(int n);
+  std::vector<gradient>& nearest_gradient_vector(std::vector<double>& position);
+  void compute_all_gradient_vectors(void);
+  void compute_gradient_vector(int n);
+  void reset_all_gradient_vectors(void);
 
   std::vector<double>& density_vector(int i, int j, int k);
   std::vector<double>& density_vector(int i, int j);

@@ -505,6 +505,88 @@ void Microenvironment::update_rates(void) {
   rates_dirty_ = true;
 }
 
+// ---- gradients (BioFVM_microenvironment.cpp:660-858) -------------------------
+
+void Microenvironment::size_gradient_vectors() {
+  // as the reference's resize_* (:213-222): existing entries keep their values
+  const int N = number_of_voxels(), S = number_of_densities();
+  gradient_vectors.resize(N);
+  for (auto& v : gradient_vectors) {
+    v.resize(S);
+    for (auto& g : v) g.resize(3, 0.0);
+  }
+  gradient_vector_computed.resize(N, false);
+}
+
+void Microenvironment::compute_all_gradient_vectors(void) {
+  // On the device (bfvm_compute_all_gradient_vectors); the components the
+  // reference writes -- axes along which the voxel has both neighbours --
+  // are copied into the host vectors, the others keep their values.
+  size_gradient_vectors();
+  sync_to_device();
+  check(bfvm_compute_all_gradient_vectors(solver_), "bfvm_compute_all_gradient_vectors");
+  const int N = number_of_voxels(), S = number_of_densities();
+  std::vector<double> g((size_t)N * S * 3);
+  check(bfvm_get_gradient_vectors(solver_, g.data()), "bfvm_get_gradient_vectors");
+  const int nx = (int)mesh.x_coordinates.size(), ny = (int)mesh.y_coordinates.size(),
+            nz = (int)mesh.z_coordinates.size();
+  for (int n = 0; n < N; ++n) {
+    const int i = n % nx, j = (n / nx) % ny, k = n / (nx * ny);
+    const bool in[3] = {i > 0 && i < nx - 1, j > 0 && j < ny - 1, k > 0 && k < nz - 1};
+    for (int s = 0; s < S; ++s)
+      for (int c = 0; c < 3; ++c)
+        if (in[c]) gradient_vectors[n][s][c] = g[((size_t)n * S + s) * 3 + c];
+    if (in[0] || in[1] || in[2]) gradient_vector_computed[n] = true;
+  }
+}
+
+void Microenvironment::compute_gradient_vector(int n) {
+  // :790-843, from the host copy of the densities
+  size_gradient_vectors();
+  const int nx = (int)mesh.x_coordinates.size(), ny = (int)mesh.y_coordinates.size(),
+            nz = (int)mesh.z_coordinates.size();
+  const int i = n % nx, j = (n / nx) % ny, k = n / (nx * ny);
+  const int jump[3] = {1, nx, nx * ny};
+  const bool in[3] = {i > 0 && i < nx - 1, j > 0 && j < ny - 1, k > 0 && k < nz - 1};
+  const double two_d[3] = {mesh.dx * 2.0, mesh.dy * 2.0, mesh.dz * 2.0};
+  const int S = number_of_densities();
+  for (int c = 0; c < 3; ++c) {
+    if (!in[c]) continue;
+    const std::vector<double>& up = mirror(n + jump[c]);
+    const std::vector<double>& down = mirror(n - jump[c]);
+    for (int s = 0; s < S; ++s) {
+      double v = up[s];
+      v -= down[s];
+      v /= two_d[c];
+      gradient_vectors[n][s][c] = v;
+    }
+    gradient_vector_computed[n] = true;
+  }
+}
+
+void Microenvironment::reset_all_gradient_vectors(void) {
+  size_gradient_vectors();
+  gradient_vector_computed.assign(number_of_voxels(), false);
+}
+
+std::vector<gradient>& Microenvironment::gradient_vector(int n) {
+  size_gradient_vectors();
+  if (!gradient_vector_computed[n]) compute_gradient_vector(n);
+  return gradient_vectors[n];
+}
+
+std::vector<gradient>& Microenvironment::gradient_vector(int i, int j, int k) {
+  return gradient_vector(mesh.voxel_index(i, j, k));
+}
+
+std::vector<gradient>& Microenvironment::gradient_vector(int i, int j) {
+  return gradient_vector(mesh.voxel_index(i, j, 0));
+}
+
+std::vector<gradient>& Microenvironment::nearest_gradient_vector(std::vector<double>& position) {
+  return gradient_vector(mesh.nearest_voxel_index(position));
+}
+
 // ---- Dirichlet nodes (BioFVM_microenvironment.cpp:146-197) ----------------
 
 void Microenvironment::add_dirichlet_node(int n, std::vector<double>& value) {

@@ -184,6 +184,16 @@ class Solver:
     def reset_diffusion_setup(self) -> None:
         call("bfvm_reset_diffusion_setup", self._h)
 
+    # -- gradients (Microenvironment::compute_all_gradient_vectors) -----------
+    def compute_all_gradient_vectors(self) -> None:
+        call("bfvm_compute_all_gradient_vectors", self._h)
+
+    def get_gradient_vectors(self) -> np.ndarray:
+        """[N, S, 3] FP64."""
+        out = np.empty((self.num_voxels, self.number_of_densities, 3))
+        call("bfvm_get_gradient_vectors", self._h, dptr(out))
+        return out
+
     def set_precision(self, bits: int) -> None:
         call("bfvm_set_precision", self._h, bits)
 

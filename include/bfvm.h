@@ -221,6 +221,18 @@ BFVM_API int bfvm_get_launch_count(bfvm_solver* m, int64_t* count);
  * Dirichlet prologue/epilogue), y sweep, z sweep. */
 BFVM_API int bfvm_profile_step(bfvm_solver* m, double dt, int nsteps, int flags, double* ms);
 
+/* Microenvironment::compute_all_gradient_vectors (BioFVM_microenvironment.cpp:
+ * 702-787): central differences (p[n+jump] - p[n-jump]) / (2 dx) along each
+ * axis at the points with a neighbour on both sides, into the solver's
+ * device gradient array [N][S][3] (FP64).  Components of points at an axis
+ * end keep their previous values (zero when the array is first made; the
+ * array is kept across steps, widened by add_density, cleared by resize).
+ * The reference takes its jumps from the LOD_3D setup and its 2 dx from the
+ * first mesh it sees (static constants); here they are the current mesh's. */
+BFVM_API int bfvm_compute_all_gradient_vectors(bfvm_solver* m);
+BFVM_API int bfvm_get_gradient_vectors(bfvm_solver* m, double* out);
+BFVM_API int bfvm_device_gradients(bfvm_solver* m, void** ptr);
+
 /* ---- derivatives (no counterpart in the reference) ----------------------
  *
  * bfvm_adjoint_forward runs nsteps steps exactly like bfvm_step(m, dt,

@@ -220,3 +220,32 @@ void or_run(int nx, int ny, int nz, int S, double dx, double dt, int nsteps, int
   free(denz);
   free(cxz);
 }
+
+void or_gradients(int nx, int ny, int nz, int S, const double* p, double dx, double dy,
+                  double dz, double* g) {
+  /* BioFVM_microenvironment.cpp:702-787; two_d = d; two_d *= 2.0 (:704-713) */
+  const double two_dx = dx * 2.0, two_dy = dy * 2.0, two_dz = dz * 2.0;
+  const int64_t jx = S, jy = (int64_t)nx * S, jz = (int64_t)nx * ny * S;
+  for (int k = 0; k < nz; ++k)
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i)
+        for (int s = 0; s < S; ++s) {
+          const int64_t q = (((int64_t)k * ny + j) * nx + i) * S + s;
+          double* o = g + 3 * q;
+          if (i > 0 && i < nx - 1) { /* :728-730 */
+            o[0] = p[q + jx];
+            o[0] -= p[q - jx];
+            o[0] /= two_dx;
+          }
+          if (j > 0 && j < ny - 1) { /* :751-753 */
+            o[1] = p[q + jy];
+            o[1] -= p[q - jy];
+            o[1] /= two_dy;
+          }
+          if (k > 0 && k < nz - 1) { /* :774-776 */
+            o[2] = p[q + jz];
+            o[2] -= p[q - jz];
+            o[2] /= two_dz;
+          }
+        }
+}

@@ -82,6 +82,12 @@ void or_run(int nx, int ny, int nz, int S, double dx, double dt, int nsteps, int
             const double* temp1, const double* temp2, int ndir, const int64_t* dir_idx,
             const double* dir_val);
 
+/* compute_all_gradient_vectors (BioFVM_microenvironment.cpp:702-787): central
+ * differences at points with both neighbours along an axis, into g
+ * [N][S][3]; other components are left as they are. */
+void or_gradients(int nx, int ny, int nz, int S, const double* p, double dx, double dy,
+                  double dz, double* g);
+
 #ifdef __cplusplus
 }
 #endif

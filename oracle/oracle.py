@@ -76,6 +76,9 @@ def load_oracle() -> ctypes.CDLL:
                                            _DP, _DP]
         lib.or_cells.restype = None
         lib.or_cells.argtypes = [c_int64, c_int, _DP, _LP, _DP, _DP]
+        lib.or_gradients.restype = None
+        lib.or_gradients.argtypes = [c_int, c_int, c_int, c_int, _DP, c_double, c_double,
+                                     c_double, _DP]
         lib.or_run.restype = None
         lib.or_run.argtypes = [c_int, c_int, c_int, c_int, c_double, c_double, c_int, c_int, _DP,
                                _DP, _DP, _DP, _DP, _DP, c_int64, _LP, _DP, _DP, c_int, _LP, _DP]
@@ -116,6 +119,7 @@ def load_reference(variant: str = "core2") -> ctypes.CDLL:
             "refh_apply_dirichlet": (None, [V]),
             "refh_run": (c_double, [V, c_double, c_int, c_int]),
             "refh_num_threads": (c_int, []),
+            "refh_gradients": (None, [V, _DP]),
         }
         for name, (res, args) in sig.items():
             f = getattr(lib, name)
@@ -270,6 +274,12 @@ class Reference:
     def apply_dirichlet(self):
         self.lib.refh_apply_dirichlet(self.h)
 
+    def gradients(self) -> np.ndarray:
+        """compute_all_gradient_vectors, then every gradient_vector(n): [N, S, 3]."""
+        out = np.zeros((self.scn.num_voxels, self.scn.S, 3))
+        self.lib.refh_gradients(self.h, _d(out))
+        return out
+
     def densities(self) -> np.ndarray:
         out = np.empty((self.scn.num_voxels, self.scn.S))
         self.lib.refh_get_densities(self.h, _d(out))
@@ -305,3 +315,17 @@ def wall(f, *args, **kw):
     t0 = time.perf_counter()
     out = f(*args, **kw)
     return out, time.perf_counter() - t0
+
+
+def oracle_gradients(p: np.ndarray, shape, dx: float, dy: float | None = None,
+                     dz: float | None = None, g: np.ndarray | None = None) -> np.ndarray:
+    """compute_all_gradient_vectors on the field p [N, S]: [N, S, 3] (entries at
+    axis ends keep g's values, zero by default)."""
+    lib = load_oracle()
+    nx, ny, nz = shape
+    p = np.ascontiguousarray(p, np.float64)
+    S = p.shape[1]
+    out = np.zeros((p.shape[0], S, 3)) if g is None else np.array(g, np.float64, copy=True)
+    lib.or_gradients(nx, ny, nz, S, _d(p), dx, dx if dy is None else dy,
+                     dx if dz is None else dz, _d(out))
+    return out

@@ -256,4 +256,19 @@ double refh_run(void* hp, double dt, int nsteps, int flags) {
 
 int refh_num_threads(void) { return omp_get_max_threads(); }
 
+// Microenvironment::compute_all_gradient_vectors (BioFVM_microenvironment.cpp:
+// 702-787), then every voxel's gradient_vector(n) as [N][S][3].  The
+// reference reads its jumps from the LOD_3D setup (BioFVM_solvers.cpp:
+// 101-103): run a diffusion step first.
+void refh_gradients(void* hp, double* out) {
+  Microenvironment* M = static_cast<RefHarness*>(hp)->M;
+  M->compute_all_gradient_vectors();
+  const int S = M->number_of_densities();
+  for (int n = 0; n < M->number_of_voxels(); ++n) {
+    std::vector<gradient>& g = M->gradient_vector(n);
+    for (int s = 0; s < S; ++s)
+      for (int c = 0; c < 3; ++c) out[((size_t)n * S + s) * 3 + c] = g[s][c];
+  }
+}
+
 }  // extern "C"

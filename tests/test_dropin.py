@@ -89,3 +89,44 @@ def test_reference_example_runs_unchanged_on_the_gpu(name, tmp_path):
         den = np.maximum(np.abs(a[4:]).max(axis=1), 1e-300)
         err = np.abs(a[4:] - b[4:]).max(axis=1) / den
         assert np.all(err <= 1e-12), (fname, err)
+
+
+def _parse_driver(text):
+    """{tag: {key tuple: value}} from the driver's 'tag ints... value' lines."""
+    out = {}
+    for line in text.splitlines():
+        f = line.split()
+        if len(f) < 4 or f[0] not in ("G", "P", "L", "Q"):
+            continue
+        out.setdefault(f[0], {})[tuple(int(x) for x in f[1:-1])] = float(f[-1])
+    return out
+
+
+@pytest.mark.gpu
+def test_api_driver_matches_the_reference_build():
+    """tests/dropin/api_driver.cpp (agents sharing voxels, Dirichlet nodes,
+    direct writes, gradients of every voxel and the lazy per-voxel path),
+    built against the reference and against the drop-in headers.  Fields:
+    relative max-norm per substrate <= 1e-12.  Gradients: within the error the
+    field bound allows, |dg| <= 2e-12 * max|p_s| / dx."""
+    gpu = os.path.join(ROOT, "biofvm_b200", "shim", "_build", "dropin", "drivers", "api_driver")
+    ref = os.path.join(ROOT, "oracle", "_ref", "drivers", "api_driver")
+    if not (os.path.exists(gpu) and os.path.exists(ref)):
+        pytest.skip("driver binaries not built (they need the reference sources)")
+    runs = {}
+    for tag, exe in (("ref", ref), ("gpu", gpu)):
+        r = subprocess.run([exe], capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, (tag, r.stdout[-2000:], r.stderr[-2000:])
+        runs[tag] = _parse_driver(r.stdout)
+    a, b = runs["ref"], runs["gpu"]
+    assert set(a) == {"G", "P", "L", "Q"} and set(a) == set(b)
+    dx = 10.0
+    for field, grads in (("P", "G"), ("Q", "L")):
+        assert a[field].keys() == b[field].keys() and a[grads].keys() == b[grads].keys()
+        S = 1 + max(k[1] for k in a[field])
+        pmax = [max(abs(v) for k, v in a[field].items() if k[1] == s) for s in range(S)]
+        for s in range(S):
+            err = max(abs(a[field][k] - b[field][k]) for k in a[field] if k[1] == s)
+            assert err <= 1e-12 * pmax[s], (field, s, err)
+            gerr = max(abs(a[grads][k] - b[grads][k]) for k in a[grads] if k[1] == s)
+            assert gerr <= 2e-12 * pmax[s] / dx, (grads, s, gerr)

@@ -105,3 +105,15 @@ def test_lod2d_oracle_matches_reference(shape):
         ref.run(3, 4)
         b = ref.densities()
     assert np.array_equal(a, b)
+
+
+@pytest.mark.skipif(not REF, reason="compiled reference (oracle/_ref) not built")
+def test_gradients_match_reference():
+    """compute_all_gradient_vectors (every scenario here uses dx = 10: the
+    reference keeps the first 2*dx it sees in static variables)."""
+    scn = W.mixed_small(shape=(9, 7, 6), S=3, n_agents=50, seed=5)
+    with O.Reference(scn) as ref:
+        ref.run(2, 7)  # the reference takes its index jumps from the LOD_3D setup
+        p = ref.densities()
+        g = ref.gradients()
+    assert np.array_equal(O.oracle_gradients(p, scn.shape, scn.mesh.dx), g)

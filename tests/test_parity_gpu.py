@@ -324,3 +324,27 @@ def test_add_density_after_agents_gives_identity_update():
         got = sv.get_densities()
     ref = O.oracle_run(scn, 2, STEP_CELLS)
     assert np.array_equal(got[:, :2], ref) and np.all(got[:, 2] == 2.5)
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_gradients_bit_exact_on_the_device_field(precision):
+    """Central differences of the device field, bit for bit as the reference's
+    compute_all_gradient_vectors computes them on the same field; the
+    components at axis ends keep their earlier values across calls."""
+    scn = W.mixed_small(shape=(11, 9, 1), S=2, n_agents=40, seed=66)
+    with Solver(0) as sv:
+        load_scenario(sv, scn)
+        if precision != 64:
+            sv.set_precision(precision)
+        sv.step(scn.dt, 2)
+        sv.compute_all_gradient_vectors()
+        g1 = sv.get_gradient_vectors()
+        p1 = sv.get_densities()
+        sv.step(scn.dt, 1)
+        sv.compute_all_gradient_vectors()
+        g2 = sv.get_gradient_vectors()
+        p2 = sv.get_densities()
+    e1 = O.oracle_gradients(p1, scn.shape, scn.mesh.dx)
+    assert np.array_equal(g1, e1)
+    assert np.array_equal(g2, O.oracle_gradients(p2, scn.shape, scn.mesh.dx, g=e1))
+    assert np.all(g2[:, :, 2] == 0)  # nz = 1: no z neighbours anywhere

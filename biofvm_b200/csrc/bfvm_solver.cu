@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <numeric>
@@ -565,6 +566,18 @@ LinesPlan plan_lines(const bfvm_solver* m, int ax) {
     L.stages = stages_for(80 * 1024, 0);
     if (L.stages < 2) L.stages = stages_for(kSmemBudget, 0);
     if (L.stages < 2) return L;
+  }
+  // tuning overrides for measurements: BFVM_LINES_TAB=0|1 (tables in shared
+  // memory), BFVM_LINES_STAGES=2..4 (ring depth; shared memory permitting)
+  static const char* env_tab = std::getenv("BFVM_LINES_TAB");
+  static const char* env_st = std::getenv("BFVM_LINES_STAGES");
+  if (env_tab || env_st) {
+    const bool want_tab = env_tab ? std::atoi(env_tab) != 0 && tab > 0 : L.smem_tab;
+    const int want_st = env_st ? std::max(2, std::min(4, std::atoi(env_st))) : L.stages;
+    if (stages_for(kSmemBudget, want_tab ? tab : 0) >= want_st) {
+      L.smem_tab = want_tab;
+      L.stages = want_st;
+    }
   }
   L.smem = L.stages * stage + fold + extra + (L.smem_tab ? tab : 0);
   L.ok = true;

@@ -531,6 +531,79 @@ def run_fp32(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_plain50(args, world, rank, local):
+    """The small launch-bound workload: 50^3 voxels x 1 substrate, all-boundary
+    Dirichlet 1.0, 1000 uptake agents, 100 steps.  Reports microseconds per
+    step for bfvm_step (kernel launches from the host) and for the same steps
+    replayed from a CUDA graph (a one-member bfvm_batch), and the reference
+    on the host cores for the same run."""
+    import numpy as np
+
+    from biofvm_b200 import STEP_ALL, Batch, Solver, load_scenario
+    from biofvm_b200 import workloads as W
+
+    scn = W.plain_50(steps=args.steps)
+    sv = Solver(local)
+    load_scenario(sv, scn)
+    p0 = scn.initial_field()
+    dt = scn.dt
+    sv.step(dt, 3, STEP_ALL)
+    sv.set_densities(p0)
+    sv.synchronize()
+    t0 = time.perf_counter()
+    sv.step(dt, args.steps, STEP_ALL)
+    sv.synchronize()
+    t_loop = time.perf_counter() - t0
+    ref = sv.get_densities()
+    bt = Batch(local)
+    bt.add(sv)
+    sv.set_densities(p0)
+    bt.step(dt, args.steps, STEP_ALL)  # captures the graph
+    bt.synchronize()
+    sv.set_densities(p0)
+    sv.synchronize()
+    with ClockSampler(local) as clocks:
+        t0 = time.perf_counter()
+        bt.step(dt, args.steps, STEP_ALL)
+        bt.synchronize()
+        t_graph = time.perf_counter() - t0
+    got = sv.get_densities()
+    err = float((np.abs(got - ref).max(axis=0) / np.maximum(np.abs(ref).max(axis=0), 1e-300)).max())
+    groups, kernels = bt.plan()
+    bt.close()
+    sv.close()
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+
+        threads = os.cpu_count() or 1
+        variant = "v3" if (O.reference_available("v3") and _host_has_avx2()) else "core2"
+        r = O.Reference(scn, variant, threads=threads, cells_single_thread=False)
+        r.run(3)
+        secs = r.run(args.steps)
+        r.close()
+        cpu = {"value": scn.num_voxels * args.steps / secs, "unit": UNIT, "cores": threads,
+               "kind": "reference", "us_per_step": 1e6 * secs / args.steps,
+               "sample": f"the whole workload ({args.steps} steps), reference build {variant}"}
+    if rank == 0:
+        vs = scn.num_voxels * scn.S * args.steps
+        line = {
+            "metric": METRIC + " (50^3 launch-bound case)", "value": vs * world / t_graph,
+            "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": 3,
+            "ms_per_step": 1e3 * t_graph / args.steps, "us_per_step": 1e6 * t_graph / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)",
+            "config": {"workload": "plain_50: 50^3 x 1 FP64, all-boundary Dirichlet 1.0, 1000 "
+                                   f"uptake agents, {args.steps} steps"},
+            "host_launched": {"us_per_step": 1e6 * t_loop / args.steps},
+            "graph": {"us_per_step": 1e6 * t_graph / args.steps, "kernels_per_call": kernels},
+            "max_rel_err_graph_vs_host_launched": err,
+            "cpu_baseline": cpu,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+
+
 def run_adjoint(args, world, rank, local):
     """The adjoint workload: 128^3 voxels x 4 substrates FP64, 20k agents,
     200 steps with checkpoints every 20.  Loss = 1/2 |p_T - target|^2, the
@@ -617,12 +690,12 @@ def main():
     ap.add_argument("--size", type=int, default=256, help="cube edge in voxels (default 256)")
     ap.add_argument("--substrates", type=int, default=10)
     ap.add_argument("--agents", type=int, default=100_000)
-    ap.add_argument("--workload", choices=["lod256", "batched", "fp32", "adjoint"],
+    ap.add_argument("--workload", choices=["lod256", "plain50", "batched", "fp32", "adjoint"],
                     default="lod256",
                     help="lod256: the headline line (default); batched: 64 independent "
                          "instances vs looped plain solves; fp32: FP32 sweeps at 512^3 x 8 "
                          "with 1M agents against FP64; adjoint: gradients at 128^3 x 4, 200 "
-                         "steps")
+                         "steps; plain50: the 50^3 launch-bound case, host-launched vs graph")
     ap.add_argument("--instances", type=int, default=64)
     args = ap.parse_args()
     if args.workload == "batched" and "--steps" not in sys.argv:
@@ -631,6 +704,8 @@ def main():
         args.steps = 50
     if args.workload == "adjoint" and "--steps" not in sys.argv:
         args.steps = 200
+    if args.workload == "plain50" and "--steps" not in sys.argv:
+        args.steps = 100
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     world, rank, local = dist_init(args)
     try:
@@ -642,6 +717,8 @@ def main():
             run_fp32(args, world, rank, local)
         elif args.workload == "adjoint":
             run_adjoint(args, world, rank, local)
+        elif args.workload == "plain50":
+            run_plain50(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:

@@ -228,8 +228,13 @@ __device__ __forceinline__ void drain_after_failure(uint64_t* full, int stages, 
 
 // ---------------------------------------------------------------------------
 
+// Largest chunk count per line of lod_lines_tma_kernel: with 32-point chunks
+// 8 (lines of up to 256 points), so that the compiler may give each thread
+// the registers for its 32 values and the chunk tables without spilling.
+constexpr int lines_max_chunks(int ch) { return ch >= 32 ? 8 : 16; }
+
 template <typename T, int CH, int W, int STAGES, bool DIR_EPI, bool SMEM_TAB>
-__global__ void __launch_bounds__(W * 16, 512 / (W * 16))
+__global__ void __launch_bounds__(W * lines_max_chunks(CH))
     lod_lines_tma_kernel(const __grid_constant__ CUtensorMap map, const LinesArgs<T> a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int NC = blockDim.y;

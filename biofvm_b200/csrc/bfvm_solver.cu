@@ -543,7 +543,7 @@ LinesPlan plan_lines(const bfvm_solver* m, int ax) {
   L.ch = m->axis[ax].ch;
   L.nc = (L.n + L.ch - 1) / L.ch;
   L.w = (es == 8) ? 16 : 32;
-  if (L.nc > 16) return L;
+  if (L.nc > bfvm::lines_max_chunks(L.ch)) return L;
   L.box_n = std::min(L.n, 256);
   L.nboxes = (L.n + L.box_n - 1) / L.box_n;
   const int64_t ctiles = (L.C + L.w - 1) / L.w;

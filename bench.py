@@ -259,8 +259,10 @@ def run_ours(args, world, rank, local):
     dt = scn.dt
     stream = torch.cuda.ExternalStream(sv.stream, device=torch.device("cuda", local))
 
-    # warm-up (also builds the Thomas coefficients and the device lists)
+    # warm-up (also builds the Thomas coefficients and the device lists), then
+    # the per-axis kernel choice timed on this field (which is restored)
     sv.step(dt, args.warmup, STEP_ALL)
+    tuned = sv.tune_sweeps(dt, 3)
     sv.synchronize()
 
     launches0 = sv.launch_count
@@ -356,6 +358,8 @@ def run_ours(args, world, rank, local):
                          "traffic": traffic,
                          "algorithmic_bytes_per_launch": BYTES_PER_VS_SWEEP * N * S},
             "kernel_ms": per,
+            "tuned_sweeps": [{"axis": "xyz"[i], "kernel": ["default", "register", "tma", "direct"][k],
+                              "chunk": ch, "columns": tw} for i, (k, ch, tw) in enumerate(tuned)],
             "gpu_launches": int(launches),
             "e2e": e2e,
             "cpu_baseline": cpu,
@@ -485,6 +489,7 @@ def run_fp32(args, world, rank, local):
 
     def timed(clocks=None):
         sv.step(dt, args.warmup, STEP_ALL)
+        sv.tune_sweeps(dt, 2)
         sv.set_densities(p0)
         sv.synchronize()
         barrier(world)

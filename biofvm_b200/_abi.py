@@ -84,6 +84,8 @@ SIGNATURES = {
     "bfvm_get_stream": (c_int, [_P, POINTER(c_void_p)]),
     "bfvm_get_launch_count": (c_int, [_P, _LP]),
     "bfvm_profile_step": (c_int, [_P, c_double, c_int, c_int, _DP]),
+    "bfvm_tune_sweeps": (c_int, [_P, c_double, c_int]),
+    "bfvm_get_sweep_kernel": (c_int, [_P, c_int, _IP]),
     "bfvm_compute_all_gradient_vectors": (c_int, [_P]),
     "bfvm_get_gradient_vectors": (c_int, [_P, _DP]),
     "bfvm_device_gradients": (c_int, [_P, POINTER(c_void_p)]),

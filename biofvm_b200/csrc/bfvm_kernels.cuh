@@ -122,8 +122,12 @@ enum : int { kSweepPlain = 0, kSweepDirEpi = 1, kSweepFull = 2 };
 
 // MINB = minimum resident blocks per SM requested from the compiler (1 or 2):
 // 2 caps registers at 64 per thread so two 512-thread blocks fit an SM.
+// Largest block of lod_sweep_kernel for a chunk length: 32-point chunks keep
+// 256 threads so that each thread has the registers for its chunk.
+constexpr int sweep_max_threads(int ch) { return ch >= 32 ? 256 : 512; }
+
 template <typename T, int CH, int MODE, int MINB>
-__global__ void __launch_bounds__(512, MINB) lod_sweep_kernel(const SweepArgs<T> a) {
+__global__ void __launch_bounds__(sweep_max_threads(CH), MINB) lod_sweep_kernel(const SweepArgs<T> a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int TW = blockDim.x;
   const int NC = blockDim.y;

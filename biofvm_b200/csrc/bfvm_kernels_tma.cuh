@@ -228,13 +228,12 @@ __device__ __forceinline__ void drain_after_failure(uint64_t* full, int stages, 
 
 // ---------------------------------------------------------------------------
 
-// Largest chunk count per line of lod_lines_tma_kernel: with 32-point chunks
-// 8 (lines of up to 256 points), so that the compiler may give each thread
-// the registers for its 32 values and the chunk tables without spilling.
-constexpr int lines_max_chunks(int ch) { return ch >= 32 ? 8 : 16; }
-
-template <typename T, int CH, int W, int STAGES, bool DIR_EPI, bool SMEM_TAB>
-__global__ void __launch_bounds__(W * lines_max_chunks(CH))
+// MAXNC: the most chunks per line the kernel is compiled for (block of
+// W x MAXNC threads).  MAXNC = 8 with 32-point chunks (lines of up to 256
+// points) lets the compiler give each thread the registers for its 32 values
+// and the chunk tables without spilling.
+template <typename T, int CH, int W, int STAGES, bool DIR_EPI, bool SMEM_TAB, int MAXNC>
+__global__ void __launch_bounds__(W * MAXNC)
     lod_lines_tma_kernel(const __grid_constant__ CUtensorMap map, const LinesArgs<T> a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int NC = blockDim.y;
@@ -336,8 +335,8 @@ __global__ void __launch_bounds__(W * lines_max_chunks(CH))
 
 // ---------------------------------------------------------------------------
 
-template <typename T, int CH, int STAGES, bool SMEM_TAB>
-__global__ void __launch_bounds__(512, 1) lod_rows_tma_kernel(const RowsArgs<T> a) {
+template <typename T, int CH, int STAGES, bool SMEM_TAB, int MAXT>
+__global__ void __launch_bounds__(MAXT) lod_rows_tma_kernel(const RowsArgs<T> a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   // Threads: column (r, s) fastest, then chunk c.  A stage holds R rows at a
   // padded pitch (pitch = S mod 16 elements), so the lanes of a warp, which
@@ -406,7 +405,7 @@ __global__ void __launch_bounds__(512, 1) lod_rows_tma_kernel(const RowsArgs<T> 
     const int nr = tile_rows(tile);
     const int64_t row = tile * R + r;
     const int lenA = (r < nr) ? len : 0;
-    T* rb = tiles + st * stage_elems + r * pitch + (size_t)k0 * S + s;
+    const T* rb = tiles + st * stage_elems + r * pitch + (size_t)k0 * S + s;
     T v[CH];
 #pragma unroll
     for (int m = 0; m < CH; ++m) v[m] = (m < lenA) ? rb[m * S] : T(0);
@@ -449,44 +448,31 @@ __global__ void __launch_bounds__(512, 1) lod_rows_tma_kernel(const RowsArgs<T> 
     chunk_local<SMEM_TAB, T, CH>(v, lenA, k1, S, qe, x0);
     Pair<T>* sF = fold + (i & 1) * NC * FW;
     if (c < NC) st_fold(sF + c * FW + fc, qe, x0);
+    // every thread has its chunk in registers: the stage can be refilled
     if (__syncthreads_or(!ok)) {
-      if (tid == 0) {
-        drain_after_failure(full, STAGES, i, issued - i, a.status);
-        tma::bulk_wait_all();
-      }
+      if (tid == 0) drain_after_failure(full, STAGES, i, issued - i, a.status);
       return;
     }
-    // Refill the stage of tile i-2, whose bulk stores were committed two
-    // iterations ago (keep at most the latest group reading shared memory).
-    if (tid == 0 && i >= 2) {
-      const int64_t nt = tile + (int64_t)(STAGES - 2) * gridDim.x;
+    if (tid == 0) {
+      const int64_t nt = tile + (int64_t)STAGES * gridDim.x;
       if (nt < a.ntiles) {
-        asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
-        issue((i - 2) % STAGES, nt);
+        issue(st, nt);
         ++issued;
       }
     }
-    if (c < NC) {
-      T cf, cb;
-      chunk_carries<SMEM_TAB, T>(sF, FW, fc, c, NC, tab, s, S, cf, cb);
-      chunk_fix<SMEM_TAB, T, CH>(v, lenA, kg, S, cf, cb);
-      // ---- epilogue: Dirichlet before the next axis
-      if (lenA > 0 && (a.fuse & kFuseDirEpi)) apply_dirichlet_seg<T, CH>(v, a.dir, seg, k0, S, s);
+    if (lenA == 0) continue;
+    T cf, cb;
+    chunk_carries<SMEM_TAB, T>(sF, FW, fc, c, NC, tab, s, S, cf, cb);
+    chunk_fix<SMEM_TAB, T, CH>(v, lenA, kg, S, cf, cb);
+    // ---- epilogue: Dirichlet before the next axis
+    if (a.fuse & kFuseDirEpi) apply_dirichlet_seg<T, CH>(v, a.dir, seg, k0, S, s);
+    // straight to global memory: the lanes of a warp write the S densities of
+    // consecutive rows at one point
+    T* out = a.p + row * (int64_t)row_elems + (int64_t)k0 * S + s;
 #pragma unroll
-      for (int m = 0; m < CH; ++m)
-        if (m < lenA) rb[m * S] = v[m];
-    }
-    tma::fence_proxy_async_smem();
-    __syncthreads();
-    if (tid == 0) {
-      const uint32_t rbytes = (uint32_t)(row_elems * sizeof(T));
-      for (int q = 0; q < nr; ++q)
-        tma::store_bulk(a.p + (tile * R + q) * row_elems, tiles + st * stage_elems + q * pitch,
-                        rbytes);
-      tma::bulk_commit();
-    }
+    for (int m = 0; m < CH; ++m)
+      if (m < lenA) out[(int64_t)m * S] = v[m];
   }
-  if (tid == 0) tma::bulk_wait_all();
 }
 
 // ---------------------------------------------------------------------------

@@ -45,15 +45,21 @@ void choose_axes(bfvm_solver* m) {
   const int ns[3] = {m->nx, m->ny, m->nz};
   for (int a = 0; a < 3; ++a) {
     const int n = ns[a];
-    if (m->axis[a].user && (n + m->axis[a].ch - 1) / m->axis[a].ch * m->axis[a].tw <= 512)
+    if (m->axis[a].user && (n + m->axis[a].ch - 1) / m->axis[a].ch * m->axis[a].tw <=
+                               bfvm::sweep_max_threads(m->axis[a].ch))
       continue;
     m->axis[a].user = false;
+    m->axis[a].kind = 0;
     int ch = (n <= 64) ? 8 : 16;
     if (a > 0 && n >= 128) ch = 32;
     while ((n + ch - 1) / ch > 16 && ch < 32) ch *= 2;
+    const int nc = (n + ch - 1) / ch;
+    // x: blocks of at most 256 threads (two per SM, measured faster at 256^3)
+    const int maxt = (a == 0) ? std::min(256, bfvm::sweep_max_threads(ch))
+                              : bfvm::sweep_max_threads(ch);
     int tw = 32;
-    if ((n + ch - 1) / ch > 16) tw = 16;
-    require((n + ch - 1) / ch <= 512 / tw,
+    while (tw > 8 && nc * tw > maxt) tw /= 2;
+    require(nc * tw <= bfvm::sweep_max_threads(ch),
             "axis with " + std::to_string(n) + " points exceeds the 1024-point line limit");
     m->axis[a].ch = ch;
     m->axis[a].tw = tw;
@@ -543,7 +549,7 @@ LinesPlan plan_lines(const bfvm_solver* m, int ax) {
   L.ch = m->axis[ax].ch;
   L.nc = (L.n + L.ch - 1) / L.ch;
   L.w = (es == 8) ? 16 : 32;
-  if (L.nc > bfvm::lines_max_chunks(L.ch)) return L;
+  if (L.nc > 16) return L;
   L.box_n = std::min(L.n, 256);
   L.nboxes = (L.n + L.box_n - 1) / L.box_n;
   const int64_t ctiles = (L.C + L.w - 1) / L.w;
@@ -587,7 +593,7 @@ LinesPlan plan_lines(const bfvm_solver* m, int ax) {
 struct RowsPlan {
   bool ok = false;
   bool smem_tab = false;
-  int ch = 0, nc = 0, R = 0, stages = 0;
+  int ch = 0, nc = 0, R = 0, stages = 0, maxt = 256;
   int64_t pitch = 0;
   size_t smem = 0;
 };
@@ -605,9 +611,8 @@ RowsPlan plan_rows(const bfvm_solver* m) {
   if (row_bytes % 16 || m->nx > 1024) return P;
   P.ch = m->axis[0].ch;
   P.nc = (m->nx + P.ch - 1) / P.ch;
-  const int cols = m->S * P.nc;
+  const int cols = m->S * P.nc;  // threads of one row
   if (cols > 512) return P;
-  P.R = (int)std::min<int64_t>(std::max(1, 512 / cols), rows);
   // pitch: row_elems rounded up so that pitch == S (mod 16 elements of 8 B,
   // 32 of 4 B) and pitch*es is a multiple of 16 bytes
   const int64_t mod = (es == 8) ? 16 : 32, step = 16 / es;
@@ -623,20 +628,25 @@ RowsPlan plan_rows(const bfvm_solver* m) {
   P.pitch = pitch;
   const size_t extra = 8 * 4 + 16 + 128;
   const size_t tab = table_bytes(m, 0);
-  // largest R whose ring (>= 3 stages) fits with the chunk tables staged in
-  // shared memory; else the largest without staging them
-  const int rmax = P.R;
-  for (int staged = 1; staged >= 0; --staged) {
-    if (staged && tab == 0) continue;
-    for (P.R = rmax; P.R >= 1; --P.R) {
-      const size_t stage = (size_t)(P.R * pitch * es);
-      const size_t fold = 4 * (size_t)P.nc * P.R * m->S * es;  // two parities of (qe, x0)
-      const size_t t = staged ? tab : 0;
-      if (kSmemBudget <= fold + extra + t) continue;
-      P.stages = (int)std::min<size_t>(4, (kSmemBudget - fold - extra - t) / stage);
-      if (P.stages >= 3) {
+  // Two blocks per SM of at most 256 threads (room for each thread's chunk
+  // in registers), a 2-stage ring of R rows, the chunk tables in shared
+  // memory when they fit; else one block of up to 512 threads.
+  for (int maxt : {256, 512}) {
+    if (cols > maxt) continue;
+    const size_t budget = (maxt == 256) ? 113 * 1024 : kSmemBudget;
+    for (int staged = 1; staged >= 0; --staged) {
+      if (staged && tab == 0) continue;
+      for (int R = (int)std::min<int64_t>(maxt / cols, rows); R >= 1; --R) {
+        const size_t stage = (size_t)(R * pitch * es);
+        const size_t fold = 4 * (size_t)P.nc * R * m->S * es;  // two parities of (qe, x0)
+        const size_t t = staged ? tab : 0;
+        const size_t smem = 2 * stage + fold + extra + t;
+        if (smem > budget) continue;
+        P.R = R;
+        P.stages = 2;
+        P.maxt = maxt;
         P.smem_tab = staged != 0;
-        P.smem = P.stages * stage + fold + extra + t;
+        P.smem = smem;
         P.ok = true;
         return P;
       }
@@ -645,17 +655,31 @@ RowsPlan plan_rows(const bfvm_solver* m) {
   return P;
 }
 
-template <typename T, int CH, int ST, bool DIR, bool TAB>
-void launch_lines_inst(const CUtensorMap& map, const bfvm::LinesArgs<T>& a, int ntiles,
-                       dim3 block, size_t smem, bfvm_solver* m) {
+template <typename T, int CH, int ST, bool DIR, bool TAB, int MAXNC>
+void launch_lines_nc(const CUtensorMap& map, const bfvm::LinesArgs<T>& a, int ntiles,
+                     dim3 block, size_t smem, bfvm_solver* m) {
   constexpr int W = sizeof(T) == 8 ? 16 : 32;
-  auto k = bfvm::lod_lines_tma_kernel<T, CH, W, ST, DIR, TAB>;
+  auto k = bfvm::lod_lines_tma_kernel<T, CH, W, ST, DIR, TAB, MAXNC>;
   allow_smem((const void*)k, m->device, smem);
   int per_sm = 0;
   BFVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, block.x * block.y, smem));
   require(per_sm > 0, "sweep kernel does not fit on an SM", BFVM_ERR_STATE);
   dim3 grid((unsigned)std::min<int64_t>(ntiles, (int64_t)per_sm * m->num_sms));
   k<<<grid, block, smem, m->stream>>>(map, a);
+}
+
+// Lines of up to 8 chunks of 32 points take the kernel compiled for 8 chunks
+// (more registers per thread); longer lines the one for 16.
+template <typename T, int CH, int ST, bool DIR, bool TAB>
+void launch_lines_inst(const CUtensorMap& map, const bfvm::LinesArgs<T>& a, int ntiles,
+                       dim3 block, size_t smem, bfvm_solver* m) {
+  if constexpr (CH >= 32) {
+    if (block.y <= 8) {
+      launch_lines_nc<T, CH, ST, DIR, TAB, 8>(map, a, ntiles, block, smem, m);
+      return;
+    }
+  }
+  launch_lines_nc<T, CH, ST, DIR, TAB, 16>(map, a, ntiles, block, smem, m);
 }
 
 template <typename T, int CH, int ST, bool TAB>
@@ -800,15 +824,30 @@ bool launch_direct(bfvm_solver* m, int ax, int fuse, double dt) {
   return true;
 }
 
-template <typename T, int CH, int ST, bool TAB>
+template <typename T, int CH, bool TAB, int MAXT>
 void launch_rows_inst(const bfvm::RowsArgs<T>& a, dim3 block, size_t smem, bfvm_solver* m) {
-  auto k = bfvm::lod_rows_tma_kernel<T, CH, ST, TAB>;
+  auto k = bfvm::lod_rows_tma_kernel<T, CH, 2, TAB, MAXT>;
   allow_smem((const void*)k, m->device, smem);
   int per_sm = 0;
   BFVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, block.x * block.y, smem));
   require(per_sm > 0, "sweep kernel does not fit on an SM", BFVM_ERR_STATE);
   dim3 grid((unsigned)std::min<int64_t>(a.ntiles, (int64_t)per_sm * m->num_sms));
   k<<<grid, block, smem, m->stream>>>(a);
+}
+
+template <typename T, int CH>
+void launch_rows_ch(const bfvm::RowsArgs<T>& a, const RowsPlan& P, dim3 block, bfvm_solver* m) {
+  if (P.maxt == 256) {
+    if (P.smem_tab)
+      launch_rows_inst<T, CH, true, 256>(a, block, P.smem, m);
+    else
+      launch_rows_inst<T, CH, false, 256>(a, block, P.smem, m);
+  } else {
+    if (P.smem_tab)
+      launch_rows_inst<T, CH, true, 512>(a, block, P.smem, m);
+    else
+      launch_rows_inst<T, CH, false, 512>(a, block, P.smem, m);
+  }
 }
 
 template <typename T>
@@ -834,27 +873,19 @@ void launch_rows(bfvm_solver* m, const RowsPlan& P, int fuse, double dt) {
   a.status = m->d_status.as<int>();
   // whole warps: threads past R*S*NC idle through the sweep
   dim3 block((unsigned)((P.R * m->S * P.nc + 31) / 32 * 32));
-  const int key = (P.smem_tab ? 1000 : 0) + P.ch * 10 + P.stages;
-  switch (key) {
-    case 83: launch_rows_inst<T, 8, 3, false>(a, block, P.smem, m); break;
-    case 84: launch_rows_inst<T, 8, 4, false>(a, block, P.smem, m); break;
-    case 163: launch_rows_inst<T, 16, 3, false>(a, block, P.smem, m); break;
-    case 164: launch_rows_inst<T, 16, 4, false>(a, block, P.smem, m); break;
-    case 323: launch_rows_inst<T, 32, 3, false>(a, block, P.smem, m); break;
-    case 324: launch_rows_inst<T, 32, 4, false>(a, block, P.smem, m); break;
-    case 1083: launch_rows_inst<T, 8, 3, true>(a, block, P.smem, m); break;
-    case 1084: launch_rows_inst<T, 8, 4, true>(a, block, P.smem, m); break;
-    case 1163: launch_rows_inst<T, 16, 3, true>(a, block, P.smem, m); break;
-    case 1164: launch_rows_inst<T, 16, 4, true>(a, block, P.smem, m); break;
-    case 1323: launch_rows_inst<T, 32, 3, true>(a, block, P.smem, m); break;
-    default: launch_rows_inst<T, 32, 4, true>(a, block, P.smem, m); break;
+  switch (P.ch) {
+    case 8: launch_rows_ch<T, 8>(a, P, block, m); break;
+    case 16: launch_rows_ch<T, 16>(a, P, block, m); break;
+    default: launch_rows_ch<T, 32>(a, P, block, m); break;
   }
   check_launch(m);
 }
 
 void sweep(bfvm_solver* m, int ax, int fuse, double dt) {
   const bool fp64 = m->precision == BFVM_FP64;
-  const int path = m->path;
+  // under AUTO an axis may carry its own kernel choice (bfvm_tune_sweeps)
+  const int path =
+      (m->path == BFVM_PATH_AUTO && m->axis[ax].kind) ? m->axis[ax].kind : m->path;
   if (path != BFVM_PATH_GENERIC) {
     // build the chunk tables first: the plans size shared memory from them
     if (fp64)
@@ -1670,13 +1701,114 @@ int bfvm_set_sweep_config(bfvm_solver* m, int axis, int chunk, int columns, int 
     require(min_blocks == 1 || min_blocks == 2, "min_blocks must be 1 or 2");
     const int ns[3] = {m->nx, m->ny, m->nz};
     const int nc = (ns[axis] + chunk - 1) / chunk;
-    require(nc * columns <= 512, "chunks x columns exceeds 512 threads per block");
+    require(nc * columns <= bfvm::sweep_max_threads(chunk),
+            "chunks x columns exceeds the block size of the sweep kernel (512 threads, 256 "
+            "with 32-point chunks)");
     Axis& A = m->axis[axis];
     if (A.ch != chunk) m->bulk_dirty = m->dir_dirty = m->ag_seg_dirty = true;
     A.ch = chunk;
     A.tw = columns;
     A.minb = min_blocks;
+    A.kind = 0;
     A.user = true;
+  });
+}
+
+}  // extern "C"
+
+namespace bfvm_rt {
+
+// Times every kernel choice of each axis on this solver's own data and keeps
+// the fastest (the field is saved before and restored after).
+void tune_sweeps(bfvm_solver* m, double dt, int reps) {
+  require(reps >= 1 && reps <= 100, "reps must be in [1, 100]");
+  check_lod_mesh(m);
+  if (!m->setup_done) thomas_setup(m, dt);
+  build_all(m);
+  const size_t bytes = m->NS() * m->elem();
+  DevBuf save;
+  save.ensure(std::max<size_t>(bytes, 16));
+  BFVM_CUDA(cudaMemcpyAsync(save.ptr, m->p.ptr, bytes, cudaMemcpyDeviceToDevice, m->stream));
+  const int saved_path = m->path;
+  m->path = BFVM_PATH_AUTO;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  BFVM_CUDA(cudaEventCreate(&e0));
+  BFVM_CUDA(cudaEventCreate(&e1));
+  struct Choice {
+    int kind, ch, tw;
+  };
+  const int ns[3] = {m->nx, m->ny, m->nz};
+  const int fuses[3] = {bfvm::kFuseDirPro | bfvm::kFuseDirEpi, bfvm::kFuseDirEpi, 0};
+  try {
+    for (int ax = 0; ax < 3; ++ax) {
+      std::vector<Choice> cand;
+      for (int ch : {8, 16, 32}) {
+        const int nc = (ns[ax] + ch - 1) / ch;
+        if (nc > 64) continue;
+        for (int tw : {32, 16, 8})
+          if (nc * tw <= bfvm::sweep_max_threads(ch)) cand.push_back({BFVM_PATH_GENERIC, ch, tw});
+        if (nc <= 16) {
+          cand.push_back({BFVM_PATH_TMA, ch, 16});
+          cand.push_back({BFVM_PATH_DIRECT, ch, 16});
+        }
+      }
+      Axis best = m->axis[ax];
+      float best_ms = 1e30f;
+      for (const Choice& c : cand) {
+        Axis& A = m->axis[ax];
+        if (A.ch != c.ch) m->bulk_dirty = m->dir_dirty = m->ag_seg_dirty = true;
+        A.ch = c.ch;
+        A.tw = c.tw;
+        A.minb = 1;
+        A.kind = c.kind;
+        A.user = true;
+        build_all(m);
+        sweep(m, ax, fuses[ax], dt);  // warm-up: tables and plans
+        BFVM_CUDA(cudaEventRecord(e0, m->stream));
+        for (int r = 0; r < reps; ++r) sweep(m, ax, fuses[ax], dt);
+        BFVM_CUDA(cudaEventRecord(e1, m->stream));
+        BFVM_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        BFVM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        if (ms < best_ms) {
+          best_ms = ms;
+          best = A;
+        }
+      }
+      if (m->axis[ax].ch != best.ch) m->bulk_dirty = m->dir_dirty = m->ag_seg_dirty = true;
+      m->axis[ax] = best;
+    }
+  } catch (...) {
+    m->path = saved_path;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaMemcpyAsync(m->p.ptr, save.ptr, bytes, cudaMemcpyDeviceToDevice, m->stream);
+    cudaStreamSynchronize(m->stream);
+    save.release();
+    throw;
+  }
+  m->path = saved_path;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  BFVM_CUDA(cudaMemcpyAsync(m->p.ptr, save.ptr, bytes, cudaMemcpyDeviceToDevice, m->stream));
+  BFVM_CUDA(cudaStreamSynchronize(m->stream));
+  save.release();
+  build_all(m);
+  check_status(m);
+}
+
+}  // namespace bfvm_rt
+
+extern "C" {
+
+int bfvm_tune_sweeps(bfvm_solver* m, double dt, int reps) {
+  return SOLVER_CALL(m, tune_sweeps(m, dt, reps));
+}
+
+int bfvm_get_sweep_kernel(bfvm_solver* m, int axis, int* kind) {
+  return SOLVER_CALL(m, {
+    require(axis >= 0 && axis < 3 && kind != nullptr, "bad arguments");
+    *kind = m->axis[axis].kind;
   });
 }
 

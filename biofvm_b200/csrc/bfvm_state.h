@@ -91,7 +91,8 @@ struct Axis {
   int ch = 16;  // points per thread
   int tw = 32;  // columns per block
   int minb = 1; // resident blocks per SM the kernel is compiled for (1 or 2)
-  bool user = false;  // set through bfvm_set_sweep_config
+  int kind = 0; // kernel under BFVM_PATH_AUTO: 0 = default, else a BFVM_PATH_* value
+  bool user = false;  // set through bfvm_set_sweep_config or the tuner
 };
 
 template <typename F>

@@ -197,6 +197,19 @@ class Solver:
     def set_precision(self, bits: int) -> None:
         call("bfvm_set_precision", self._h, bits)
 
+    def tune_sweeps(self, dt: float, reps: int = 5):
+        """Picks each axis's fastest sweep kernel by timing them on this field
+        (which is restored); returns [(kernel, chunk, columns)] per axis."""
+        call("bfvm_tune_sweeps", self._h, dt, reps)
+        out = []
+        for ax in range(3):
+            k = ctypes.c_int()
+            call("bfvm_get_sweep_kernel", self._h, ax, ctypes.byref(k))
+            cfg = (ctypes.c_int * 3)()
+            call("bfvm_get_sweep_config", self._h, ax, cfg)
+            out.append((k.value, cfg[0], cfg[1]))
+        return out
+
     def set_sweep_config(self, axis: int, chunk: int, columns: int, min_blocks: int = 1) -> None:
         call("bfvm_set_sweep_config", self._h, axis, chunk, columns, min_blocks)
 

@@ -216,6 +216,17 @@ BFVM_API int bfvm_get_stream(bfvm_solver* m, void** stream);
 /* Kernel launches enqueued by this solver since creation. */
 BFVM_API int bfvm_get_launch_count(bfvm_solver* m, int64_t* count);
 
+/* Sweep tuner (no counterpart in the reference): for each axis, times every
+ * kernel that can run it -- the register kernel at each chunk length and
+ * block width, the TMA-fed kernel and the direct kernel at each chunk
+ * length -- over reps sweeps of this solver's own field, and keeps the
+ * fastest for later steps (used while the kernel path is BFVM_PATH_AUTO).
+ * The field is saved before and restored after; bfvm_set_sweep_config or
+ * a resize resets the choice.  bfvm_get_sweep_kernel returns the axis's
+ * kernel (0 = the default choice, else a BFVM_PATH_* value). */
+BFVM_API int bfvm_tune_sweeps(bfvm_solver* m, double dt, int reps);
+BFVM_API int bfvm_get_sweep_kernel(bfvm_solver* m, int axis, int* kind);
+
 /* Times bfvm_step's kernels with CUDA events on the solver's stream, averaged
  * over nsteps steps: ms[4] = source kernels (bulk + cells), x sweep (with its
  * Dirichlet prologue/epilogue), y sweep, z sweep. */

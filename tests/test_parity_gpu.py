@@ -348,3 +348,20 @@ def test_gradients_bit_exact_on_the_device_field(precision):
     assert np.array_equal(g1, e1)
     assert np.array_equal(g2, O.oracle_gradients(p2, scn.shape, scn.mesh.dx, g=e1))
     assert np.all(g2[:, :, 2] == 0)  # nz = 1: no z neighbours anywhere
+
+
+@pytest.mark.parametrize("shape", [(24, 20, 16), (70, 33, 9)])
+def test_sweep_tuner_keeps_the_field_and_the_results(shape):
+    """bfvm_tune_sweeps times every kernel of every axis on the solver's own
+    field: the field must come back unchanged, and steps with the chosen
+    kernels must still match the oracle."""
+    scn = W.mixed_small(shape=shape, S=3, n_agents=300, seed=sum(shape))
+    with Solver(0) as sv:
+        load_scenario(sv, scn)
+        before = sv.get_densities()
+        chosen = sv.tune_sweeps(scn.dt, 2)
+        assert np.array_equal(sv.get_densities(), before)
+        assert len(chosen) == 3
+        sv.step(scn.dt, 3)
+        got = sv.get_densities()
+    assert np.all(rel_err(got, O.oracle_run(scn, 3, 7)) <= TOL64), chosen

@@ -262,7 +262,7 @@ def run_ours(args, world, rank, local):
     # warm-up (also builds the Thomas coefficients and the device lists), then
     # the per-axis kernel choice timed on this field (which is restored)
     sv.step(dt, args.warmup, STEP_ALL)
-    tuned = sv.tune_sweeps(dt, 3)
+    tuned = sv.tune_sweeps(dt, 3) if not args.no_tune else [(0, 0, 0)] * 3
     sv.synchronize()
 
     launches0 = sv.launch_count
@@ -475,6 +475,7 @@ def run_fp32(args, world, rank, local):
 
     from biofvm_b200 import FP32, STEP_ALL, Solver, load_scenario
     from biofvm_b200 import workloads as W
+    from biofvm_b200._abi import FP32_FP64MATH
 
     n = args.size if "--size" in sys.argv else 512
     S = args.substrates if "--substrates" in sys.argv else 8
@@ -510,6 +511,12 @@ def run_fp32(args, world, rank, local):
     got = sv.get_densities()
     den = np.maximum(np.abs(ref).max(axis=0), 1e-300)
     err = (np.abs(got - ref).max(axis=0) / den).tolist()
+    # the FP32 field swept in FP64 arithmetic (FP32_FP64MATH)
+    sv.set_precision(FP32_FP64MATH)
+    sv.set_densities(p0)
+    ms_mixed = timed()
+    got = sv.get_densities()
+    err_mixed = (np.abs(got - ref).max(axis=0) / den).tolist()
     sv.close()
     if rank == 0:
         hbm, peak_kind = peaks()
@@ -531,6 +538,10 @@ def run_fp32(args, world, rank, local):
             "fp64_same_workload": {"value": N * S * args.steps * world / (ms64 / 1e3),
                                    "ms_per_step": ms64 / args.steps},
             "max_rel_err_vs_fp64_per_substrate": err,
+            "fp32_field_fp64_sweeps": {
+                "value": N * S * args.steps * world / (ms_mixed / 1e3),
+                "ms_per_step": ms_mixed / args.steps,
+                "max_rel_err_vs_fp64_per_substrate": err_mixed},
             "clocks": clocks.summary(),
         }
         print(json.dumps(line), flush=True)
@@ -692,6 +703,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="keep the default kernel per axis (for profiler launch lists)")
     ap.add_argument("--size", type=int, default=256, help="cube edge in voxels (default 256)")
     ap.add_argument("--substrates", type=int, default=10)
     ap.add_argument("--agents", type=int, default=100_000)

@@ -33,6 +33,7 @@ PATH_DIRECT = 3
 
 FP64 = 64
 FP32 = 32
+FP32_FP64MATH = 3264
 
 _P = c_void_p  # opaque solver handle
 _DP = POINTER(c_double)

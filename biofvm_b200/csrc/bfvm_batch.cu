@@ -537,6 +537,8 @@ int bfvm_batch_add(bfvm_batch* b, bfvm_solver* m) {
   return BATCH_CALL(b, {
     require(m != nullptr, "null solver handle");
     require(m->device == b->device, "instance lives on another device");
+    require(m->precision != BFVM_FP32_FP64MATH,
+            "batches take FP64 or FP32 instances (not BFVM_FP32_FP64MATH)");
     require(b->inst.empty() || m->precision == b->inst[0]->precision,
             "instances of one batch must share the precision");
     require(std::find(b->inst.begin(), b->inst.end(), m) == b->inst.end(),

@@ -62,7 +62,9 @@ struct SegList {
   const double* b = nullptr;
 };
 
-template <typename T>
+// T: the field's element type; CT: the type the sweep computes in (CT = T,
+// or double over a float field).
+template <typename T, typename CT = T>
 struct SweepArgs {
   T* p;
   int64_t ncols;         // number of (line, substrate) columns
@@ -72,7 +74,7 @@ struct SweepArgs {
   int n;                 // points per line
   int nchunks;           // NC = ceil(n / CH)
   int S;
-  AxisCoef<T> coef;
+  AxisCoef<CT> coef;
   SegList bulk, cells, dir_pro, dir_epi;
   double dt;
   int fuse;
@@ -126,15 +128,16 @@ enum : int { kSweepPlain = 0, kSweepDirEpi = 1, kSweepFull = 2 };
 // 256 threads so that each thread has the registers for its chunk.
 constexpr int sweep_max_threads(int ch) { return ch >= 32 ? 256 : 512; }
 
-template <typename T, int CH, int MODE, int MINB>
-__global__ void __launch_bounds__(sweep_max_threads(CH), MINB) lod_sweep_kernel(const SweepArgs<T> a) {
+template <typename T, int CH, int MODE, int MINB, typename CT = T>
+__global__ void __launch_bounds__(sweep_max_threads(CH), MINB)
+    lod_sweep_kernel(const SweepArgs<T, CT> a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int TW = blockDim.x;
   const int NC = blockDim.y;
-  T* sQ = reinterpret_cast<T*>(smem_raw);  // [NC][TW] forward chunk end values
-  T* sP = sQ + NC * TW;                    // forward chunk slope products
-  T* sX = sP + NC * TW;                    // backward chunk start values
-  T* sR = sX + NC * TW;                    // backward chunk slope products
+  CT* sQ = reinterpret_cast<CT*>(smem_raw);  // [NC][TW] forward chunk end values
+  CT* sP = sQ + NC * TW;                    // forward chunk slope products
+  CT* sX = sP + NC * TW;                    // backward chunk start values
+  CT* sR = sX + NC * TW;                    // backward chunk slope products
 
   const int tx = threadIdx.x;
   const int c = threadIdx.y;
@@ -157,9 +160,9 @@ __global__ void __launch_bounds__(sweep_max_threads(CH), MINB) lod_sweep_kernel(
   }
   const int64_t ls = a.line_stride;
 
-  T v[CH];
+  CT v[CH];
 #pragma unroll
-  for (int m = 0; m < CH; ++m) v[m] = (m < len) ? ptr[m * ls] : T(0);
+  for (int m = 0; m < CH; ++m) v[m] = (m < len) ? (CT)ptr[m * ls] : CT(0);
 
   if (MODE == kSweepFull && active) {
     if (a.fuse & kFuseBulk) {
@@ -167,9 +170,9 @@ __global__ void __launch_bounds__(sweep_max_threads(CH), MINB) lod_sweep_kernel(
       for (int e = e0; e < e1; ++e) {
         const int m = __ldg(a.bulk.pos + e) - k0;
         const int64_t q = (int64_t)e * S + s;
-        double x = (double)reg_get<T, CH>(v, m);
+        double x = (double)reg_get<CT, CH>(v, m);
         x = bulk_update(x, __ldg(a.bulk.a + q), __ldg(a.bulk.b + q), a.dt);
-        reg_set<T, CH>(v, m, (T)x);
+        reg_set<CT, CH>(v, m, (CT)x);
       }
     }
     if (a.fuse & kFuseCells) {
@@ -181,26 +184,26 @@ __global__ void __launch_bounds__(sweep_max_threads(CH), MINB) lod_sweep_kernel(
       while (e < e1) {
         const int pos = __ldg(a.cells.pos + e);
         const int m = pos - k0;
-        double x = (double)reg_get<T, CH>(v, m);
+        double x = (double)reg_get<CT, CH>(v, m);
         do {
           const int64_t q = (int64_t)e * S + s;
           x = cell_update(x, __ldg(a.cells.a + q), __ldg(a.cells.b + q));
           ++e;
         } while (e < e1 && __ldg(a.cells.pos + e) == pos);
-        reg_set<T, CH>(v, m, (T)x);
+        reg_set<CT, CH>(v, m, (CT)x);
       }
     }
-    if (a.fuse & kFuseDirPro) apply_dirichlet_seg<T, CH>(v, a.dir_pro, seg, k0, S, s);
+    if (a.fuse & kFuseDirPro) apply_dirichlet_seg<CT, CH>(v, a.dir_pro, seg, k0, S, s);
   }
 
   // Coefficient rows of this chunk: [k][S] tables, stride S along the line.
-  const T* c_inv = a.coef.inv_den + (int64_t)k0 * S + s;
-  const T* c_fwd = a.coef.fwd + (int64_t)k0 * S + s;
-  const T* c_bwd = a.coef.bwd + (int64_t)k0 * S + s;
+  const CT* c_inv = a.coef.inv_den + (int64_t)k0 * S + s;
+  const CT* c_fwd = a.coef.fwd + (int64_t)k0 * S + s;
+  const CT* c_bwd = a.coef.bwd + (int64_t)k0 * S + s;
 
   // ---- forward elimination, chunk-local with carry-in 0 ----
-  const T c1 = active ? __ldg(a.coef.c1 + s) : T(0);
-  T q = T(0), P = T(1);
+  const CT c1 = active ? __ldg(a.coef.c1 + s) : CT(0);
+  CT q = CT(0), P = CT(1);
 #pragma unroll
   for (int m = 0; m < CH; ++m) {
     if (m < len) {
@@ -213,9 +216,9 @@ __global__ void __launch_bounds__(sweep_max_threads(CH), MINB) lod_sweep_kernel(
   sP[c * TW + tx] = P;
   __syncthreads();
   if (c > 0 && len > 0) {
-    T carry = T(0);
+    CT carry = CT(0);
     for (int cc = 0; cc < c; ++cc) carry = sP[cc * TW + tx] * carry + sQ[cc * TW + tx];
-    T Pm = T(1);
+    CT Pm = CT(1);
 #pragma unroll
     for (int m = 0; m < CH; ++m) {
       if (m < len) {
@@ -226,11 +229,11 @@ __global__ void __launch_bounds__(sweep_max_threads(CH), MINB) lod_sweep_kernel(
   }
 
   // ---- back substitution, chunk-local with carry-in 0 ----
-  T x = T(0), R = T(1);
+  CT x = CT(0), R = CT(1);
 #pragma unroll
   for (int m = CH - 1; m >= 0; --m) {
     if (m < len) {
-      const T b = __ldg(c_bwd + m * S);
+      const CT b = __ldg(c_bwd + m * S);
       x = v[m] + b * x;
       R = R * b;
       v[m] = x;
@@ -240,9 +243,9 @@ __global__ void __launch_bounds__(sweep_max_threads(CH), MINB) lod_sweep_kernel(
   sR[c * TW + tx] = R;
   __syncthreads();
   if (c < NC - 1 && len > 0) {
-    T carry = T(0);
+    CT carry = CT(0);
     for (int cc = NC - 1; cc > c; --cc) carry = sR[cc * TW + tx] * carry + sX[cc * TW + tx];
-    T Rm = T(1);
+    CT Rm = CT(1);
 #pragma unroll
     for (int m = CH - 1; m >= 0; --m) {
       if (m < len) {
@@ -253,11 +256,11 @@ __global__ void __launch_bounds__(sweep_max_threads(CH), MINB) lod_sweep_kernel(
   }
 
   if (MODE != kSweepPlain && active && (a.fuse & kFuseDirEpi))
-    apply_dirichlet_seg<T, CH>(v, a.dir_epi, seg, k0, S, s);
+    apply_dirichlet_seg<CT, CH>(v, a.dir_epi, seg, k0, S, s);
 
 #pragma unroll
   for (int m = 0; m < CH; ++m)
-    if (m < len) ptr[m * ls] = v[m];
+    if (m < len) ptr[m * ls] = (T)v[m];
 }
 
 // ---------------------------------------------------------------------------

@@ -113,7 +113,7 @@ __device__ __forceinline__ size_t chunk_row(const ChunkCoef<T>& cc, int c, int s
   return ((size_t)ld_one<SMEM>(cc.slot + c) * cc.ch * S + s) * 2;
 }
 
-template <typename T>
+template <typename T, typename CT = T>
 struct LinesArgs {
   T* p;
   int64_t C;       // contiguous columns per outer block (< 2^31)
@@ -126,12 +126,12 @@ struct LinesArgs {
   int box_n;        // rows per TMA box (<= 256)
   int nboxes;       // boxes per tile
   int nchunks;
-  ChunkCoef<T> cc;
+  ChunkCoef<CT> cc;
   SegList dir_epi;  // (line, chunk) segments, line = (outer*C + col) / S
   int* status;
 };
 
-template <typename T>
+template <typename T, typename CT = T>
 struct RowsArgs {
   T* p;
   int64_t rows;  // ny * nz
@@ -141,7 +141,7 @@ struct RowsArgs {
   int64_t pitch;  // shared-memory elements between the rows of a tile
   int64_t ntiles;
   int nchunks;
-  ChunkCoef<T> cc;
+  ChunkCoef<CT> cc;
   // (row, chunk) segment lists, as for lod_sweep_kernel
   SegList bulk, cells, dir;
   double dt;
@@ -232,9 +232,10 @@ __device__ __forceinline__ void drain_after_failure(uint64_t* full, int stages, 
 // W x MAXNC threads).  MAXNC = 8 with 32-point chunks (lines of up to 256
 // points) lets the compiler give each thread the registers for its 32 values
 // and the chunk tables without spilling.
-template <typename T, int CH, int W, int STAGES, bool DIR_EPI, bool SMEM_TAB, int MAXNC>
+template <typename T, int CH, int W, int STAGES, bool DIR_EPI, bool SMEM_TAB, int MAXNC,
+          typename CT = T>
 __global__ void __launch_bounds__(W * MAXNC)
-    lod_lines_tma_kernel(const __grid_constant__ CUtensorMap map, const LinesArgs<T> a) {
+    lod_lines_tma_kernel(const __grid_constant__ CUtensorMap map, const LinesArgs<T, CT> a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int NC = blockDim.y;
   const int npad = a.box_n * a.nboxes;
@@ -242,16 +243,16 @@ __global__ void __launch_bounds__(W * MAXNC)
   // tensor copies need 128-B aligned shared-memory destinations
   T* tiles =
       reinterpret_cast<T*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~(uintptr_t)127);
-  Pair<T>* fold = reinterpret_cast<Pair<T>*>(tiles + STAGES * stage_elems);  // 2 x [NC][W]
+  Pair<CT>* fold = reinterpret_cast<Pair<CT>*>(tiles + STAGES * stage_elems);  // 2 x [NC][W]
   uint64_t* full = reinterpret_cast<uint64_t*>(fold + 2 * NC * W);
-  T* sm_tab = reinterpret_cast<T*>(full + 4);  // chunk tables (SMEM_TAB)
+  CT* sm_tab = reinterpret_cast<CT*>(full + 4);  // chunk tables (SMEM_TAB)
   int* sm_slot = reinterpret_cast<int*>(sm_tab + (SMEM_TAB ? a.cc.tab_elems : 0));
 
   const int tx = threadIdx.x;
   const int c = threadIdx.y;
   const int tid = c * W + tx;
   const uint32_t stage_bytes = (uint32_t)(stage_elems * sizeof(T));
-  const ChunkCoef<T> tab =
+  const ChunkCoef<CT> tab =
       SMEM_TAB ? stage_tables(a.cc, sm_tab, sm_slot, tid, W * NC) : a.cc;
 
   if (tid == 0) {
@@ -294,14 +295,14 @@ __global__ void __launch_bounds__(W * MAXNC)
     const int s = (int)(col % (uint32_t)S);
     const T* buf = tiles + st * stage_elems + (size_t)k0 * W + tx;
 
-    T v[CH];
+    CT v[CH];
 #pragma unroll
-    for (int m = 0; m < CH; ++m) v[m] = (m < lenA) ? buf[m * W] : T(0);
+    for (int m = 0; m < CH; ++m) v[m] = (m < lenA) ? (CT)buf[m * W] : CT(0);
 
     const size_t row = chunk_row<SMEM_TAB>(tab, c, s, S);
-    T qe, x0;
-    chunk_local<SMEM_TAB, T, CH>(v, lenA, tab.k1 + row, S, qe, x0);
-    Pair<T>* sF = fold + (i & 1) * NC * W;
+    CT qe, x0;
+    chunk_local<SMEM_TAB, CT, CH>(v, lenA, tab.k1 + row, S, qe, x0);
+    Pair<CT>* sF = fold + (i & 1) * NC * W;
     st_fold(sF + c * W + tx, qe, x0);
     // every thread has read its chunk of this stage: it can be refilled
     if (__syncthreads_or(!ok)) {
@@ -315,19 +316,19 @@ __global__ void __launch_bounds__(W * MAXNC)
         ++issued;
       }
     }
-    T cf, cb;
-    chunk_carries<SMEM_TAB, T>(sF, W, tx, c, NC, tab, s, S, cf, cb);
+    CT cf, cb;
+    chunk_carries<SMEM_TAB, CT>(sF, W, tx, c, NC, tab, s, S, cf, cb);
     if (lenA == 0) continue;
-    chunk_fix<SMEM_TAB, T, CH>(v, lenA, tab.kg + row, S, cf, cb);
+    chunk_fix<SMEM_TAB, CT, CH>(v, lenA, tab.kg + row, S, cf, cb);
     if (DIR_EPI) {
       const int64_t vcol = (int64_t)outer * a.C + col;
       const int64_t seg = (vcol / S) * a.nchunks + c;
-      apply_dirichlet_seg<T, CH>(v, a.dir_epi, seg, k0, S, s);
+      apply_dirichlet_seg<CT, CH>(v, a.dir_epi, seg, k0, S, s);
     }
     T* ptr = a.p + (int64_t)outer * a.os + col + (int64_t)k0 * a.ls;
 #pragma unroll
     for (int m = 0; m < CH; ++m) {
-      if (m < lenA) *ptr = v[m];
+      if (m < lenA) *ptr = (T)v[m];
       ptr += a.ls;
     }
   }
@@ -335,8 +336,8 @@ __global__ void __launch_bounds__(W * MAXNC)
 
 // ---------------------------------------------------------------------------
 
-template <typename T, int CH, int STAGES, bool SMEM_TAB, int MAXT>
-__global__ void __launch_bounds__(MAXT) lod_rows_tma_kernel(const RowsArgs<T> a) {
+template <typename T, int CH, int STAGES, bool SMEM_TAB, int MAXT, typename CT = T>
+__global__ void __launch_bounds__(MAXT) lod_rows_tma_kernel(const RowsArgs<T, CT> a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   // Threads: column (r, s) fastest, then chunk c.  A stage holds R rows at a
   // padded pitch (pitch = S mod 16 elements), so the lanes of a warp, which
@@ -351,10 +352,10 @@ __global__ void __launch_bounds__(MAXT) lod_rows_tma_kernel(const RowsArgs<T> a)
   const size_t stage_elems = pitch * R;
   T* tiles =
       reinterpret_cast<T*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~(uintptr_t)127);
-  Pair<T>* fold = reinterpret_cast<Pair<T>*>(tiles + STAGES * stage_elems);  // 2 x [NC][FW]
+  Pair<CT>* fold = reinterpret_cast<Pair<CT>*>(tiles + STAGES * stage_elems);  // 2 x [NC][FW]
   uint64_t* full = reinterpret_cast<uint64_t*>(
       (reinterpret_cast<uintptr_t>(fold + 2 * NC * FW) + 15) & ~(uintptr_t)15);
-  T* sm_tab = reinterpret_cast<T*>(full + 4);  // chunk tables (SMEM_TAB)
+  CT* sm_tab = reinterpret_cast<CT*>(full + 4);  // chunk tables (SMEM_TAB)
   int* sm_slot = reinterpret_cast<int*>(sm_tab + (SMEM_TAB ? a.cc.tab_elems : 0));
 
   const int tid = threadIdx.x;
@@ -365,7 +366,7 @@ __global__ void __launch_bounds__(MAXT) lod_rows_tma_kernel(const RowsArgs<T> a)
   const int s = fc - r * S;
   const int k0 = c * CH;
   const int len = (c < NC) ? max(0, min(CH, n - k0)) : 0;
-  const ChunkCoef<T> tab =
+  const ChunkCoef<CT> tab =
       SMEM_TAB ? stage_tables(a.cc, sm_tab, sm_slot, tid, nthreads) : a.cc;
   if (tid == 0) {
     for (int st = 0; st < STAGES; ++st) tma::mbar_init(&full[st], 1);
@@ -373,8 +374,8 @@ __global__ void __launch_bounds__(MAXT) lod_rows_tma_kernel(const RowsArgs<T> a)
   }
   __syncthreads();
   const size_t crow = (c < NC) ? chunk_row<SMEM_TAB>(tab, c, s, S) : 0;
-  const T* k1 = tab.k1 + crow;
-  const T* kg = tab.kg + crow;
+  const CT* k1 = tab.k1 + crow;
+  const CT* kg = tab.kg + crow;
 
   auto tile_rows = [&](int64_t tile) -> int {
     return (int)min((int64_t)R, a.rows - tile * R);
@@ -406,9 +407,9 @@ __global__ void __launch_bounds__(MAXT) lod_rows_tma_kernel(const RowsArgs<T> a)
     const int64_t row = tile * R + r;
     const int lenA = (r < nr) ? len : 0;
     const T* rb = tiles + st * stage_elems + r * pitch + (size_t)k0 * S + s;
-    T v[CH];
+    CT v[CH];
 #pragma unroll
-    for (int m = 0; m < CH; ++m) v[m] = (m < lenA) ? rb[m * S] : T(0);
+    for (int m = 0; m < CH; ++m) v[m] = (m < lenA) ? (CT)rb[m * S] : CT(0);
 
     // ---- prologue in registers: bulk -> cells -> Dirichlet for this chunk
     const int64_t seg = row * NC + c;
@@ -418,9 +419,9 @@ __global__ void __launch_bounds__(MAXT) lod_rows_tma_kernel(const RowsArgs<T> a)
         for (int e = e0; e < e1; ++e) {
           const int m = __ldg(a.bulk.pos + e) - k0;
           const int64_t q = (int64_t)e * S + s;
-          double x = (double)reg_get<T, CH>(v, m);
+          double x = (double)reg_get<CT, CH>(v, m);
           x = bulk_update(x, __ldg(a.bulk.a + q), __ldg(a.bulk.b + q), a.dt);
-          reg_set<T, CH>(v, m, (T)x);
+          reg_set<CT, CH>(v, m, (CT)x);
         }
       }
       if (a.fuse & kFuseCells) {
@@ -431,22 +432,22 @@ __global__ void __launch_bounds__(MAXT) lod_rows_tma_kernel(const RowsArgs<T> a)
         while (e < e1) {
           const int pos = __ldg(a.cells.pos + e);
           const int m = pos - k0;
-          double x = (double)reg_get<T, CH>(v, m);
+          double x = (double)reg_get<CT, CH>(v, m);
           do {
             const int64_t q = (int64_t)e * S + s;
             x = cell_update(x, __ldg(a.cells.a + q), __ldg(a.cells.b + q));
             ++e;
           } while (e < e1 && __ldg(a.cells.pos + e) == pos);
-          reg_set<T, CH>(v, m, (T)x);
+          reg_set<CT, CH>(v, m, (CT)x);
         }
       }
-      if (a.fuse & kFuseDirPro) apply_dirichlet_seg<T, CH>(v, a.dir, seg, k0, S, s);
+      if (a.fuse & kFuseDirPro) apply_dirichlet_seg<CT, CH>(v, a.dir, seg, k0, S, s);
     }
 
     // ---- sweep
-    T qe, x0;
-    chunk_local<SMEM_TAB, T, CH>(v, lenA, k1, S, qe, x0);
-    Pair<T>* sF = fold + (i & 1) * NC * FW;
+    CT qe, x0;
+    chunk_local<SMEM_TAB, CT, CH>(v, lenA, k1, S, qe, x0);
+    Pair<CT>* sF = fold + (i & 1) * NC * FW;
     if (c < NC) st_fold(sF + c * FW + fc, qe, x0);
     // every thread has its chunk in registers: the stage can be refilled
     if (__syncthreads_or(!ok)) {
@@ -461,17 +462,17 @@ __global__ void __launch_bounds__(MAXT) lod_rows_tma_kernel(const RowsArgs<T> a)
       }
     }
     if (lenA == 0) continue;
-    T cf, cb;
-    chunk_carries<SMEM_TAB, T>(sF, FW, fc, c, NC, tab, s, S, cf, cb);
-    chunk_fix<SMEM_TAB, T, CH>(v, lenA, kg, S, cf, cb);
+    CT cf, cb;
+    chunk_carries<SMEM_TAB, CT>(sF, FW, fc, c, NC, tab, s, S, cf, cb);
+    chunk_fix<SMEM_TAB, CT, CH>(v, lenA, kg, S, cf, cb);
     // ---- epilogue: Dirichlet before the next axis
-    if (a.fuse & kFuseDirEpi) apply_dirichlet_seg<T, CH>(v, a.dir, seg, k0, S, s);
+    if (a.fuse & kFuseDirEpi) apply_dirichlet_seg<CT, CH>(v, a.dir, seg, k0, S, s);
     // straight to global memory: the lanes of a warp write the S densities of
     // consecutive rows at one point
     T* out = a.p + row * (int64_t)row_elems + (int64_t)k0 * S + s;
 #pragma unroll
     for (int m = 0; m < CH; ++m)
-      if (m < lenA) out[(int64_t)m * S] = v[m];
+      if (m < lenA) out[(int64_t)m * S] = (T)v[m];
   }
 }
 
@@ -486,7 +487,7 @@ __global__ void __launch_bounds__(MAXT) lod_rows_tma_kernel(const RowsArgs<T> a)
 // for x the rest of the step (bulk, cells, Dirichlet) is applied to the
 // chunk in registers before the sweep.
 
-template <typename T>
+template <typename T, typename CT = T>
 struct DirectArgs {
   T* p;
   int64_t ncols;         // (line, density) columns
@@ -496,19 +497,19 @@ struct DirectArgs {
   int n;
   int nchunks;
   int S;
-  ChunkCoef<T> cc;
+  ChunkCoef<CT> cc;
   SegList bulk, cells, dir_pro, dir_epi;
   double dt;
   int fuse;
 };
 
-template <typename T, int CH, int W, int MODE>
-__global__ void __launch_bounds__(512) lod_sweep_direct_kernel(const DirectArgs<T> a) {
+template <typename T, int CH, int W, int MODE, typename CT = T>
+__global__ void __launch_bounds__(512) lod_sweep_direct_kernel(const DirectArgs<T, CT> a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int NC = blockDim.y;
-  Pair<T>* fold = reinterpret_cast<Pair<T>*>(smem_raw);  // [NC][W]
+  Pair<CT>* fold = reinterpret_cast<Pair<CT>*>(smem_raw);  // [NC][W]
   // this block's copy of the per-chunk constants and the slot map
-  T* kc_sm = reinterpret_cast<T*>(fold + NC * W);        // [NC][S][4]
+  CT* kc_sm = reinterpret_cast<CT*>(fold + NC * W);        // [NC][S][4]
   int* slot_sm = reinterpret_cast<int*>(kc_sm + (size_t)4 * NC * a.S);
   const int tx = threadIdx.x;
   const int c = threadIdx.y;
@@ -534,12 +535,12 @@ __global__ void __launch_bounds__(512) lod_sweep_direct_kernel(const DirectArgs<
   }
   const int64_t ls = a.line_stride;
 
-  T v[CH];
+  CT v[CH];
   {
     const T* q = ptr;
 #pragma unroll
     for (int m = 0; m < CH; ++m) {
-      v[m] = (m < lenA) ? *q : T(0);
+      v[m] = (m < lenA) ? (CT)*q : CT(0);
       q += ls;
     }
   }
@@ -550,9 +551,9 @@ __global__ void __launch_bounds__(512) lod_sweep_direct_kernel(const DirectArgs<
       for (int e = e0; e < e1; ++e) {
         const int m = __ldg(a.bulk.pos + e) - k0;
         const int64_t q = (int64_t)e * S + s;
-        double x = (double)reg_get<T, CH>(v, m);
+        double x = (double)reg_get<CT, CH>(v, m);
         x = bulk_update(x, __ldg(a.bulk.a + q), __ldg(a.bulk.b + q), a.dt);
-        reg_set<T, CH>(v, m, (T)x);
+        reg_set<CT, CH>(v, m, (CT)x);
       }
     }
     if (a.fuse & kFuseCells) {
@@ -563,36 +564,36 @@ __global__ void __launch_bounds__(512) lod_sweep_direct_kernel(const DirectArgs<
       while (e < e1) {
         const int pos = __ldg(a.cells.pos + e);
         const int m = pos - k0;
-        double x = (double)reg_get<T, CH>(v, m);
+        double x = (double)reg_get<CT, CH>(v, m);
         do {
           const int64_t q = (int64_t)e * S + s;
           x = cell_update(x, __ldg(a.cells.a + q), __ldg(a.cells.b + q));
           ++e;
         } while (e < e1 && __ldg(a.cells.pos + e) == pos);
-        reg_set<T, CH>(v, m, (T)x);
+        reg_set<CT, CH>(v, m, (CT)x);
       }
     }
-    if (a.fuse & kFuseDirPro) apply_dirichlet_seg<T, CH>(v, a.dir_pro, seg, k0, S, s);
+    if (a.fuse & kFuseDirPro) apply_dirichlet_seg<CT, CH>(v, a.dir_pro, seg, k0, S, s);
   }
 
   __syncthreads();  // kc_sm, slot_sm
-  ChunkCoef<T> tab = a.cc;
+  ChunkCoef<CT> tab = a.cc;
   tab.kc = kc_sm;
   tab.slot = slot_sm;
   const size_t row = active ? ((size_t)slot_sm[c] * tab.ch * S + s) * 2 : 0;
-  T qe, x0;
-  chunk_local<false, T, CH>(v, lenA, a.cc.k1 + row, S, qe, x0);
+  CT qe, x0;
+  chunk_local<false, CT, CH>(v, lenA, a.cc.k1 + row, S, qe, x0);
   st_fold(fold + c * W + tx, qe, x0);
   __syncthreads();
-  T cf, cb;
-  chunk_carries<true, T>(fold, W, tx, c, NC, tab, s, S, cf, cb);
+  CT cf, cb;
+  chunk_carries<true, CT>(fold, W, tx, c, NC, tab, s, S, cf, cb);
   if (lenA == 0) return;
-  chunk_fix<false, T, CH>(v, lenA, a.cc.kg + row, S, cf, cb);
+  chunk_fix<false, CT, CH>(v, lenA, a.cc.kg + row, S, cf, cb);
   if (MODE != kSweepPlain && (a.fuse & kFuseDirEpi))
-    apply_dirichlet_seg<T, CH>(v, a.dir_epi, seg, k0, S, s);
+    apply_dirichlet_seg<CT, CH>(v, a.dir_epi, seg, k0, S, s);
 #pragma unroll
   for (int m = 0; m < CH; ++m) {
-    if (m < lenA) *ptr = v[m];
+    if (m < lenA) *ptr = (T)v[m];
     ptr += ls;
   }
 }

@@ -105,7 +105,7 @@ void thomas_setup(bfvm_solver* m, double dt) {
       tab[(size_t)2 * n * S + i] = -cx[i];
     }
     for (int s = 0; s < S; ++s) tab[(size_t)3 * n * S + s] = c1[s];
-    if (m->precision == BFVM_FP64) {
+    if (m->math_elem() == sizeof(double)) {
       upload(m->coef[a], tab, m->stream);
     } else {
       std::vector<float> tf(tab.begin(), tab.end());
@@ -406,35 +406,35 @@ void build_all(bfvm_solver* m) {
 
 // ---- launches ---------------------------------------------------------------
 
-template <typename T, int CH, int MINB>
-void launch_sweep_mb(const bfvm::SweepArgs<T>& a, int mode, dim3 grid, dim3 block, size_t smem,
+template <typename T, typename CT, int CH, int MINB>
+void launch_sweep_mb(const bfvm::SweepArgs<T, CT>& a, int mode, dim3 grid, dim3 block, size_t smem,
                      cudaStream_t st) {
   if (mode == bfvm::kSweepFull)
-    bfvm::lod_sweep_kernel<T, CH, bfvm::kSweepFull, MINB><<<grid, block, smem, st>>>(a);
+    bfvm::lod_sweep_kernel<T, CH, bfvm::kSweepFull, MINB, CT><<<grid, block, smem, st>>>(a);
   else if (mode == bfvm::kSweepDirEpi)
-    bfvm::lod_sweep_kernel<T, CH, bfvm::kSweepDirEpi, MINB><<<grid, block, smem, st>>>(a);
+    bfvm::lod_sweep_kernel<T, CH, bfvm::kSweepDirEpi, MINB, CT><<<grid, block, smem, st>>>(a);
   else
-    bfvm::lod_sweep_kernel<T, CH, bfvm::kSweepPlain, MINB><<<grid, block, smem, st>>>(a);
+    bfvm::lod_sweep_kernel<T, CH, bfvm::kSweepPlain, MINB, CT><<<grid, block, smem, st>>>(a);
 }
 
-template <typename T, int CH>
-void launch_sweep_ch(const bfvm::SweepArgs<T>& a, int mode, int minb, dim3 grid, dim3 block,
+template <typename T, typename CT, int CH>
+void launch_sweep_ch(const bfvm::SweepArgs<T, CT>& a, int mode, int minb, dim3 grid, dim3 block,
                      size_t smem, cudaStream_t st) {
   if (minb == 2)
-    launch_sweep_mb<T, CH, 2>(a, mode, grid, block, smem, st);
+    launch_sweep_mb<T, CT, CH, 2>(a, mode, grid, block, smem, st);
   else
-    launch_sweep_mb<T, CH, 1>(a, mode, grid, block, smem, st);
+    launch_sweep_mb<T, CT, CH, 1>(a, mode, grid, block, smem, st);
 }
 
-template <typename T>
+template <typename T, typename CT>
 void launch_sweep(bfvm_solver* m, int ax, int fuse, double dt) {
   const int S = m->S;
   const int64_t nx = m->nx, ny = m->ny, nz = m->nz;
-  bfvm::SweepArgs<T> a{};
+  bfvm::SweepArgs<T, CT> a{};
   a.p = m->p.as<T>();
   a.S = S;
   a.dt = dt;
-  a.coef = coef_view<T>(m, ax);
+  a.coef = coef_view<CT>(m, ax);
   const int64_t nzp = (m->lod_dims == 2) ? 1 : nz;  // planes swept
   if (ax == 0) {
     a.n = (int)nx;
@@ -468,16 +468,16 @@ void launch_sweep(bfvm_solver* m, int ax, int fuse, double dt) {
   a.dir_epi = dseg.view();
   dim3 block(A.tw, a.nchunks);
   dim3 grid((unsigned)blocks_for(a.ncols, A.tw));
-  const size_t smem = 4 * sizeof(T) * (size_t)A.tw * a.nchunks;
+  const size_t smem = 4 * sizeof(CT) * (size_t)A.tw * a.nchunks;
   int mode = bfvm::kSweepPlain;
   if (fuse & (bfvm::kFuseBulk | bfvm::kFuseCells | bfvm::kFuseDirPro))
     mode = bfvm::kSweepFull;
   else if (fuse & bfvm::kFuseDirEpi)
     mode = bfvm::kSweepDirEpi;
   switch (A.ch) {
-    case 8: launch_sweep_ch<T, 8>(a, mode, A.minb, grid, block, smem, m->stream); break;
-    case 16: launch_sweep_ch<T, 16>(a, mode, A.minb, grid, block, smem, m->stream); break;
-    case 32: launch_sweep_ch<T, 32>(a, mode, A.minb, grid, block, smem, m->stream); break;
+    case 8: launch_sweep_ch<T, CT, 8>(a, mode, A.minb, grid, block, smem, m->stream); break;
+    case 16: launch_sweep_ch<T, CT, 16>(a, mode, A.minb, grid, block, smem, m->stream); break;
+    case 32: launch_sweep_ch<T, CT, 32>(a, mode, A.minb, grid, block, smem, m->stream); break;
     default: throw Error(BFVM_ERR_STATE, "unsupported chunk length");
   }
   check_launch(m);
@@ -520,7 +520,7 @@ size_t table_bytes(const bfvm_solver* m, int a) {
   const size_t ch = m->axis[a].ch, S = m->S, nsl = m->chunk_nslots[a];
   const size_t nc = (ns[a] + ch - 1) / ch;
   const size_t elems = up4(nsl * ch * S * 2) * 2 + up4(nc * S * 4);
-  return elems * m->elem() + nc * sizeof(int) + 16;
+  return elems * m->math_elem() + nc * sizeof(int) + 16;
 }
 
 struct LinesPlan {
@@ -548,14 +548,14 @@ LinesPlan plan_lines(const bfvm_solver* m, int ax) {
   // the chunk length of the axis: the (line, chunk) segment lists are built with it
   L.ch = m->axis[ax].ch;
   L.nc = (L.n + L.ch - 1) / L.ch;
-  L.w = (es == 8) ? 16 : 32;
+  L.w = (m->math_elem() == 8) ? 16 : 32;
   if (L.nc > 16) return L;
   L.box_n = std::min(L.n, 256);
   L.nboxes = (L.n + L.box_n - 1) / L.box_n;
   const int64_t ctiles = (L.C + L.w - 1) / L.w;
   if (ctiles * L.nouter >= ((int64_t)1 << 31)) return L;
   const size_t stage = (size_t)L.box_n * L.nboxes * L.w * es;
-  const size_t fold = 4 * (size_t)L.nc * L.w * es;  // two parities of (qe, x0) pairs
+  const size_t fold = 4 * (size_t)L.nc * L.w * m->math_elem();  // two parities of (qe, x0) pairs
   const size_t extra = 8 * 4 + 128;
   const size_t tab = table_bytes(m, ax);
   // preferred: the chunk tables staged in shared memory, two blocks per SM
@@ -638,7 +638,7 @@ RowsPlan plan_rows(const bfvm_solver* m) {
       if (staged && tab == 0) continue;
       for (int R = (int)std::min<int64_t>(maxt / cols, rows); R >= 1; --R) {
         const size_t stage = (size_t)(R * pitch * es);
-        const size_t fold = 4 * (size_t)P.nc * R * m->S * es;  // two parities of (qe, x0)
+        const size_t fold = 4 * (size_t)P.nc * R * m->S * m->math_elem();  // two parities of (qe, x0)
         const size_t t = staged ? tab : 0;
         const size_t smem = 2 * stage + fold + extra + t;
         if (smem > budget) continue;
@@ -655,11 +655,11 @@ RowsPlan plan_rows(const bfvm_solver* m) {
   return P;
 }
 
-template <typename T, int CH, int ST, bool DIR, bool TAB, int MAXNC>
-void launch_lines_nc(const CUtensorMap& map, const bfvm::LinesArgs<T>& a, int ntiles,
+template <typename T, typename CT, int CH, int ST, bool DIR, bool TAB, int MAXNC>
+void launch_lines_nc(const CUtensorMap& map, const bfvm::LinesArgs<T, CT>& a, int ntiles,
                      dim3 block, size_t smem, bfvm_solver* m) {
-  constexpr int W = sizeof(T) == 8 ? 16 : 32;
-  auto k = bfvm::lod_lines_tma_kernel<T, CH, W, ST, DIR, TAB, MAXNC>;
+  constexpr int W = sizeof(CT) == 8 ? 16 : 32;
+  auto k = bfvm::lod_lines_tma_kernel<T, CH, W, ST, DIR, TAB, MAXNC, CT>;
   allow_smem((const void*)k, m->device, smem);
   int per_sm = 0;
   BFVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, block.x * block.y, smem));
@@ -670,47 +670,47 @@ void launch_lines_nc(const CUtensorMap& map, const bfvm::LinesArgs<T>& a, int nt
 
 // Lines of up to 8 chunks of 32 points take the kernel compiled for 8 chunks
 // (more registers per thread); longer lines the one for 16.
-template <typename T, int CH, int ST, bool DIR, bool TAB>
-void launch_lines_inst(const CUtensorMap& map, const bfvm::LinesArgs<T>& a, int ntiles,
+template <typename T, typename CT, int CH, int ST, bool DIR, bool TAB>
+void launch_lines_inst(const CUtensorMap& map, const bfvm::LinesArgs<T, CT>& a, int ntiles,
                        dim3 block, size_t smem, bfvm_solver* m) {
   if constexpr (CH >= 32) {
     if (block.y <= 8) {
-      launch_lines_nc<T, CH, ST, DIR, TAB, 8>(map, a, ntiles, block, smem, m);
+      launch_lines_nc<T, CT, CH, ST, DIR, TAB, 8>(map, a, ntiles, block, smem, m);
       return;
     }
   }
-  launch_lines_nc<T, CH, ST, DIR, TAB, 16>(map, a, ntiles, block, smem, m);
+  launch_lines_nc<T, CT, CH, ST, DIR, TAB, 16>(map, a, ntiles, block, smem, m);
 }
 
-template <typename T, int CH, int ST, bool TAB>
-void launch_lines_dir(const CUtensorMap& map, const bfvm::LinesArgs<T>& a, bool dir, int ntiles,
+template <typename T, typename CT, int CH, int ST, bool TAB>
+void launch_lines_dir(const CUtensorMap& map, const bfvm::LinesArgs<T, CT>& a, bool dir, int ntiles,
                       dim3 block, size_t smem, bfvm_solver* m) {
   if (dir)
-    launch_lines_inst<T, CH, ST, true, TAB>(map, a, ntiles, block, smem, m);
+    launch_lines_inst<T, CT, CH, ST, true, TAB>(map, a, ntiles, block, smem, m);
   else
-    launch_lines_inst<T, CH, ST, false, TAB>(map, a, ntiles, block, smem, m);
+    launch_lines_inst<T, CT, CH, ST, false, TAB>(map, a, ntiles, block, smem, m);
 }
 
-template <typename T, int CH, int ST>
-void launch_lines_tab(const CUtensorMap& map, const bfvm::LinesArgs<T>& a, bool dir, bool tab,
+template <typename T, typename CT, int CH, int ST>
+void launch_lines_tab(const CUtensorMap& map, const bfvm::LinesArgs<T, CT>& a, bool dir, bool tab,
                       int ntiles, dim3 block, size_t smem, bfvm_solver* m) {
   if (tab)
-    launch_lines_dir<T, CH, ST, true>(map, a, dir, ntiles, block, smem, m);
+    launch_lines_dir<T, CT, CH, ST, true>(map, a, dir, ntiles, block, smem, m);
   else
-    launch_lines_dir<T, CH, ST, false>(map, a, dir, ntiles, block, smem, m);
+    launch_lines_dir<T, CT, CH, ST, false>(map, a, dir, ntiles, block, smem, m);
 }
 
-template <typename T, int CH>
-void launch_lines_st(const CUtensorMap& map, const bfvm::LinesArgs<T>& a, int stages, bool dir,
+template <typename T, typename CT, int CH>
+void launch_lines_st(const CUtensorMap& map, const bfvm::LinesArgs<T, CT>& a, int stages, bool dir,
                      bool tab, int ntiles, dim3 block, size_t smem, bfvm_solver* m) {
   switch (stages) {
-    case 2: launch_lines_tab<T, CH, 2>(map, a, dir, tab, ntiles, block, smem, m); break;
-    case 3: launch_lines_tab<T, CH, 3>(map, a, dir, tab, ntiles, block, smem, m); break;
-    default: launch_lines_tab<T, CH, 4>(map, a, dir, tab, ntiles, block, smem, m); break;
+    case 2: launch_lines_tab<T, CT, CH, 2>(map, a, dir, tab, ntiles, block, smem, m); break;
+    case 3: launch_lines_tab<T, CT, CH, 3>(map, a, dir, tab, ntiles, block, smem, m); break;
+    default: launch_lines_tab<T, CT, CH, 4>(map, a, dir, tab, ntiles, block, smem, m); break;
   }
 }
 
-template <typename T>
+template <typename T, typename CT>
 void launch_lines(bfvm_solver* m, int ax, const LinesPlan& L, bool dir) {
   // (re)encode the tensor map when the field moved
   if (m->map_key[ax] != m->p.ptr || m->map_w[ax] != L.w) {
@@ -729,7 +729,7 @@ void launch_lines(bfvm_solver* m, int ax, const LinesPlan& L, bool dir) {
     m->map_key[ax] = m->p.ptr;
     m->map_w[ax] = L.w;
   }
-  bfvm::LinesArgs<T> a{};
+  bfvm::LinesArgs<T, CT> a{};
   a.p = m->p.as<T>();
   a.C = L.C;
   a.n = L.n;
@@ -741,44 +741,44 @@ void launch_lines(bfvm_solver* m, int ax, const LinesPlan& L, bool dir) {
   a.box_n = L.box_n;
   a.nboxes = L.nboxes;
   a.nchunks = L.nc;
-  a.cc = chunk_view<T>(m, ax);
+  a.cc = chunk_view<CT>(m, ax);
   a.status = m->d_status.as<int>();
   if (dir) a.dir_epi = m->seg_dir_y.view();
   dim3 block(L.w, L.nc);
   switch (L.ch) {
-    case 8: launch_lines_st<T, 8>(m->maps[ax], a, L.stages, dir, L.smem_tab, a.ntiles, block, L.smem, m); break;
-    case 16: launch_lines_st<T, 16>(m->maps[ax], a, L.stages, dir, L.smem_tab, a.ntiles, block, L.smem, m); break;
-    default: launch_lines_st<T, 32>(m->maps[ax], a, L.stages, dir, L.smem_tab, a.ntiles, block, L.smem, m); break;
+    case 8: launch_lines_st<T, CT, 8>(m->maps[ax], a, L.stages, dir, L.smem_tab, a.ntiles, block, L.smem, m); break;
+    case 16: launch_lines_st<T, CT, 16>(m->maps[ax], a, L.stages, dir, L.smem_tab, a.ntiles, block, L.smem, m); break;
+    default: launch_lines_st<T, CT, 32>(m->maps[ax], a, L.stages, dir, L.smem_tab, a.ntiles, block, L.smem, m); break;
   }
   check_launch(m);
 }
 
-template <typename T, int CH, int MODE>
-void launch_direct_inst(const bfvm::DirectArgs<T>& a, dim3 grid, dim3 block, bfvm_solver* m) {
+template <typename T, typename CT, int CH, int MODE>
+void launch_direct_inst(const bfvm::DirectArgs<T, CT>& a, dim3 grid, dim3 block, bfvm_solver* m) {
   constexpr int W = 32;
-  auto k = bfvm::lod_sweep_direct_kernel<T, CH, W, MODE>;
+  auto k = bfvm::lod_sweep_direct_kernel<T, CH, W, MODE, CT>;
   // fold pairs + per-chunk constants + slot map
-  const size_t smem = sizeof(T) * 2 * block.x * block.y + sizeof(T) * 4 * block.y * a.S +
+  const size_t smem = sizeof(CT) * 2 * block.x * block.y + sizeof(CT) * 4 * block.y * a.S +
                       sizeof(int) * block.y + 16;
   k<<<grid, block, smem, m->stream>>>(a);
 }
 
-template <typename T, int CH>
-void launch_direct_mode(const bfvm::DirectArgs<T>& a, int mode, dim3 grid, dim3 block,
+template <typename T, typename CT, int CH>
+void launch_direct_mode(const bfvm::DirectArgs<T, CT>& a, int mode, dim3 grid, dim3 block,
                         bfvm_solver* m) {
   if (mode == bfvm::kSweepFull)
-    launch_direct_inst<T, CH, bfvm::kSweepFull>(a, grid, block, m);
+    launch_direct_inst<T, CT, CH, bfvm::kSweepFull>(a, grid, block, m);
   else if (mode == bfvm::kSweepDirEpi)
-    launch_direct_inst<T, CH, bfvm::kSweepDirEpi>(a, grid, block, m);
+    launch_direct_inst<T, CT, CH, bfvm::kSweepDirEpi>(a, grid, block, m);
   else
-    launch_direct_inst<T, CH, bfvm::kSweepPlain>(a, grid, block, m);
+    launch_direct_inst<T, CT, CH, bfvm::kSweepPlain>(a, grid, block, m);
 }
 
 // Any axis with direct loads: blocks of 32 columns x all chunks of a line.
-template <typename T>
+template <typename T, typename CT>
 bool launch_direct(bfvm_solver* m, int ax, int fuse, double dt) {
   const int64_t nx = m->nx, ny = m->ny, nz = m->nz, S = m->S;
-  bfvm::DirectArgs<T> a{};
+  bfvm::DirectArgs<T, CT> a{};
   const int64_t nzp = (m->lod_dims == 2) ? 1 : nz;  // planes swept
   if (ax == 0) {
     a.n = (int)nx; a.C = S; a.outer_stride = nx * S; a.line_stride = S; a.ncols = ny * nzp * S;
@@ -797,7 +797,7 @@ bool launch_direct(bfvm_solver* m, int ax, int fuse, double dt) {
   a.p = m->p.as<T>();
   a.S = (int)S;
   a.nchunks = nc;
-  a.cc = chunk_view<T>(m, ax);
+  a.cc = chunk_view<CT>(m, ax);
   a.dt = dt;
   if ((fuse & bfvm::kFuseBulk) && !m->seg_bulk.present) fuse &= ~bfvm::kFuseBulk;
   if ((fuse & bfvm::kFuseCells) && !m->seg_cells.present) fuse &= ~bfvm::kFuseCells;
@@ -816,17 +816,17 @@ bool launch_direct(bfvm_solver* m, int ax, int fuse, double dt) {
   dim3 block(W, nc);
   dim3 grid((unsigned)nblocks);
   switch (ch) {
-    case 8: launch_direct_mode<T, 8>(a, mode, grid, block, m); break;
-    case 16: launch_direct_mode<T, 16>(a, mode, grid, block, m); break;
-    default: launch_direct_mode<T, 32>(a, mode, grid, block, m); break;
+    case 8: launch_direct_mode<T, CT, 8>(a, mode, grid, block, m); break;
+    case 16: launch_direct_mode<T, CT, 16>(a, mode, grid, block, m); break;
+    default: launch_direct_mode<T, CT, 32>(a, mode, grid, block, m); break;
   }
   check_launch(m);
   return true;
 }
 
-template <typename T, int CH, bool TAB, int MAXT>
-void launch_rows_inst(const bfvm::RowsArgs<T>& a, dim3 block, size_t smem, bfvm_solver* m) {
-  auto k = bfvm::lod_rows_tma_kernel<T, CH, 2, TAB, MAXT>;
+template <typename T, typename CT, int CH, bool TAB, int MAXT>
+void launch_rows_inst(const bfvm::RowsArgs<T, CT>& a, dim3 block, size_t smem, bfvm_solver* m) {
+  auto k = bfvm::lod_rows_tma_kernel<T, CH, 2, TAB, MAXT, CT>;
   allow_smem((const void*)k, m->device, smem);
   int per_sm = 0;
   BFVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, block.x * block.y, smem));
@@ -835,24 +835,24 @@ void launch_rows_inst(const bfvm::RowsArgs<T>& a, dim3 block, size_t smem, bfvm_
   k<<<grid, block, smem, m->stream>>>(a);
 }
 
-template <typename T, int CH>
-void launch_rows_ch(const bfvm::RowsArgs<T>& a, const RowsPlan& P, dim3 block, bfvm_solver* m) {
+template <typename T, typename CT, int CH>
+void launch_rows_ch(const bfvm::RowsArgs<T, CT>& a, const RowsPlan& P, dim3 block, bfvm_solver* m) {
   if (P.maxt == 256) {
     if (P.smem_tab)
-      launch_rows_inst<T, CH, true, 256>(a, block, P.smem, m);
+      launch_rows_inst<T, CT, CH, true, 256>(a, block, P.smem, m);
     else
-      launch_rows_inst<T, CH, false, 256>(a, block, P.smem, m);
+      launch_rows_inst<T, CT, CH, false, 256>(a, block, P.smem, m);
   } else {
     if (P.smem_tab)
-      launch_rows_inst<T, CH, true, 512>(a, block, P.smem, m);
+      launch_rows_inst<T, CT, CH, true, 512>(a, block, P.smem, m);
     else
-      launch_rows_inst<T, CH, false, 512>(a, block, P.smem, m);
+      launch_rows_inst<T, CT, CH, false, 512>(a, block, P.smem, m);
   }
 }
 
-template <typename T>
+template <typename T, typename CT>
 void launch_rows(bfvm_solver* m, const RowsPlan& P, int fuse, double dt) {
-  bfvm::RowsArgs<T> a{};
+  bfvm::RowsArgs<T, CT> a{};
   a.p = m->p.as<T>();
   a.rows = (int64_t)m->ny * (m->lod_dims == 2 ? 1 : m->nz);
   a.n = m->nx;
@@ -861,7 +861,7 @@ void launch_rows(bfvm_solver* m, const RowsPlan& P, int fuse, double dt) {
   a.nchunks = P.nc;
   a.R = P.R;
   a.pitch = P.pitch;
-  a.cc = chunk_view<T>(m, 0);
+  a.cc = chunk_view<CT>(m, 0);
   a.dt = dt;
   if ((fuse & bfvm::kFuseBulk) && !m->seg_bulk.present) fuse &= ~bfvm::kFuseBulk;
   if ((fuse & bfvm::kFuseCells) && !m->seg_cells.present) fuse &= ~bfvm::kFuseCells;
@@ -874,61 +874,60 @@ void launch_rows(bfvm_solver* m, const RowsPlan& P, int fuse, double dt) {
   // whole warps: threads past R*S*NC idle through the sweep
   dim3 block((unsigned)((P.R * m->S * P.nc + 31) / 32 * 32));
   switch (P.ch) {
-    case 8: launch_rows_ch<T, 8>(a, P, block, m); break;
-    case 16: launch_rows_ch<T, 16>(a, P, block, m); break;
-    default: launch_rows_ch<T, 32>(a, P, block, m); break;
+    case 8: launch_rows_ch<T, CT, 8>(a, P, block, m); break;
+    case 16: launch_rows_ch<T, CT, 16>(a, P, block, m); break;
+    default: launch_rows_ch<T, CT, 32>(a, P, block, m); break;
   }
   check_launch(m);
 }
 
+// The field's element type T and the type the sweeps compute in: FP64 over
+// FP64, FP32 over FP32, or FP64 arithmetic over an FP32 field.
+template <typename F>
+void with_types(const bfvm_solver* m, F&& f) {
+  if (m->precision == BFVM_FP64)
+    f(double(), double());
+  else if (m->precision == BFVM_FP32_FP64MATH)
+    f(float(), double());
+  else
+    f(float(), float());
+}
+
 void sweep(bfvm_solver* m, int ax, int fuse, double dt) {
-  const bool fp64 = m->precision == BFVM_FP64;
   // under AUTO an axis may carry its own kernel choice (bfvm_tune_sweeps)
   const int path =
       (m->path == BFVM_PATH_AUTO && m->axis[ax].kind) ? m->axis[ax].kind : m->path;
-  if (path != BFVM_PATH_GENERIC) {
-    // build the chunk tables first: the plans size shared memory from them
-    if (fp64)
-      chunk_view<double>(m, ax);
-    else
-      chunk_view<float>(m, ax);
-    // AUTO: the register kernel for x (measured fastest there), TMA tiles
-    // for y and z
-    if (path == BFVM_PATH_AUTO && ax == 0) {
-      if (fp64)
-        launch_sweep<double>(m, ax, fuse, dt);
-      else
-        launch_sweep<float>(m, ax, fuse, dt);
-      return;
-    }
-    const bool want_tma = (path == BFVM_PATH_TMA) || (path == BFVM_PATH_AUTO);
-    if (want_tma && ax == 0) {
-      const RowsPlan P = plan_rows(m);
-      if (P.ok) {
-        if (fp64)
-          launch_rows<double>(m, P, fuse, dt);
-        else
-          launch_rows<float>(m, P, fuse, dt);
+  with_types(m, [&](auto t, auto ct) {
+    using T = decltype(t);
+    using CT = decltype(ct);
+    if (path != BFVM_PATH_GENERIC) {
+      // build the chunk tables first: the plans size shared memory from them
+      chunk_view<CT>(m, ax);
+      // AUTO: the register kernel for x (measured fastest there), TMA tiles
+      // for y and z
+      if (path == BFVM_PATH_AUTO && ax == 0) {
+        launch_sweep<T, CT>(m, ax, fuse, dt);
         return;
       }
-    } else if (want_tma) {
-      const LinesPlan L = plan_lines(m, ax);
-      if (L.ok) {
-        const bool dir = (ax == 1) && (fuse & bfvm::kFuseDirEpi) && m->seg_dir_y.present;
-        if (fp64)
-          launch_lines<double>(m, ax, L, dir);
-        else
-          launch_lines<float>(m, ax, L, dir);
-        return;
+      const bool want_tma = (path == BFVM_PATH_TMA) || (path == BFVM_PATH_AUTO);
+      if (want_tma && ax == 0) {
+        const RowsPlan P = plan_rows(m);
+        if (P.ok) {
+          launch_rows<T, CT>(m, P, fuse, dt);
+          return;
+        }
+      } else if (want_tma) {
+        const LinesPlan L = plan_lines(m, ax);
+        if (L.ok) {
+          const bool dir = (ax == 1) && (fuse & bfvm::kFuseDirEpi) && m->seg_dir_y.present;
+          launch_lines<T, CT>(m, ax, L, dir);
+          return;
+        }
       }
+      if (launch_direct<T, CT>(m, ax, fuse, dt)) return;
     }
-    if (fp64 ? launch_direct<double>(m, ax, fuse, dt) : launch_direct<float>(m, ax, fuse, dt))
-      return;
-  }
-  if (fp64)
-    launch_sweep<double>(m, ax, fuse, dt);
-  else
-    launch_sweep<float>(m, ax, fuse, dt);
+    launch_sweep<T, CT>(m, ax, fuse, dt);
+  });
 }
 
 void check_status(bfvm_solver* m) {
@@ -1666,26 +1665,32 @@ int bfvm_reset_diffusion_setup(bfvm_solver* m) {
 
 int bfvm_set_precision(bfvm_solver* m, int precision) {
   return SOLVER_CALL(m, {
-    require(precision == BFVM_FP64 || precision == BFVM_FP32, "precision must be 64 or 32");
+    require(precision == BFVM_FP64 || precision == BFVM_FP32 || precision == BFVM_FP32_FP64MATH,
+            "precision must be BFVM_FP64, BFVM_FP32 or BFVM_FP32_FP64MATH");
     if (precision == m->precision) return;
-    const int64_t NS = m->NS();
-    DevBuf np;
-    np.ensure(std::max<size_t>(NS * (precision == BFVM_FP64 ? 8 : 4), 16));
-    if (NS > 0) {
-      if (precision == BFVM_FP32)
-        bfvm::convert_kernel<float, double><<<(unsigned)blocks_for(NS, 256), 256, 0, m->stream>>>(
-            np.as<float>(), m->p.as<double>(), NS);
-      else
-        bfvm::convert_kernel<double, float><<<(unsigned)blocks_for(NS, 256), 256, 0, m->stream>>>(
-            np.as<double>(), m->p.as<float>(), NS);
-      check_launch(m);
+    const bool was64 = m->precision == BFVM_FP64, is64 = precision == BFVM_FP64;
+    if (was64 != is64) {  // the field changes element type
+      const int64_t NS = m->NS();
+      DevBuf np;
+      np.ensure(std::max<size_t>(NS * (is64 ? 8 : 4), 16));
+      if (NS > 0) {
+        if (!is64)
+          bfvm::convert_kernel<float, double>
+              <<<(unsigned)blocks_for(NS, 256), 256, 0, m->stream>>>(np.as<float>(),
+                                                                   m->p.as<double>(), NS);
+        else
+          bfvm::convert_kernel<double, float>
+              <<<(unsigned)blocks_for(NS, 256), 256, 0, m->stream>>>(np.as<double>(),
+                                                                   m->p.as<float>(), NS);
+        check_launch(m);
+      }
+      BFVM_CUDA(cudaStreamSynchronize(m->stream));
+      m->p.release();
+      m->p = np;
+      np.ptr = nullptr;
     }
-    BFVM_CUDA(cudaStreamSynchronize(m->stream));
-    m->p.release();
-    m->p = np;
-    np.ptr = nullptr;
     m->precision = precision;
-    m->setup_done = false;  // coefficient tables are kept in the sweep precision
+    m->setup_done = false;  // coefficient tables are kept in the sweeps' arithmetic type
     choose_axes(m);
     // segment lists depend on the chunk lengths
     m->bulk_dirty = m->dir_dirty = m->ag_seg_dirty = true;

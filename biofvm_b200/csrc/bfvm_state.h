@@ -206,6 +206,8 @@ struct bfvm_solver {
   int64_t N() const { return (int64_t)nx * ny * nz; }
   int64_t NS() const { return N() * S; }
   size_t elem() const { return precision == BFVM_FP64 ? sizeof(double) : sizeof(float); }
+  // element size of the sweeps' arithmetic and coefficient tables
+  size_t math_elem() const { return precision == BFVM_FP32 ? sizeof(float) : sizeof(double); }
 };
 
 namespace bfvm_rt {

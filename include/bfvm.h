@@ -44,6 +44,9 @@ extern "C" {
 /* precision of the density field and the sweeps */
 #define BFVM_FP64 64
 #define BFVM_FP32 32
+/* FP32 field (half the memory traffic of FP64) swept in FP64 arithmetic with
+ * FP64 coefficients: only the stored field is rounded to FP32 */
+#define BFVM_FP32_FP64MATH 3264
 
 typedef struct bfvm_solver bfvm_solver;
 

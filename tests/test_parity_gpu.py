@@ -9,7 +9,7 @@ import pytest
 
 from biofvm_b200 import STEP_BULK, STEP_CELLS, STEP_DIFFUSION, Solver, load_scenario
 from biofvm_b200 import workloads as W
-from biofvm_b200._abi import PATH_AUTO, PATH_DIRECT, PATH_GENERIC, PATH_TMA, BfvmError
+from biofvm_b200._abi import FP32_FP64MATH, PATH_AUTO, PATH_DIRECT, PATH_GENERIC, PATH_TMA, BfvmError
 from cases import CASES, sha
 from conftest import load_golden
 from oracle import oracle as O
@@ -187,6 +187,18 @@ def test_fp32_sweeps_error_bound(path):
     p32 = run_gpu(scn, 20, 7, precision=32, path=path)
     err = rel_err(p32, ref)
     assert np.all(err <= TOL32), err
+
+
+@pytest.mark.parametrize("path", PATHS, ids=PATH_IDS)
+def test_fp32_field_with_fp64_sweeps(path):
+    """BFVM_FP32_FP64MATH: only the stored field is rounded to FP32 (once per
+    sweep and source update), so after 20 steps the error stays within a few
+    hundred FP32 units in the last place (<= 1e-6 relative)."""
+    scn = W.lod_cube(48, 4, 2000, steps=20, seed=5, bulk_radius=150.0, name="lod_48")
+    ref = O.oracle_run(scn, 20, 7)
+    got = run_gpu(scn, 20, 7, precision=FP32_FP64MATH, path=path)
+    err = rel_err(got, ref)
+    assert np.all(err <= 1e-6), err
 
 
 @pytest.mark.parametrize("shape,S", [((7, 5, 3), 1), ((13, 11, 9), 3), ((40, 33, 21), 2)])

@@ -35,6 +35,9 @@ class General_Mesh {
   bool use_voxel_faces;
   std::string units;
   void display_information(std::ostream& os);
+  // [4][voxels] MATLAB matrix "mesh": centre x, y, z and volume per voxel
+  // (BioFVM_mesh.cpp:350-367)
+  void write_to_matlab(std::string filename);
 };
 
 class Cartesian_Mesh : public General_Mesh {

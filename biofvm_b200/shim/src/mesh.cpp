@@ -5,6 +5,7 @@
 #include <cmath>
 
 #include "BioFVM_mesh.h"
+#include "BioFVM_matlab.h"
 
 namespace BioFVM {
 
@@ -28,6 +29,16 @@ bool General_Mesh::is_position_valid(double x, double y, double z) {
   // BioFVM_mesh.cpp:208-217
   return !(x < bounding_box[0] || x > bounding_box[3] || y < bounding_box[1] ||
            y > bounding_box[4] || z < bounding_box[2] || z > bounding_box[5]);
+}
+
+void General_Mesh::write_to_matlab(std::string filename) {
+  FILE* fp = write_matlab_header(4, (int)voxels.size(), filename, "mesh");
+  if (!fp) return;
+  for (const Voxel& v : voxels) {
+    const double col[4] = {v.center[0], v.center[1], v.center[2], v.volume};
+    std::fwrite(col, sizeof(double), 4, fp);
+  }
+  std::fclose(fp);
 }
 
 void General_Mesh::display_information(std::ostream& os) {

@@ -130,3 +130,35 @@ def test_api_driver_matches_the_reference_build():
             assert err <= 1e-12 * pmax[s], (field, s, err)
             gerr = max(abs(a[grads][k] - b[grads][k]) for k in a[grads] if k[1] == s)
             assert gerr <= 2e-12 * pmax[s] / dx, (grads, s, gerr)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("data_matlab,mesh_matlab", [(1, 0), (0, 1), (0, 0)],
+                         ids=["data-mat", "mesh-mat", "all-xml"])
+def test_multicellds_files_match_the_reference_build(tmp_path, data_matlab, mesh_matlab):
+    """tests/dropin/multicellds_driver.cpp saves a microenvironment twice (the
+    second save updates the document of the first) and reads the first file
+    back.  The XML files must be the same text as the reference build's, the
+    MATLAB files the same numbers, and what is read back the same."""
+    gpu = os.path.join(ROOT, "biofvm_b200", "shim", "_build", "dropin", "drivers",
+                       "multicellds_driver")
+    ref = os.path.join(ROOT, "oracle", "_ref", "drivers", "multicellds_driver")
+    if not (os.path.exists(gpu) and os.path.exists(ref)):
+        pytest.skip("driver binaries not built (they need the reference sources)")
+    outs = {}
+    for tag, exe in (("ref", ref), ("gpu", gpu)):
+        d = tmp_path / tag
+        d.mkdir()
+        r = subprocess.run([exe, str(data_matlab), str(mesh_matlab)], cwd=d, capture_output=True,
+                           text=True, timeout=300)
+        assert r.returncode == 0, (tag, r.stdout[-2000:], r.stderr[-2000:])
+        files = {os.path.basename(p): p for p in glob.glob(str(d / "*"))}
+        outs[tag] = (files, [l for l in r.stdout.splitlines() if l.startswith("R ")])
+    (fa, la), (fb, lb) = outs["ref"], outs["gpu"]
+    assert set(fa) == set(fb)
+    for name, pa in fa.items():
+        if name.endswith(".xml"):
+            assert open(pa).read() == open(fb[name]).read(), name
+        elif name.endswith(".mat"):
+            assert np.array_equal(read_mat4(pa), read_mat4(fb[name])), name
+    assert la == lb

@@ -109,7 +109,7 @@ std::string escape(const std::string& s, bool attribute) {
     switch (c) {
       case '&': o += "&amp;"; break;
       case '<': o += "&lt;"; break;
-      case '>': o += attribute ? "&gt;" : "&gt;"; break;
+      case '>': o += "&gt;"; break;
       case '"':
         if (attribute)
           o += "&quot;";
@@ -297,8 +297,6 @@ void build_document(const std::string& filename_base, Microenvironment& M) {
   }
   if (M.mesh.Cartesian_mesh) {
     mesh.add("x_coordinates").attr("delimiter", ",").text = csv_of(M.mesh.x_coordinates, "%f");
-    // the reference writes the text before the attribute; the order in the
-    // file is attribute first either way
     mesh.add("y_coordinates").attr("delimiter", ",").text = csv_of(M.mesh.y_coordinates, "%f");
     mesh.add("z_coordinates").attr("delimiter", ",").text = csv_of(M.mesh.z_coordinates, "%f");
   }

@@ -432,11 +432,21 @@ def run_batched(args, world, rank, local):
         bt.synchronize()
         t_batch = max_over_ranks(time.perf_counter() - t0, world)
     groups, kernels = bt.plan()
+    mode = bt.get_mode()
     err = 0.0
     for sv, ref in zip(sols, plain):
         p = sv.get_densities()
         den = np.maximum(np.abs(ref).max(axis=0), 1e-300)
         err = max(err, float((np.abs(p - ref).max(axis=0) / den).max()))
+    # for reference: the members keep the sweep kernels the batch tuner chose
+    # for each of them; the same instances solved one by one with those
+    reset()
+    barrier(world)
+    t0 = time.perf_counter()
+    for sv in sols:
+        sv.step(dt, args.steps, STEP_ALL)
+        sv.synchronize()
+    t_plain_tuned = max_over_ranks(time.perf_counter() - t0, world)
     bt.close()
     for sv in sols:
         sv.close()
@@ -452,10 +462,12 @@ def run_batched(args, world, rank, local):
                        "field_bytes": vs_per_step * 8},
             "looped_plain": {"value": vs_per_step * args.steps * world / t_plain,
                              "seconds": t_plain},
+            "looped_with_tuned_members": {"value": vs_per_step * args.steps * world /
+                                          t_plain_tuned, "seconds": t_plain_tuned},
             "batched_seconds": t_batch, "speedup_vs_looped_plain": t_plain / t_batch,
             "max_rel_err_vs_looped_plain": err,
-            "tuned": {"chunk": cfg[0], "threads": cfg[1], "group_bytes": cfg[2],
-                      "tune_seconds": t_tune},
+            "tuned": {"mode": ["fused", "branches"][mode], "chunk": cfg[0], "threads": cfg[1],
+                      "group_bytes": cfg[2], "tune_seconds": t_tune},
             "graph": {"groups": groups, "kernels_per_call": kernels,
                       "first_call_seconds": t_first},
             "gpu_launches": kernels,

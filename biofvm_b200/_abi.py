@@ -35,6 +35,9 @@ FP64 = 64
 FP32 = 32
 FP32_FP64MATH = 3264
 
+BATCH_FUSED = 0
+BATCH_BRANCHES = 1
+
 _P = c_void_p  # opaque solver handle
 _DP = POINTER(c_double)
 _LP = POINTER(c_int64)
@@ -81,9 +84,12 @@ SIGNATURES = {
     "bfvm_get_sweep_config": (c_int, [_P, c_int, _IP]),
     "bfvm_set_kernel_path": (c_int, [_P, c_int]),
     "bfvm_set_fuse_sources": (c_int, [_P, c_int]),
+    "bfvm_get_fuse_sources": (c_int, [_P, _IP]),
     "bfvm_synchronize": (c_int, [_P]),
     "bfvm_get_stream": (c_int, [_P, POINTER(c_void_p)]),
     "bfvm_get_launch_count": (c_int, [_P, _LP]),
+    "bfvm_set_slab_planes": (c_int, [_P, c_int]),
+    "bfvm_get_slab_planes": (c_int, [_P, _IP]),
     "bfvm_profile_step": (c_int, [_P, c_double, c_int, c_int, _DP]),
     "bfvm_tune_sweeps": (c_int, [_P, c_double, c_int]),
     "bfvm_get_sweep_kernel": (c_int, [_P, c_int, _IP]),
@@ -102,6 +108,8 @@ SIGNATURES = {
     "bfvm_batch_tune": (c_int, [_P, c_double, c_int, c_int]),
     "bfvm_batch_set_config": (c_int, [_P, _IP, _IP, c_int64]),
     "bfvm_batch_get_config": (c_int, [_P, _IP, _IP, _LP]),
+    "bfvm_batch_set_mode": (c_int, [_P, c_int]),
+    "bfvm_batch_get_mode": (c_int, [_P, _IP]),
     "bfvm_batch_get_plan": (c_int, [_P, _IP, _LP]),
     "bfvm_batch_synchronize": (c_int, [_P]),
 }

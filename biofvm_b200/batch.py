@@ -3,7 +3,9 @@
 
 ``Batch.step(dt, n, flags)`` has the effect of ``Solver.step(dt, n, flags)``
 on every member; the members are packed into L2-sized groups and the whole
-run is one CUDA-graph replay.  The reference has no such object: its drivers
+run is one CUDA-graph replay, either one launch per phase over a group
+(``BATCH_FUSED``) or every member's own kernels on concurrent graph branches
+(``BATCH_BRANCHES``).  The reference has no such object: its drivers
 loop over Microenvironment instances one by one.
 """
 from __future__ import annotations
@@ -70,6 +72,17 @@ class Batch:
         gb = ctypes.c_int64()
         call("bfvm_batch_get_config", self._h, ch, th, ctypes.byref(gb))
         return tuple(ch), tuple(th), gb.value
+
+    def set_mode(self, mode: int) -> None:
+        """BATCH_FUSED (one launch per phase over a group's members) or
+        BATCH_BRANCHES (every member's own kernels on concurrent graph
+        branches)."""
+        call("bfvm_batch_set_mode", self._h, mode)
+
+    def get_mode(self) -> int:
+        m = ctypes.c_int()
+        call("bfvm_batch_get_mode", self._h, ctypes.byref(m))
+        return m.value
 
     def plan(self):
         """(groups of the last plan, kernel launches per step() call)."""

@@ -11,12 +11,21 @@
 // groups whose density fields together stay within a byte budget (by
 // default a fraction of the L2 cache), and all n steps of one group run
 // before the next group starts: a group small enough for L2 keeps its fields
-// on chip across the three sweeps of a step and from step to step.  Within a
-// group every phase of a step is one launch over all of the group's
-// instances (the kernels of bfvm_batch_kernels.cuh).  The whole sequence --
-// groups x steps x phases -- is captured once into a CUDA graph and replayed
-// by one graph launch per call; the graph is rebuilt only when the plan
-// changes (instances, their lists or device buffers, dt, n, flags, tuning).
+// on chip across the three sweeps of a step and from step to step.  Two
+// ways to run a group (bfvm_batch_set_mode):
+//   BFVM_BATCH_FUSED     every phase of a step is one launch over all of the
+//                        group's instances (the kernels of
+//                        bfvm_batch_kernels.cuh);
+//   BFVM_BATCH_BRANCHES  every instance runs its own single-instance step
+//                        kernels (its own sweep kernel choices) on a branch
+//                        of its own: the branches of a group are independent
+//                        graph paths that the GPU runs concurrently, so the
+//                        short kernels of small instances overlap instead of
+//                        running one after another.
+// The whole sequence -- groups x steps x phases -- is captured once into a
+// CUDA graph and replayed by one graph launch per call; the graph is rebuilt
+// only when the plan changes (instances, their lists or device buffers, dt,
+// n, flags, mode, tuning).
 //
 // The tuner (bfvm_batch_tune) picks, per axis, the chunk length (points per
 // thread) and threads per block, then the group budget, by timing short
@@ -40,10 +49,12 @@ struct BatchConfig {
   int ch[3] = {0, 0, 0};       // 0 = choose from the longest line
   int threads[3] = {0, 0, 0};  // 0 = choose
   int64_t group_bytes = -1;    // -1 = default (half of L2), 0 = one group
+  int mode = BFVM_BATCH_FUSED;
 };
 
 // Device descriptors of one group, all in one buffer.
 struct GroupPlan {
+  int first_inst = 0, n_inst = 0;  // members b->inst[first_inst ..]
   int64_t field_bytes = 0;
   size_t off_sweep[3] = {0, 0, 0}, off_bulk = 0, off_cells = 0, off_dir = 0;
   int n_sweep[3] = {0, 0, 0}, n_bulk = 0, n_cells = 0, n_dir = 0;
@@ -177,9 +188,13 @@ void build_plan(bfvm_batch* b) {
   std::vector<unsigned char>& buf = b->host_desc;
   buf.clear();
   b->groups.clear();
+  int next_inst = 0;
   for (auto& members : groups) {
     GroupPlan G;
     std::memset(&G, 0, sizeof G);
+    G.first_inst = next_inst;
+    G.n_inst = (int)members.size();
+    next_inst += G.n_inst;
     for (bfvm_solver* m : members) G.field_bytes += (int64_t)(m->NS() * m->elem());
     for (int a = 0; a < 3; ++a) {
       align_to(buf, 64);
@@ -331,20 +346,76 @@ void drop_graph(bfvm_batch* b) {
   b->key.clear();
 }
 
+// Branch mode: one step of one instance with its own kernels, on its own
+// stream (bfvm_step's statements).  `axes` limits the sweeps as above.
+void enqueue_instance_step(bfvm_solver* m, double dt, int flags, int axes) {
+  if (!(flags & BFVM_STEP_DIFFUSION)) {
+    if (flags & BFVM_STEP_BULK) bulk_any(m, dt);
+    if (flags & BFVM_STEP_CELLS) cells_any(m);
+    return;
+  }
+  if (axes == 7) {
+    step_once(m, dt, flags, nullptr);
+    return;
+  }
+  const int fuses[3] = {kFuseDirPro | kFuseDirEpi, kFuseDirEpi, 0};
+  for (int a = 0; a < 3; ++a)
+    if (axes & (1 << a)) sweep(m, a, fuses[a], dt);
+}
+
+// Branch mode: runs one step of every instance outside any capture, on its
+// field saved before and restored after, so that everything a step prepares
+// on first use (coefficient and chunk tables, kernel attributes) exists
+// before the capture, which must not upload or synchronise.
+void warm_instances(bfvm_batch* b, double dt, int flags) {
+  for (bfvm_solver* m : b->inst) {
+    const size_t bytes = m->NS() * m->elem();
+    if (bytes == 0) continue;
+    DevBuf save;
+    save.ensure(bytes);
+    BFVM_CUDA(cudaMemcpyAsync(save.ptr, m->p.ptr, bytes, cudaMemcpyDeviceToDevice, m->stream));
+    enqueue_instance_step(m, dt, flags, 7);
+    BFVM_CUDA(cudaMemcpyAsync(m->p.ptr, save.ptr, bytes, cudaMemcpyDeviceToDevice, m->stream));
+    BFVM_CUDA(cudaStreamSynchronize(m->stream));
+    check_status(m);
+  }
+}
+
 // Captures groups x nsteps x phases into one graph executable.
 cudaGraphExec_t capture(bfvm_batch* b, double dt, int nsteps, int flags, int axes,
                         int64_t* kernels) {
   *kernels = 0;
   cudaGraph_t graph = nullptr;
+  const bool branches = b->cfg.mode == BFVM_BATCH_BRANCHES;
+  if (branches) warm_instances(b, dt, flags);
   BFVM_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
   try {
-    for (const GroupPlan& G : b->groups)
+    for (const GroupPlan& G : b->groups) {
+      if (branches) {
+        // fork: every member's own stream joins the capture after the work
+        // captured so far; join: the batch stream waits for every member
+        BFVM_CUDA(cudaEventRecord(b->ev, b->stream));
+        for (int i = G.first_inst; i < G.first_inst + G.n_inst; ++i)
+          BFVM_CUDA(cudaStreamWaitEvent(b->inst[i]->stream, b->ev, 0));
+        for (int i = G.first_inst; i < G.first_inst + G.n_inst; ++i) {
+          bfvm_solver* m = b->inst[i];
+          const int64_t before = m->launches;
+          for (int it = 0; it < nsteps; ++it) enqueue_instance_step(m, dt, flags, axes);
+          *kernels += m->launches - before;
+        }
+        for (int i = G.first_inst; i < G.first_inst + G.n_inst; ++i) {
+          BFVM_CUDA(cudaEventRecord(b->ev, b->inst[i]->stream));
+          BFVM_CUDA(cudaStreamWaitEvent(b->stream, b->ev, 0));
+        }
+        continue;
+      }
       for (int it = 0; it < nsteps; ++it) {
         if (fp64(b))
           enqueue_group_step<double>(b, G, dt, flags, axes, kernels);
         else
           enqueue_group_step<float>(b, G, dt, flags, axes, kernels);
       }
+    }
   } catch (...) {
     cudaStreamEndCapture(b->stream, &graph);
     if (graph) cudaGraphDestroy(graph);
@@ -365,6 +436,46 @@ std::string plan_key(const bfvm_batch* b, double dt, int nsteps, int flags) {
   k.append(reinterpret_cast<const char*>(&flags), sizeof flags);
   k.append(reinterpret_cast<const char*>(b->ch), sizeof b->ch);
   k.append(reinterpret_cast<const char*>(b->threads), sizeof b->threads);
+  k.append(reinterpret_cast<const char*>(&b->cfg.mode), sizeof b->cfg.mode);
+  // branch mode bakes each member's own kernel choices and device buffers
+  // into the graph
+  if (b->cfg.mode == BFVM_BATCH_BRANCHES)
+    for (const bfvm_solver* m : b->inst) {
+      for (int a = 0; a < 3; ++a) {
+        const Axis& A = m->axis[a];
+        const int v[5] = {A.ch, A.tw, A.minb, A.kind, m->chunk_nslots[a]};
+        k.append(reinterpret_cast<const char*>(v), sizeof v);
+      }
+      const int64_t v[8] = {m->path, m->fuse_sources, m->precision, m->n_agents,
+                            (int64_t)m->bulk_vox.size(), m->dir_unique, m->NS(), m->S};
+      k.append(reinterpret_cast<const char*>(v), sizeof v);
+      auto buf = [&](const DevBuf& d) {
+        k.append(reinterpret_cast<const char*>(&d.ptr), sizeof d.ptr);
+        k.append(reinterpret_cast<const char*>(&d.bytes), sizeof d.bytes);
+      };
+      auto seg = [&](const DevSegList& L) {
+        buf(L.off);
+        buf(L.pos);
+        buf(L.a);
+        buf(L.b);
+        k.push_back(L.present ? 1 : 0);
+      };
+      buf(m->p);
+      for (int a = 0; a < 3; ++a) {
+        buf(m->coef[a]);
+        buf(m->chunk[a]);
+        buf(m->chunk_slots[a]);
+      }
+      for (const DevBuf* d : {&m->d_bulk_vox, &m->d_bulk_st, &m->d_bulk_su, &m->d_dir_vox,
+                              &m->d_dir_val, &m->d_ag_vox_orig, &m->d_ag_t1, &m->d_ag_t2,
+                              &m->d_ag_key, &m->d_ag_idx_in, &m->d_ag_idx, &m->d_sort_tmp,
+                              &m->d_gather, &m->d_status})
+        buf(*d);
+      seg(m->seg_bulk);
+      seg(m->seg_dir_x);
+      seg(m->seg_dir_y);
+      seg(m->seg_cells);
+    }
   for (const GroupPlan& G : b->groups) k.append(reinterpret_cast<const char*>(&G), sizeof G);
   return k;
 }
@@ -460,21 +571,32 @@ void batch_tune(bfvm_batch* b, double dt, int flags, int trial_steps) {
           }
         }
     }
-    // 2. the group budget, whole steps
+    // 2. every member's own sweep kernels and slabs (what branch mode runs;
+    // each member's field is saved and restored by its tuner)
+    for (bfvm_solver* m : b->inst) {
+      BFVM_CUDA(cudaStreamSynchronize(b->stream));
+      tune_sweeps(m, dt, 3);
+    }
+    // 3. the mode and the group budget, whole steps
     float best_ms = 1e30f;
     int64_t best_budget = 0;
-    for (int64_t budget : {(int64_t)0, (int64_t)b->l2_bytes, (int64_t)b->l2_bytes / 2,
-                           (int64_t)b->l2_bytes / 4, (int64_t)b->l2_bytes / 8}) {
-      b->cfg = best;
-      b->cfg.group_bytes = budget;
-      plan(b);
-      const float ms = time_graph(b, dt, trial_steps, flags, 7);
-      if (ms < best_ms) {
-        best_ms = ms;
-        best_budget = budget;
+    int best_mode = BFVM_BATCH_FUSED;
+    for (int mode : {BFVM_BATCH_FUSED, BFVM_BATCH_BRANCHES})
+      for (int64_t budget : {(int64_t)0, (int64_t)b->l2_bytes, (int64_t)b->l2_bytes / 2,
+                             (int64_t)b->l2_bytes / 4, (int64_t)b->l2_bytes / 8}) {
+        b->cfg = best;
+        b->cfg.group_bytes = budget;
+        b->cfg.mode = mode;
+        plan(b);
+        const float ms = time_graph(b, dt, trial_steps, flags, 7);
+        if (ms < best_ms) {
+          best_ms = ms;
+          best_budget = budget;
+          best_mode = mode;
+        }
       }
-    }
     best.group_bytes = best_budget;
+    best.mode = best_mode;
     b->cfg = best;
   } catch (...) {
     b->cfg = user;
@@ -586,6 +708,7 @@ int bfvm_batch_set_config(bfvm_batch* b, const int* chunk, const int* threads,
       require((c.ch[a] == 0) == (c.threads[a] == 0), "chunk and threads are set together");
     }
     c.group_bytes = group_bytes;
+    c.mode = b->cfg.mode;
     b->cfg = c;
   });
 }
@@ -599,6 +722,21 @@ int bfvm_batch_get_config(bfvm_batch* b, int* chunk, int* threads, int64_t* grou
     }
     if (group_bytes)
       *group_bytes = b->cfg.group_bytes < 0 ? (int64_t)b->l2_bytes / 2 : b->cfg.group_bytes;
+  });
+}
+
+int bfvm_batch_set_mode(bfvm_batch* b, int mode) {
+  return BATCH_CALL(b, {
+    require(mode == BFVM_BATCH_FUSED || mode == BFVM_BATCH_BRANCHES,
+            "mode must be BFVM_BATCH_FUSED or BFVM_BATCH_BRANCHES");
+    b->cfg.mode = mode;
+  });
+}
+
+int bfvm_batch_get_mode(bfvm_batch* b, int* mode) {
+  return BATCH_CALL(b, {
+    require(mode != nullptr, "null output pointer");
+    *mode = b->cfg.mode;
   });
 }
 

@@ -4,6 +4,7 @@
 #include "bfvm_host_math.h"
 
 #include <cmath>
+#include <vector>
 
 namespace bfvm {
 
@@ -109,6 +110,107 @@ void chunk_tables(int n, int S, int ch, const double* c1, const double* denom, c
     }
   }
   (void)c1;
+}
+
+
+namespace {
+
+// The float nearest v first, then the float on v's other side (if v is not
+// a float itself).
+int float_candidates(double v, float out[2]) {
+  const float r = (float)v;
+  out[0] = r;
+  if ((double)r == v) return 1;
+  out[1] = std::nextafter(r, (double)r < v ? INFINITY : -INFINITY);
+  return 2;
+}
+
+}  // namespace
+
+void fp32_tables(int n, int S, const double* c1, const double* denom, const double* cx,
+                 float* inv, float* fwd, float* bwd, float* c1f, double* tile_den,
+                 double* tile_cx) {
+  constexpr int kPeriod = 8, kBlock = 32;
+  std::vector<double> qe(n), xe(n);
+  std::vector<float> tinv(n);
+  std::vector<char> per((size_t)(n + kBlock - 1) / kBlock, 0);
+  // nearest float first, then the one on the other side of v
+  auto pick = [](double v, auto err) {
+    float cand[2];
+    const int nc = float_candidates(v, cand);
+    float best = cand[0];
+    double best_e = err(cand[0]);
+    for (int j = 1; j < nc; ++j) {
+      const double e = err(cand[j]);
+      if (std::fabs(e) < std::fabs(best_e)) {
+        best = cand[j];
+        best_e = e;
+      }
+    }
+    return best;
+  };
+  for (int s = 0; s < S; ++s) {
+    auto at = [&](const double* a, int k) { return a[(size_t)k * S + s]; };
+    c1f[s] = (float)c1[s];
+    const double c1r = (double)c1f[s];
+    // exact solve of a unit right-hand side (the reference's elimination)
+    double q = 0.0;
+    for (int k = 0; k < n; ++k) {
+      q = (1.0 + c1[s] * q) / at(denom, k);
+      qe[k] = q;
+    }
+    double x = 0.0;
+    for (int k = n - 1; k >= 0; --k) {
+      x = qe[k] - at(cx, k) * x;
+      xe[k] = x;
+    }
+    // Whole 32-point blocks whose exact coefficients repeat with period 8
+    // (the converged interior of a long line): there the roundings repeat
+    // too, so that every chunk of 8, 16 or 32 points inside keeps identical
+    // tables (the tile kernels share the tables of identical chunks).  The
+    // greedy choices of the 8 points where such a region is entered (its
+    // last 8 points backward, its first 8 forward) are the repeated period.
+    for (size_t j = 0; j < per.size(); ++j) {
+      bool ok = j > 0 && (int)((j + 1) * kBlock) <= n;
+      for (int k = (int)j * kBlock; ok && k < (int)(j + 1) * kBlock; ++k)
+        ok = at(denom, k) == at(denom, k - kPeriod) && at(cx, k) == at(cx, k - kPeriod);
+      per[j] = ok;
+    }
+    auto periodic = [&](int k) { return k >= 0 && k < n && per[k / kBlock]; };
+    // backward coefficients (shared by both forms): x_k = q_k + b_k x_{k+1}
+    double xc = 0.0;
+    for (int k = n - 1; k >= 0; --k) {
+      const size_t i = (size_t)k * S + s;
+      float b;
+      if (periodic(k) && periodic(k + kPeriod))
+        b = bwd[i + (size_t)kPeriod * S];
+      else
+        b = pick(-cx[i], [&](float c) { return qe[k] + (double)c * xc - xe[k]; });
+      bwd[i] = b;
+      tile_cx[i] = -(double)b;
+      xc = qe[k] + (double)b * xc;
+    }
+    // forward: register form q_k = (1 + c1 q_{k-1}) inv_k, every point chosen
+    // (its tables are not shared between chunks); tile form
+    // q_k = a_k q_{k-1} + inv'_k with a_k = b_k
+    double qr = 0.0, qt = 0.0;
+    for (int k = 0; k < n; ++k) {
+      const size_t i = (size_t)k * S + s;
+      const double v = 1.0 / denom[i];
+      const float r = pick(v, [&](float c) { return (1.0 + c1r * qr) * (double)c - qe[k]; });
+      inv[i] = r;
+      fwd[i] = (float)(c1r * (double)r);
+      qr = (1.0 + c1r * qr) * (double)r;
+      float t;
+      if (periodic(k) && periodic(k - kPeriod))
+        t = tinv[k - kPeriod];
+      else
+        t = pick(v, [&](float c) { return (double)bwd[i] * qt + (double)c - qe[k]; });
+      tinv[k] = t;
+      tile_den[i] = 1.0 / (double)t;
+      qt = (double)bwd[i] * qt + (double)t;
+    }
+  }
 }
 
 }  // namespace bfvm

@@ -37,4 +37,27 @@ namespace bfvm {
 void chunk_tables(int n, int S, int ch, const double* c1, const double* denom, const double* cx,
                   double* k1, double* kg, double* kc);
 
+// FP32 Thomas tables of one axis whose roundings keep a constant field's
+// decay rate.  Rounded to nearest one by one, every interior point of a line
+// gets the same rounded coefficients, so every sweep scales the field by the
+// same slightly wrong factor and the bias grows linearly with the step count
+// (up to ~2e-5 relative after 150 sweeps of a 512-point line at
+// c1 = dt D / dx^2 = 10).  Here each coefficient is rounded down or up
+// (one of the two floats around it), greedily along the line, so that the
+// solve of a unit right-hand side carried out with the FP32 coefficients
+// stays closest to the exact one (error diffusion).  Where the exact
+// coefficients repeat with period 8 (the converged interior of a line, in
+// whole 32-point blocks) the choices of the first 8 points there repeat, so
+// chunks of 8, 16 or 32 points inside keep identical tables.
+//   register form (lod_sweep_kernel): q_k = (p_k + c1 q_{k-1}) inv_k,
+//     x_k = q_k + bwd_k x_{k+1}; fwd_k = c1 inv_k (the carry products);
+//     out: inv, fwd, bwd [n][S], c1f [S];
+//   tile form (line and row kernels): q_k = a_k q_{k-1} + p_k inv'_k,
+//     x_k = a_k x_{k+1} + q_k with a_k = bwd_k; out as FP64 arrays
+//     den' = 1 / inv'_k and cx' = -a_k [n][S], from which chunk_tables
+//     builds tables that round back to exactly these floats.
+void fp32_tables(int n, int S, const double* c1, const double* denom, const double* cx,
+                 float* inv, float* fwd, float* bwd, float* c1f, double* tile_den,
+                 double* tile_cx);
+
 }  // namespace bfvm

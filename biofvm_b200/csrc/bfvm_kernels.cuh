@@ -67,7 +67,8 @@ struct SegList {
 template <typename T, typename CT = T>
 struct SweepArgs {
   T* p;
-  int64_t ncols;         // number of (line, substrate) columns
+  int64_t col0;          // first column of this launch (a slab of planes)
+  int64_t ncols;         // end of the launch's columns (all (line, substrate) columns)
   int64_t C;             // columns per outer block
   int64_t outer_stride;  // elements between outer blocks
   int64_t line_stride;   // elements between consecutive points of a line
@@ -141,7 +142,7 @@ __global__ void __launch_bounds__(sweep_max_threads(CH), MINB)
 
   const int tx = threadIdx.x;
   const int c = threadIdx.y;
-  const int64_t vcol = (int64_t)blockIdx.x * TW + tx;
+  const int64_t vcol = a.col0 + (int64_t)blockIdx.x * TW + tx;
   const bool active = vcol < a.ncols;
   const int S = a.S;
   const int k0 = c * CH;

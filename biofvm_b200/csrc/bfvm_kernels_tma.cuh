@@ -122,6 +122,7 @@ struct LinesArgs {
   int64_t os;      // element stride between outer blocks
   int S;
   uint32_t ctiles;  // ceil(C / W)
+  uint32_t tile0;   // tiles tile0 .. ntiles-1 (a slab of outer blocks)
   uint32_t ntiles;  // outer blocks * ctiles
   int box_n;        // rows per TMA box (<= 256)
   int nboxes;       // boxes per tile
@@ -139,6 +140,7 @@ struct RowsArgs {
   int S;
   int R;          // rows per tile
   int64_t pitch;  // shared-memory elements between the rows of a tile
+  int64_t tile0;  // tiles tile0 .. ntiles-1 (a slab of rows)
   int64_t ntiles;
   int nchunks;
   ChunkCoef<CT> cc;
@@ -273,7 +275,7 @@ __global__ void __launch_bounds__(W * MAXNC)
   int issued = 0;  // tiles issued by this block (meaningful in thread 0)
   if (tid == 0) {
     for (int s = 0; s < STAGES; ++s) {
-      const uint32_t t = blockIdx.x + (uint32_t)s * gridDim.x;
+      const uint32_t t = a.tile0 + blockIdx.x + (uint32_t)s * gridDim.x;
       if (t < a.ntiles) {
         issue(s, t);
         ++issued;
@@ -285,7 +287,7 @@ __global__ void __launch_bounds__(W * MAXNC)
   const int k0 = c * CH;
   const int len = max(0, min(CH, a.n - k0));
   int i = 0;
-  for (uint32_t tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x, ++i) {
+  for (uint32_t tile = a.tile0 + blockIdx.x; tile < a.ntiles; tile += gridDim.x, ++i) {
     const int st = i % STAGES;
     const bool ok = tma::mbar_wait(&full[st], (uint32_t)((i / STAGES) & 1));
     const uint32_t outer = tile / a.ctiles;
@@ -391,7 +393,7 @@ __global__ void __launch_bounds__(MAXT) lod_rows_tma_kernel(const RowsArgs<T, CT
   int issued = 0;
   if (tid == 0) {
     for (int st = 0; st < STAGES; ++st) {
-      const int64_t t = blockIdx.x + (int64_t)st * gridDim.x;
+      const int64_t t = a.tile0 + blockIdx.x + (int64_t)st * gridDim.x;
       if (t < a.ntiles) {
         issue(st, t);
         ++issued;
@@ -400,7 +402,7 @@ __global__ void __launch_bounds__(MAXT) lod_rows_tma_kernel(const RowsArgs<T, CT
   }
 
   int i = 0;
-  for (int64_t tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x, ++i) {
+  for (int64_t tile = a.tile0 + blockIdx.x; tile < a.ntiles; tile += gridDim.x, ++i) {
     const int st = i % STAGES;
     const bool ok = tma::mbar_wait(&full[st], (uint32_t)((i / STAGES) & 1));
     const int nr = tile_rows(tile);
@@ -490,7 +492,8 @@ __global__ void __launch_bounds__(MAXT) lod_rows_tma_kernel(const RowsArgs<T, CT
 template <typename T, typename CT = T>
 struct DirectArgs {
   T* p;
-  int64_t ncols;         // (line, density) columns
+  int64_t col0;          // first column of this launch (a slab of planes)
+  int64_t ncols;         // end of the launch's (line, density) columns
   int64_t C;             // columns per outer block
   int64_t outer_stride;  // elements
   int64_t line_stride;   // elements between points of a line
@@ -520,7 +523,7 @@ __global__ void __launch_bounds__(512) lod_sweep_direct_kernel(const DirectArgs<
   }
   const int S = a.S;
   const int k0 = c * CH;
-  const int64_t vcol = (int64_t)blockIdx.x * W + tx;
+  const int64_t vcol = a.col0 + (int64_t)blockIdx.x * W + tx;
   const bool active = vcol < a.ncols;
   const int lenA = active ? max(0, min(CH, a.n - k0)) : 0;
   int s = 0;

@@ -108,8 +108,16 @@ void thomas_setup(bfvm_solver* m, double dt) {
     if (m->math_elem() == sizeof(double)) {
       upload(m->coef[a], tab, m->stream);
     } else {
-      std::vector<float> tf(tab.begin(), tab.end());
+      // FP32 arithmetic: roundings chosen along each line (error diffusion);
+      // the chunk tables of the tile kernels follow the floats chosen for them
+      const size_t nS = (size_t)n * S;
+      std::vector<float> tf(3 * nS + S);
+      std::vector<double> tden(nS), tcx(nS);
+      bfvm::fp32_tables(n, S, c1.data(), den.data(), cx.data(), tf.data(), tf.data() + nS,
+                        tf.data() + 2 * nS, tf.data() + 3 * nS, tden.data(), tcx.data());
       upload(m->coef[a], tf, m->stream);
+      den.swap(tden);
+      cx.swap(tcx);
     }
     m->h_c1[a] = c1;
     m->h_den[a] = den;
@@ -426,8 +434,11 @@ void launch_sweep_ch(const bfvm::SweepArgs<T, CT>& a, int mode, int minb, dim3 g
     launch_sweep_mb<T, CT, CH, 1>(a, mode, grid, block, smem, st);
 }
 
+// Sweeps take a range of z planes [z0, z1) for the x and y axes (z1 < 0:
+// every plane): the x and y lines of a slab of planes are independent of the
+// other planes' (see step_once).
 template <typename T, typename CT>
-void launch_sweep(bfvm_solver* m, int ax, int fuse, double dt) {
+void launch_sweep(bfvm_solver* m, int ax, int fuse, double dt, int64_t z0 = 0, int64_t z1 = -1) {
   const int S = m->S;
   const int64_t nx = m->nx, ny = m->ny, nz = m->nz;
   bfvm::SweepArgs<T, CT> a{};
@@ -466,8 +477,13 @@ void launch_sweep(bfvm_solver* m, int ax, int fuse, double dt) {
   a.cells = m->seg_cells.view();
   a.dir_pro = dseg.view();
   a.dir_epi = dseg.view();
+  if (z1 >= 0 && ax < 2) {  // columns of planes z0 .. z1-1
+    const int64_t per_plane = (ax == 0 ? ny : nx) * S;
+    a.col0 = z0 * per_plane;
+    a.ncols = z1 * per_plane;
+  }
   dim3 block(A.tw, a.nchunks);
-  dim3 grid((unsigned)blocks_for(a.ncols, A.tw));
+  dim3 grid((unsigned)blocks_for(a.ncols - a.col0, A.tw));
   const size_t smem = 4 * sizeof(CT) * (size_t)A.tw * a.nchunks;
   int mode = bfvm::kSweepPlain;
   if (fuse & (bfvm::kFuseBulk | bfvm::kFuseCells | bfvm::kFuseDirPro))
@@ -711,7 +727,8 @@ void launch_lines_st(const CUtensorMap& map, const bfvm::LinesArgs<T, CT>& a, in
 }
 
 template <typename T, typename CT>
-void launch_lines(bfvm_solver* m, int ax, const LinesPlan& L, bool dir) {
+void launch_lines(bfvm_solver* m, int ax, const LinesPlan& L, bool dir, int64_t z0 = 0,
+                  int64_t z1 = -1) {
   // (re)encode the tensor map when the field moved
   if (m->map_key[ax] != m->p.ptr || m->map_w[ax] != L.w) {
     const int64_t es = (int64_t)sizeof(T);
@@ -738,6 +755,11 @@ void launch_lines(bfvm_solver* m, int ax, const LinesPlan& L, bool dir) {
   a.S = m->S;
   a.ctiles = (uint32_t)((L.C + L.w - 1) / L.w);
   a.ntiles = (uint32_t)(a.ctiles * L.nouter);
+  if (z1 >= 0 && ax == 1) {  // the outer blocks of the y lines are the z planes
+    a.tile0 = (uint32_t)(a.ctiles * z0);
+    a.ntiles = (uint32_t)(a.ctiles * z1);
+  }
+  const int run_tiles = (int)(a.ntiles - a.tile0);
   a.box_n = L.box_n;
   a.nboxes = L.nboxes;
   a.nchunks = L.nc;
@@ -746,9 +768,9 @@ void launch_lines(bfvm_solver* m, int ax, const LinesPlan& L, bool dir) {
   if (dir) a.dir_epi = m->seg_dir_y.view();
   dim3 block(L.w, L.nc);
   switch (L.ch) {
-    case 8: launch_lines_st<T, CT, 8>(m->maps[ax], a, L.stages, dir, L.smem_tab, a.ntiles, block, L.smem, m); break;
-    case 16: launch_lines_st<T, CT, 16>(m->maps[ax], a, L.stages, dir, L.smem_tab, a.ntiles, block, L.smem, m); break;
-    default: launch_lines_st<T, CT, 32>(m->maps[ax], a, L.stages, dir, L.smem_tab, a.ntiles, block, L.smem, m); break;
+    case 8: launch_lines_st<T, CT, 8>(m->maps[ax], a, L.stages, dir, L.smem_tab, run_tiles, block, L.smem, m); break;
+    case 16: launch_lines_st<T, CT, 16>(m->maps[ax], a, L.stages, dir, L.smem_tab, run_tiles, block, L.smem, m); break;
+    default: launch_lines_st<T, CT, 32>(m->maps[ax], a, L.stages, dir, L.smem_tab, run_tiles, block, L.smem, m); break;
   }
   check_launch(m);
 }
@@ -776,7 +798,8 @@ void launch_direct_mode(const bfvm::DirectArgs<T, CT>& a, int mode, dim3 grid, d
 
 // Any axis with direct loads: blocks of 32 columns x all chunks of a line.
 template <typename T, typename CT>
-bool launch_direct(bfvm_solver* m, int ax, int fuse, double dt) {
+bool launch_direct(bfvm_solver* m, int ax, int fuse, double dt, int64_t z0 = 0,
+                   int64_t z1 = -1) {
   const int64_t nx = m->nx, ny = m->ny, nz = m->nz, S = m->S;
   bfvm::DirectArgs<T, CT> a{};
   const int64_t nzp = (m->lod_dims == 2) ? 1 : nz;  // planes swept
@@ -789,10 +812,15 @@ bool launch_direct(bfvm_solver* m, int ax, int fuse, double dt) {
     a.n = (int)nz; a.C = nx * ny * S; a.outer_stride = 0; a.line_stride = nx * ny * S;
     a.ncols = nx * ny * S;
   }
+  if (z1 >= 0 && ax < 2) {  // columns of planes z0 .. z1-1
+    const int64_t per_plane = (ax == 0 ? ny : nx) * S;
+    a.col0 = z0 * per_plane;
+    a.ncols = z1 * per_plane;
+  }
   const int ch = m->axis[ax].ch;
   const int nc = (a.n + ch - 1) / ch;
   constexpr int W = 32;
-  const int64_t nblocks = (a.ncols + W - 1) / W;
+  const int64_t nblocks = (a.ncols - a.col0 + W - 1) / W;
   if (W * nc > 512 || nblocks >= ((int64_t)1 << 31)) return false;
   a.p = m->p.as<T>();
   a.S = (int)S;
@@ -831,7 +859,7 @@ void launch_rows_inst(const bfvm::RowsArgs<T, CT>& a, dim3 block, size_t smem, b
   int per_sm = 0;
   BFVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, block.x * block.y, smem));
   require(per_sm > 0, "sweep kernel does not fit on an SM", BFVM_ERR_STATE);
-  dim3 grid((unsigned)std::min<int64_t>(a.ntiles, (int64_t)per_sm * m->num_sms));
+  dim3 grid((unsigned)std::min<int64_t>(a.ntiles - a.tile0, (int64_t)per_sm * m->num_sms));
   k<<<grid, block, smem, m->stream>>>(a);
 }
 
@@ -851,13 +879,23 @@ void launch_rows_ch(const bfvm::RowsArgs<T, CT>& a, const RowsPlan& P, dim3 bloc
 }
 
 template <typename T, typename CT>
-void launch_rows(bfvm_solver* m, const RowsPlan& P, int fuse, double dt) {
+void launch_rows(bfvm_solver* m, const RowsPlan& P, int fuse, double dt, int64_t z0 = 0,
+                 int64_t z1 = -1) {
   bfvm::RowsArgs<T, CT> a{};
   a.p = m->p.as<T>();
   a.rows = (int64_t)m->ny * (m->lod_dims == 2 ? 1 : m->nz);
   a.n = m->nx;
   a.S = m->S;
   a.ntiles = (a.rows + P.R - 1) / P.R;
+  if (z1 >= 0) {
+    // tiles of R rows from the first one starting in plane z0 to the last
+    // one starting before plane z1: a slab's rows that begin in an earlier
+    // tile were swept with the slab before
+    const int64_t r0 = z0 * m->ny, r1 = z1 * m->ny;
+    a.tile0 = (r0 + P.R - 1) / P.R;
+    a.ntiles = std::min(a.ntiles, (r1 + P.R - 1) / P.R);
+    if (a.ntiles <= a.tile0) return;  // every row of the slab was swept before
+  }
   a.nchunks = P.nc;
   a.R = P.R;
   a.pitch = P.pitch;
@@ -893,7 +931,7 @@ void with_types(const bfvm_solver* m, F&& f) {
     f(float(), float());
 }
 
-void sweep(bfvm_solver* m, int ax, int fuse, double dt) {
+void sweep(bfvm_solver* m, int ax, int fuse, double dt, int64_t z0, int64_t z1) {
   // under AUTO an axis may carry its own kernel choice (bfvm_tune_sweeps)
   const int path =
       (m->path == BFVM_PATH_AUTO && m->axis[ax].kind) ? m->axis[ax].kind : m->path;
@@ -906,27 +944,27 @@ void sweep(bfvm_solver* m, int ax, int fuse, double dt) {
       // AUTO: the register kernel for x (measured fastest there), TMA tiles
       // for y and z
       if (path == BFVM_PATH_AUTO && ax == 0) {
-        launch_sweep<T, CT>(m, ax, fuse, dt);
+        launch_sweep<T, CT>(m, ax, fuse, dt, z0, z1);
         return;
       }
       const bool want_tma = (path == BFVM_PATH_TMA) || (path == BFVM_PATH_AUTO);
       if (want_tma && ax == 0) {
         const RowsPlan P = plan_rows(m);
         if (P.ok) {
-          launch_rows<T, CT>(m, P, fuse, dt);
+          launch_rows<T, CT>(m, P, fuse, dt, z0, z1);
           return;
         }
       } else if (want_tma) {
         const LinesPlan L = plan_lines(m, ax);
         if (L.ok) {
           const bool dir = (ax == 1) && (fuse & bfvm::kFuseDirEpi) && m->seg_dir_y.present;
-          launch_lines<T, CT>(m, ax, L, dir);
+          launch_lines<T, CT>(m, ax, L, dir, z0, z1);
           return;
         }
       }
-      if (launch_direct<T, CT>(m, ax, fuse, dt)) return;
+      if (launch_direct<T, CT>(m, ax, fuse, dt, z0, z1)) return;
     }
-    launch_sweep<T, CT>(m, ax, fuse, dt);
+    launch_sweep<T, CT>(m, ax, fuse, dt, z0, z1);
   });
 }
 
@@ -970,9 +1008,24 @@ void step_once(bfvm_solver* m, double dt, int flags, cudaEvent_t* ev) {
     if (flags & BFVM_STEP_CELLS) cells_any(m);
   }
   if (ev) BFVM_CUDA(cudaEventRecord(ev[1], m->stream));
-  sweep(m, 0, fuse | bfvm::kFuseDirPro | bfvm::kFuseDirEpi, dt);
-  if (ev) BFVM_CUDA(cudaEventRecord(ev[2], m->stream));
-  sweep(m, 1, bfvm::kFuseDirEpi, dt);
+  const int k = m->slab_planes;
+  if (k > 0 && k < m->nz && m->lod_dims == 3) {
+    // x then y on slabs of k planes: an x line and a y line lie in one z
+    // plane, so the y sweep of a slab needs only that slab's x sweep, and a
+    // slab small enough for L2 is read back by the y sweep from L2 (the field
+    // crosses HBM once for both sweeps instead of twice)
+    for (int64_t z0 = 0; z0 < m->nz; z0 += k) {
+      const int64_t z1 = std::min<int64_t>(m->nz, z0 + k);
+      sweep(m, 0, fuse | bfvm::kFuseDirPro | bfvm::kFuseDirEpi, dt, z0, z1);
+      sweep(m, 1, bfvm::kFuseDirEpi, dt, z0, z1);
+    }
+    // profiles: the x entry holds both sweeps, the y entry nothing
+    if (ev) BFVM_CUDA(cudaEventRecord(ev[2], m->stream));
+  } else {
+    sweep(m, 0, fuse | bfvm::kFuseDirPro | bfvm::kFuseDirEpi, dt);
+    if (ev) BFVM_CUDA(cudaEventRecord(ev[2], m->stream));
+    sweep(m, 1, bfvm::kFuseDirEpi, dt);
+  }
   if (ev) BFVM_CUDA(cudaEventRecord(ev[3], m->stream));
   sweep(m, 2, 0, dt);
   if (ev) BFVM_CUDA(cudaEventRecord(ev[4], m->stream));
@@ -1697,6 +1750,20 @@ int bfvm_set_precision(bfvm_solver* m, int precision) {
   });
 }
 
+int bfvm_set_slab_planes(bfvm_solver* m, int planes) {
+  return SOLVER_CALL(m, {
+    require(planes >= 0, "planes must be >= 0");
+    m->slab_planes = planes;
+  });
+}
+
+int bfvm_get_slab_planes(bfvm_solver* m, int* planes) {
+  return SOLVER_CALL(m, {
+    require(planes != nullptr, "null output pointer");
+    *planes = m->slab_planes;
+  });
+}
+
 int bfvm_set_sweep_config(bfvm_solver* m, int axis, int chunk, int columns, int min_blocks) {
   return SOLVER_CALL(m, {
     require(axis >= 0 && axis < 3, "axis must be 0, 1 or 2");
@@ -1735,6 +1802,8 @@ void tune_sweeps(bfvm_solver* m, double dt, int reps) {
   save.ensure(std::max<size_t>(bytes, 16));
   BFVM_CUDA(cudaMemcpyAsync(save.ptr, m->p.ptr, bytes, cudaMemcpyDeviceToDevice, m->stream));
   const int saved_path = m->path;
+  const int saved_slab = m->slab_planes;
+  const int saved_fuse = m->fuse_sources;
   m->path = BFVM_PATH_AUTO;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   BFVM_CUDA(cudaEventCreate(&e0));
@@ -1783,7 +1852,54 @@ void tune_sweeps(bfvm_solver* m, double dt, int reps) {
       if (m->axis[ax].ch != best.ch) m->bulk_dirty = m->dir_dirty = m->ag_seg_dirty = true;
       m->axis[ax] = best;
     }
+    // the slab thickness of the x and y sweeps (0 = whole axes), over whole
+    // diffusion steps; slabs up to the size of L2
+    build_all(m);
+    int l2 = 0;
+    BFVM_CUDA(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, m->device));
+    const size_t plane_bytes = (size_t)m->nx * m->ny * m->S * m->elem();
+    int best_k = 0;
+    float best_ms = 1e30f;
+    for (int k : {0, 2, 4, 8, 16, 32, 64}) {
+      if (k > 0 && (k >= m->nz || (size_t)k * plane_bytes > (size_t)l2)) continue;
+      m->slab_planes = k;
+      step_once(m, dt, BFVM_STEP_DIFFUSION, nullptr);  // warm-up
+      BFVM_CUDA(cudaEventRecord(e0, m->stream));
+      for (int r = 0; r < reps; ++r) step_once(m, dt, BFVM_STEP_DIFFUSION, nullptr);
+      BFVM_CUDA(cudaEventRecord(e1, m->stream));
+      BFVM_CUDA(cudaEventSynchronize(e1));
+      float ms = 0;
+      BFVM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      if (ms < best_ms) {
+        best_ms = ms;
+        best_k = k;
+      }
+    }
+    m->slab_planes = best_k;
+    // whether the bulk and cell updates run inside the x sweep's prologue
+    // (same results either way), over whole steps
+    if (!m->bulk_vox.empty() || m->n_agents > 0) {
+      int best_f = 0;
+      best_ms = 1e30f;
+      for (int f : {0, 1}) {
+        m->fuse_sources = f;
+        step_once(m, dt, BFVM_STEP_ALL, nullptr);  // warm-up (and its lists)
+        BFVM_CUDA(cudaEventRecord(e0, m->stream));
+        for (int r = 0; r < reps; ++r) step_once(m, dt, BFVM_STEP_ALL, nullptr);
+        BFVM_CUDA(cudaEventRecord(e1, m->stream));
+        BFVM_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        BFVM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        if (ms < best_ms) {
+          best_ms = ms;
+          best_f = f;
+        }
+      }
+      m->fuse_sources = best_f;
+    }
   } catch (...) {
+    m->fuse_sources = saved_fuse;
+    m->slab_planes = saved_slab;
     m->path = saved_path;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -1835,6 +1951,13 @@ int bfvm_synchronize(bfvm_solver* m) {
 
 int bfvm_set_fuse_sources(bfvm_solver* m, int fuse) {
   return SOLVER_CALL(m, { m->fuse_sources = fuse ? 1 : 0; });
+}
+
+int bfvm_get_fuse_sources(bfvm_solver* m, int* fuse) {
+  return SOLVER_CALL(m, {
+    require(fuse != nullptr, "null output pointer");
+    *fuse = m->fuse_sources;
+  });
 }
 
 int bfvm_set_kernel_path(bfvm_solver* m, int path) {

@@ -192,6 +192,7 @@ struct bfvm_solver {
   int path = 0;  // BFVM_PATH_*
   int fuse_sources = 0;  // bulk/cell updates in the x sweep's prologue
   int lod_dims = 3;      // 2 while a LOD_2D step runs: sweeps of the z = 0 plane only
+  int slab_planes = 0;   // x and y sweeps by slabs of this many z planes (0: whole field)
   // cached tensor maps of the y and z sweeps (keyed by field pointer)
   CUtensorMap maps[3];
   const void* map_key[3] = {nullptr, nullptr, nullptr};
@@ -236,7 +237,8 @@ void build_all(bfvm_solver* m);
 void check_lod_mesh(bfvm_solver* m);
 void check_status(bfvm_solver* m);
 void step_once(bfvm_solver* m, double dt, int flags, cudaEvent_t* ev);
-void sweep(bfvm_solver* m, int ax, int fuse, double dt);
+void sweep(bfvm_solver* m, int ax, int fuse, double dt, int64_t z0 = 0, int64_t z1 = -1);
+void tune_sweeps(bfvm_solver* m, double dt, int reps);
 void bulk_any(bfvm_solver* m, double dt);
 void cells_any(bfvm_solver* m);
 template <typename T>

@@ -224,6 +224,11 @@ class Solver:
     def set_fuse_sources(self, fuse: bool) -> None:
         call("bfvm_set_fuse_sources", self._h, 1 if fuse else 0)
 
+    def get_fuse_sources(self) -> bool:
+        f = ctypes.c_int()
+        call("bfvm_get_fuse_sources", self._h, ctypes.byref(f))
+        return bool(f.value)
+
     def synchronize(self) -> None:
         call("bfvm_synchronize", self._h)
 
@@ -238,6 +243,15 @@ class Solver:
         n = ctypes.c_int64()
         call("bfvm_get_launch_count", self._h, ctypes.byref(n))
         return n.value
+
+    def set_slab_planes(self, planes: int) -> None:
+        """x and y sweeps by slabs of `planes` z planes (0: whole axes)."""
+        call("bfvm_set_slab_planes", self._h, planes)
+
+    def get_slab_planes(self) -> int:
+        k = ctypes.c_int()
+        call("bfvm_get_slab_planes", self._h, ctypes.byref(k))
+        return k.value
 
     def profile_step(self, dt: float, nsteps: int, flags: int = _abi.STEP_ALL):
         """(sources, x, y, z) milliseconds per step."""

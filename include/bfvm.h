@@ -211,6 +211,7 @@ BFVM_API int bfvm_set_kernel_path(bfvm_solver* m, int path);
  * over the stored voxel lists before the x sweep; 1 applies them inside the
  * x sweep's prologue.  Same results either way. */
 BFVM_API int bfvm_set_fuse_sources(bfvm_solver* m, int fuse);
+BFVM_API int bfvm_get_fuse_sources(bfvm_solver* m, int* fuse);
 BFVM_API int bfvm_get_sweep_config(bfvm_solver* m, int axis, int* config);
 
 BFVM_API int bfvm_synchronize(bfvm_solver* m);
@@ -223,16 +224,31 @@ BFVM_API int bfvm_get_launch_count(bfvm_solver* m, int64_t* count);
  * kernel that can run it -- the register kernel at each chunk length and
  * block width, the TMA-fed kernel and the direct kernel at each chunk
  * length -- over reps sweeps of this solver's own field, and keeps the
- * fastest for later steps (used while the kernel path is BFVM_PATH_AUTO).
+ * fastest for later steps (used while the kernel path is BFVM_PATH_AUTO);
+ * then the slab thickness of bfvm_set_slab_planes and bfvm_set_fuse_sources,
+ * over whole steps.
  * The field is saved before and restored after; bfvm_set_sweep_config or
  * a resize resets the choice.  bfvm_get_sweep_kernel returns the axis's
  * kernel (0 = the default choice, else a BFVM_PATH_* value). */
 BFVM_API int bfvm_tune_sweeps(bfvm_solver* m, double dt, int reps);
 BFVM_API int bfvm_get_sweep_kernel(bfvm_solver* m, int axis, int* kind);
 
+/* Runs the x and y sweeps of a step slab by slab: for each slab of `planes`
+ * z planes the x sweep, then the y sweep (an x line and a y line lie in one
+ * plane, so the y sweep of a slab needs only that slab's x sweep).  A slab
+ * that fits in L2 is written by the x sweep and read back by the y sweep
+ * from L2, so the field crosses HBM once for both sweeps instead of twice.
+ * 0 (the default) sweeps whole axes; bfvm_tune_sweeps also picks this.
+ * Results equal the whole-axis sweeps' to the last bit whenever the same
+ * kernels run. */
+BFVM_API int bfvm_set_slab_planes(bfvm_solver* m, int planes);
+BFVM_API int bfvm_get_slab_planes(bfvm_solver* m, int* planes);
+
 /* Times bfvm_step's kernels with CUDA events on the solver's stream, averaged
  * over nsteps steps: ms[4] = source kernels (bulk + cells), x sweep (with its
- * Dirichlet prologue/epilogue), y sweep, z sweep. */
+ * Dirichlet prologue/epilogue), y sweep, z sweep.  With slabs
+ * (bfvm_set_slab_planes) the x entry holds the x and y sweeps together and
+ * the y entry is 0. */
 BFVM_API int bfvm_profile_step(bfvm_solver* m, double dt, int nsteps, int flags, double* ms);
 
 /* Microenvironment::compute_all_gradient_vectors (BioFVM_microenvironment.cpp:
@@ -290,8 +306,10 @@ BFVM_API int bfvm_batch_clear(bfvm_batch* b);
 BFVM_API int bfvm_batch_size(bfvm_batch* b, int* count);
 BFVM_API int bfvm_batch_step(bfvm_batch* b, double dt, int nsteps, int flags);
 /* Autotuner: times short graph runs (trial_steps steps) of candidate chunk
- * lengths x threads per block for each axis, then candidate group budgets,
- * and keeps the fastest.  The members' fields are saved before and restored
+ * lengths x threads per block for each axis, tunes every member's own sweeps
+ * (bfvm_tune_sweeps, which branch mode runs), then candidate group budgets
+ * in both modes (BFVM_BATCH_FUSED, BFVM_BATCH_BRANCHES), and keeps the
+ * fastest.  The members' fields are saved before and restored
  * after, so tuning does not advance the simulation. */
 BFVM_API int bfvm_batch_tune(bfvm_batch* b, double dt, int flags, int trial_steps);
 /* chunk[3] in {8,16,32} with threads[3] in {128,256,512} per axis, or 0/0 to
@@ -299,6 +317,18 @@ BFVM_API int bfvm_batch_tune(bfvm_batch* b, double dt, int flags, int trial_step
 BFVM_API int bfvm_batch_set_config(bfvm_batch* b, const int* chunk, const int* threads,
                                    int64_t group_bytes);
 BFVM_API int bfvm_batch_get_config(bfvm_batch* b, int* chunk, int* threads, int64_t* group_bytes);
+/* How a group of members runs (the whole call stays one CUDA-graph launch):
+ *   BFVM_BATCH_FUSED     every phase of a step is one launch over all of the
+ *                        group's members (default);
+ *   BFVM_BATCH_BRANCHES  every member runs its own single-instance kernels
+ *                        (its own sweep choices, bfvm_tune_sweeps) on its own
+ *                        branch of the graph; the branches of a group run
+ *                        concurrently.
+ * bfvm_batch_tune chooses between them. */
+#define BFVM_BATCH_FUSED 0
+#define BFVM_BATCH_BRANCHES 1
+BFVM_API int bfvm_batch_set_mode(bfvm_batch* b, int mode);
+BFVM_API int bfvm_batch_get_mode(bfvm_batch* b, int* mode);
 /* Groups of the last plan and kernel launches in its graph. */
 BFVM_API int bfvm_batch_get_plan(bfvm_batch* b, int* groups, int64_t* kernels_per_call);
 BFVM_API int bfvm_batch_synchronize(bfvm_batch* b);

@@ -7,6 +7,7 @@ import pytest
 
 from biofvm_b200 import STEP_ALL, STEP_CELLS, STEP_DIFFUSION, Batch, BfvmError, Solver, load_scenario
 from biofvm_b200 import workloads as W
+from biofvm_b200._abi import BATCH_BRANCHES, BATCH_FUSED
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
@@ -28,7 +29,7 @@ def members(seed=71, count=6):
     return out
 
 
-def run_batch(scns, steps, flags=STEP_ALL, config=None, tune=False, calls=1):
+def run_batch(scns, steps, flags=STEP_ALL, config=None, tune=False, calls=1, mode=BATCH_FUSED):
     sols = [Solver(0) for _ in scns]
     for sv, scn in zip(sols, scns):
         load_scenario(sv, scn)
@@ -37,6 +38,7 @@ def run_batch(scns, steps, flags=STEP_ALL, config=None, tune=False, calls=1):
             bt.add(sv)
         if config:
             bt.set_config(*config)
+        bt.set_mode(mode)
         if tune:
             bt.tune(scns[0].dt, flags, 2)
         for _ in range(calls):
@@ -167,3 +169,107 @@ def test_batched_workload_small_sample_matches_plain():
             sv.step(scn.dt, 5)
             plain = sv.get_densities()
         assert np.all(O.max_rel_err(p, plain) <= TOL_BATCH_VS_PLAIN), scn.shape
+
+
+# ---- branch mode: every member's own single-instance kernels on concurrent
+# graph branches ----
+
+def plain_solves(scns, steps, flags=STEP_ALL):
+    out = []
+    for scn in scns:
+        with Solver(0) as sv:
+            load_scenario(sv, scn)
+            sv.step(scn.dt, steps, flags)
+            out.append(sv.get_densities())
+    return out
+
+
+@pytest.mark.parametrize("budget", [-1, 0, 200_000], ids=["default-groups", "one-group",
+                                                         "small-groups"])
+def test_branches_reproduce_plain_solves_bit_for_bit(budget):
+    """The same kernels in the same order per member: identical fields."""
+    scns = members(seed=81, count=6)
+    got, (groups, kernels) = run_batch(scns, 3, config=((0, 0, 0), (0, 0, 0), budget),
+                                       mode=BATCH_BRANCHES)
+    assert kernels > 0
+    if budget == 0:
+        assert groups == 1
+    for p, ref in zip(got, plain_solves(scns, 3)):
+        assert np.array_equal(p, ref)
+
+
+def test_branches_match_oracle_per_member():
+    scns = members(seed=82, count=5)
+    got, _ = run_batch(scns, 3, mode=BATCH_BRANCHES)
+    for scn, p in zip(scns, got):
+        ref = O.oracle_run(scn, 3, 7)
+        assert np.all(O.max_rel_err(p, ref) <= TOL64), scn.shape
+
+
+def test_branches_graph_replay_and_partial_flags():
+    scns = members(seed=83, count=4)
+    got, _ = run_batch(scns, 2, calls=3, mode=BATCH_BRANCHES)
+    for p, ref in zip(got, plain_solves(scns, 6)):
+        assert np.array_equal(p, ref)
+    for flags in (STEP_DIFFUSION, STEP_CELLS | 1):
+        got, _ = run_batch(scns, 2, flags=flags, mode=BATCH_BRANCHES)
+        for scn, p in zip(scns, got):
+            ref = O.oracle_run(scn, 2, flags)
+            assert np.all(O.max_rel_err(p, ref) <= TOL64), (flags, scn.shape)
+
+
+def test_branches_see_member_changes_between_calls():
+    """New agents on a member between calls (another count: new device
+    buffers): the graph is captured again."""
+    a = W.mixed_small(shape=(10, 9, 8), S=2, n_agents=100, seed=84)
+    b = W.mixed_small(shape=(10, 9, 8), S=2, n_agents=400, seed=85)
+    c = W.mixed_small(shape=(7, 12, 5), S=3, n_agents=60, seed=86)
+    s1, s2 = Solver(0), Solver(0)
+    load_scenario(s1, a)
+    load_scenario(s2, c)
+    r1, r2 = Solver(0), Solver(0)
+    load_scenario(r1, a)
+    load_scenario(r2, c)
+    with Batch(0) as bt:
+        bt.set_mode(BATCH_BRANCHES)
+        bt.add(s1)
+        bt.add(s2)
+        bt.step(a.dt, 2)
+        r1.step(a.dt, 2)
+        r2.step(a.dt, 2)
+        for sv in (s1, r1):
+            sv.set_agents(*b.agent_arrays())
+        bt.step(a.dt, 2)
+        r1.step(a.dt, 2)
+        r2.step(a.dt, 2)
+        bt.synchronize()
+        assert np.array_equal(s1.get_densities(), r1.get_densities())
+        assert np.array_equal(s2.get_densities(), r2.get_densities())
+    for sv in (s1, s2, r1, r2):
+        sv.close()
+
+
+def test_tuner_picks_a_mode_and_keeps_fields():
+    scns = members(seed=87, count=4)
+    sols = [Solver(0) for _ in scns]
+    for sv, scn in zip(sols, scns):
+        load_scenario(sv, scn)
+    with Batch(0) as bt:
+        for sv in sols:
+            bt.add(sv)
+        bt.tune(scns[0].dt, STEP_ALL, 2)
+        assert bt.get_mode() in (BATCH_FUSED, BATCH_BRANCHES)
+        bt.step(scns[0].dt, 2)
+        bt.synchronize()
+        got = [sv.get_densities() for sv in sols]
+    for sv in sols:
+        sv.close()
+    for scn, p in zip(scns, got):
+        ref = O.oracle_run(scn, 2, 7)
+        assert np.all(O.max_rel_err(p, ref) <= TOL64), scn.shape
+
+
+def test_set_mode_rejects_unknown_modes():
+    with Batch(0) as bt:
+        with pytest.raises(BfvmError):
+            bt.set_mode(7)

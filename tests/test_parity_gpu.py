@@ -377,3 +377,70 @@ def test_sweep_tuner_keeps_the_field_and_the_results(shape):
         sv.step(scn.dt, 3)
         got = sv.get_densities()
     assert np.all(rel_err(got, O.oracle_run(scn, 3, 7)) <= TOL64), chosen
+
+
+# ---- x and y sweeps by slabs of z planes (bfvm_set_slab_planes) ----
+
+def _run_slabs(scn, steps, planes, path=PATH_AUTO, flags=7, precision=64):
+    with Solver(0) as sv:
+        load_scenario(sv, scn)
+        sv.set_kernel_path(path)
+        if precision != 64:
+            sv.set_precision(precision)
+        sv.set_slab_planes(planes)
+        assert sv.get_slab_planes() == planes
+        sv.step(scn.dt, steps, flags)
+        return sv.get_densities()
+
+
+@pytest.mark.parametrize("path", [PATH_AUTO, PATH_TMA, PATH_GENERIC], ids=["auto", "tma", "generic"])
+@pytest.mark.parametrize("planes", [1, 2, 3, 7, 29])
+def test_slabs_reproduce_whole_axis_sweeps(planes, path):
+    """The same kernels on every line, only in another order: identical
+    fields (Dirichlet nodes, bulk and agents included; 30 planes, so the last
+    slab is partial for most thicknesses)."""
+    scn = W.mixed_small(shape=(33, 21, 30), S=3, n_agents=400, seed=95)
+    whole = _run_slabs(scn, 3, 0, path)
+    got = _run_slabs(scn, 3, planes, path)
+    assert np.array_equal(got, whole)
+    assert np.all(rel_err(got, O.oracle_run(scn, 3, 7)) <= TOL64)
+
+
+@pytest.mark.parametrize("planes", [2, 5])
+def test_slabs_on_the_direct_path_and_fp32(planes):
+    """Slabs through the direct kernel, and in FP32: the same fields as the
+    whole-axis sweeps."""
+    scn = W.mixed_small(shape=(40, 24, 17), S=2, n_agents=200, seed=96)
+    got = _run_slabs(scn, 3, planes, PATH_DIRECT)
+    assert np.array_equal(got, _run_slabs(scn, 3, 0, PATH_DIRECT))
+    assert np.all(rel_err(got, O.oracle_run(scn, 3, 7)) <= TOL64)
+    got32 = _run_slabs(scn, 3, planes, PATH_AUTO, precision=32)
+    whole32 = _run_slabs(scn, 3, 0, PATH_AUTO, precision=32)
+    assert np.array_equal(got32, whole32)
+
+
+def test_slabs_leave_lod2d_alone_and_reject_negative():
+    scn = W.mixed_small(shape=(17, 13, 1), S=2, n_agents=0, seed=97, bulk=False)
+    ref = O.oracle_lod2d_run(scn, 3)
+    with Solver(0) as sv:
+        load_scenario(sv, scn)
+        sv.set_slab_planes(1)
+        for _ in range(3):
+            sv.simulate_diffusion_decay_2d(scn.dt)
+        assert np.all(rel_err(sv.get_densities(), ref) <= TOL64)
+        with pytest.raises(BfvmError):
+            sv.set_slab_planes(-1)
+
+
+def test_tuner_picks_a_slab_thickness():
+    scn = W.mixed_small(shape=(48, 40, 64), S=4, n_agents=500, seed=98)
+    with Solver(0) as sv:
+        load_scenario(sv, scn)
+        before = sv.get_densities()
+        sv.tune_sweeps(scn.dt, 2)
+        assert np.array_equal(sv.get_densities(), before)
+        k = sv.get_slab_planes()
+        assert k in (0, 2, 4, 8, 16, 32)
+        sv.step(scn.dt, 3)
+        got = sv.get_densities()
+    assert np.all(rel_err(got, O.oracle_run(scn, 3, 7)) <= TOL64), k

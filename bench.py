@@ -262,7 +262,7 @@ def run_ours(args, world, rank, local):
     # warm-up (also builds the Thomas coefficients and the device lists), then
     # the per-axis kernel choice timed on this field (which is restored)
     sv.step(dt, args.warmup, STEP_ALL)
-    tuned = sv.tune_sweeps(dt, 3) if not args.no_tune else [(0, 0, 0)] * 3
+    tuned = sv.tune_sweeps(dt, 3) if not args.no_tune else [(0, 0, 0, 0)] * 3
     sv.synchronize()
 
     launches0 = sv.launch_count
@@ -286,11 +286,17 @@ def run_ours(args, world, rank, local):
 
     # per-kernel device times on the solver's stream (CUDA events between sweeps)
     ks, kx, ky, kz = sv.profile_step(dt, max(3, min(args.steps, 10)), STEP_ALL)
-    per = {"x_sweep": kx, "y_sweep": ky, "z_sweep": kz}
+    if sv.get_slab_planes() > 0:
+        # x and y by slabs: their events bracket both sweeps together
+        per = {"xy_sweeps_by_slabs": kx, "z_sweep": kz}
+        sweeps_in = {"xy_sweeps_by_slabs": 2, "z_sweep": 1}
+    else:
+        per = {"x_sweep": kx, "y_sweep": ky, "z_sweep": kz}
+        sweeps_in = {"x_sweep": 1, "y_sweep": 1, "z_sweep": 1}
     dom = max(per, key=per.get)
     per["sources"] = ks
     hbm, peak_kind = peaks()
-    achieved = BYTES_PER_VS_SWEEP * N * S / (per[dom] / 1e3) / 1e9
+    achieved = sweeps_in[dom] * BYTES_PER_VS_SWEEP * N * S / (per[dom] / 1e3) / 1e9
     traffic = ncu_traffic(dom)
 
     # end to end through the C ABI with host buffers: every step uploads the
@@ -356,10 +362,12 @@ def run_ours(args, world, rank, local):
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / hbm,
                          "traffic": traffic,
-                         "algorithmic_bytes_per_launch": BYTES_PER_VS_SWEEP * N * S},
+                         "algorithmic_bytes_per_launch": sweeps_in[dom] * BYTES_PER_VS_SWEEP * N * S},
             "kernel_ms": per,
             "tuned_sweeps": [{"axis": "xyz"[i], "kernel": ["default", "register", "tma", "direct"][k],
-                              "chunk": ch, "columns": tw} for i, (k, ch, tw) in enumerate(tuned)],
+                              "chunk": ch, "columns": tw, "min_blocks": mb}
+                             for i, (k, ch, tw, mb) in enumerate(tuned)],
+            "slab_planes": sv.get_slab_planes(), "fuse_sources": sv.get_fuse_sources(),
             "gpu_launches": int(launches),
             "e2e": e2e,
             "cpu_baseline": cpu,
@@ -638,8 +646,8 @@ def run_adjoint(args, world, rank, local):
     target made by the forward run with every parameter scaled by
     (1 + 0.01 N(0,1)) (seeded).  Reports the forward (with checkpoints) and
     backward device times, their ratio, and the agreement of the gradient
-    with central finite differences (h = 1e-6 relative) along random
-    directions."""
+    with central finite differences (h = 1e-6 relative) along a random
+    direction in each parameter group and in all of them."""
     import numpy as np
 
     from biofvm_b200 import workloads as W
@@ -678,16 +686,22 @@ def run_adjoint(args, world, rank, local):
     sv.step(scn.dt, args.steps)
     sv.synchronize()
     t_plain = time.perf_counter() - t_plain
+    # central differences (h = 1e-6, relative: theta +- h * theta * N(0,1))
+    # along a random direction in each parameter group, then in all groups
+    # at once (the groups' contributions partly cancel there, so that check
+    # sits closer to the differences' rounding floor)
     checks = []
-    for d in range(2):
-        v = [x * rng.standard_normal(x.shape) for x in th]
+    names = ["secretion", "uptake", "D", "decay"]
+    for group in [0, 1, 2, 3, None]:
+        v = [x * rng.standard_normal(x.shape) if group in (None, j) else np.zeros_like(x)
+             for j, x in enumerate(th)]
         h = 1e-6
         pp = prob.run(*[a + h * b for a, b in zip(th, v)])
         pm = prob.run(*[a - h * b for a, b in zip(th, v)])
         fd = loss_difference(pp, pm, target) / (2 * h)
-        adj = (np.sum(g["secretion"] * v[0]) + np.sum(g["uptake"] * v[1]) +
-               np.sum(g["D"] * v[2]) + np.sum(g["decay"] * v[3]))
-        checks.append({"fd": fd, "adjoint": adj, "rel_diff": abs(adj - fd) / abs(fd)})
+        adj = sum(float(np.sum(g[nm] * vj)) for nm, vj in zip(names, v))
+        checks.append({"direction": names[group] if group is not None else "all",
+                       "fd": fd, "adjoint": adj, "rel_diff": abs(adj - fd) / abs(fd)})
     prob.close()
     if rank == 0:
         vs = scn.num_voxels * S * args.steps
@@ -702,6 +716,8 @@ def run_adjoint(args, world, rank, local):
             "forward_seconds": t_fwd, "backward_seconds": t_bwd,
             "plain_forward_seconds": t_plain, "backward_over_forward": t_bwd / t_plain,
             "gradient_vs_central_differences": checks,
+            "max_rel_diff_per_group": max(c["rel_diff"] for c in checks
+                                          if c["direction"] != "all"),
             "clocks": clocks.summary(),
         }
         print(json.dumps(line), flush=True)

@@ -199,7 +199,8 @@ class Solver:
 
     def tune_sweeps(self, dt: float, reps: int = 5):
         """Picks each axis's fastest sweep kernel by timing them on this field
-        (which is restored); returns [(kernel, chunk, columns)] per axis."""
+        (which is restored); returns [(kernel, chunk, columns, min_blocks)]
+        per axis."""
         call("bfvm_tune_sweeps", self._h, dt, reps)
         out = []
         for ax in range(3):
@@ -207,7 +208,7 @@ class Solver:
             call("bfvm_get_sweep_kernel", self._h, ax, ctypes.byref(k))
             cfg = (ctypes.c_int * 3)()
             call("bfvm_get_sweep_config", self._h, ax, cfg)
-            out.append((k.value, cfg[0], cfg[1]))
+            out.append((k.value, cfg[0], cfg[1], cfg[2]))
         return out
 
     def set_sweep_config(self, axis: int, chunk: int, columns: int, min_blocks: int = 1) -> None:

@@ -338,8 +338,13 @@ __global__ void __launch_bounds__(W * MAXNC)
 
 // ---------------------------------------------------------------------------
 
+// Blocks of up to 256 threads with chunks of up to 16 points are compiled for
+// two resident blocks per SM (the plan sizes their shared memory for two).
+constexpr int rows_min_blocks(int ch, int maxt) { return (ch <= 16 && maxt <= 256) ? 2 : 1; }
+
 template <typename T, int CH, int STAGES, bool SMEM_TAB, int MAXT, typename CT = T>
-__global__ void __launch_bounds__(MAXT) lod_rows_tma_kernel(const RowsArgs<T, CT> a) {
+__global__ void __launch_bounds__(MAXT, rows_min_blocks(CH, MAXT))
+    lod_rows_tma_kernel(const RowsArgs<T, CT> a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   // Threads: column (r, s) fastest, then chunk c.  A stage holds R rows at a
   // padded pitch (pitch = S mod 16 elements), so the lanes of a warp, which

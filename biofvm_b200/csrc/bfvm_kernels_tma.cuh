@@ -218,6 +218,21 @@ __device__ __forceinline__ void chunk_fix(T (&v)[CH], int len, const T* kg, int 
   }
 }
 
+// Self-test of the error path of the bounded waits: one thread initialises a
+// barrier that expects one arrival, never arrives, and waits on it with the
+// sweeps' wait (limit_ns).  The wait gives up, the kernel records it in
+// status as a sweep that gave up would, and returns; no copy was issued, so
+// none is in flight.
+static __global__ void bounded_wait_selftest_kernel(unsigned long long limit_ns,
+                                                    int* __restrict__ status) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x != 0) return;
+  tma::mbar_init(&bar, 1);
+  tma::fence_barrier_init();
+  if (!tma::mbar_wait(&bar, 0, limit_ns)) atomicExch(status, 1);
+  tma::mbar_inval(&bar);
+}
+
 // Bounded waits for the copies still in flight after a failure, then status.
 __device__ __forceinline__ void drain_after_failure(uint64_t* full, int stages, int next_i,
                                                     int outstanding, int* status) {

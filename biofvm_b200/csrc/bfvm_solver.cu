@@ -1750,6 +1750,48 @@ int bfvm_set_precision(bfvm_solver* m, int precision) {
   });
 }
 
+int bfvm_selftest_bounded_wait(int device, int64_t limit_ns, int* gave_up, double* waited_ms) {
+  return guarded([&] {
+    require(gave_up != nullptr && waited_ms != nullptr, "null output pointer");
+    require(limit_ns >= 1000 && limit_ns <= (int64_t)bfvm::tma::kWaitLimitNs,
+            "limit_ns must be in [1e3, 2e9]");
+    int ndev = 0;
+    BFVM_CUDA(cudaGetDeviceCount(&ndev));
+    require(device >= 0 && device < ndev, "no CUDA device " + std::to_string(device));
+    DeviceGuard dg(device);
+    cudaStream_t st = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    DevBuf status;
+    struct Release {
+      cudaStream_t& st;
+      cudaEvent_t& e0;
+      cudaEvent_t& e1;
+      ~Release() {
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        if (st) cudaStreamDestroy(st);
+      }
+    } release{st, e0, e1};
+    BFVM_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    BFVM_CUDA(cudaEventCreate(&e0));
+    BFVM_CUDA(cudaEventCreate(&e1));
+    status.ensure(sizeof(int));
+    BFVM_CUDA(cudaMemsetAsync(status.ptr, 0, sizeof(int), st));
+    BFVM_CUDA(cudaEventRecord(e0, st));
+    bfvm::bounded_wait_selftest_kernel<<<1, 32, 0, st>>>((unsigned long long)limit_ns,
+                                                        status.as<int>());
+    BFVM_CUDA(cudaGetLastError());
+    BFVM_CUDA(cudaEventRecord(e1, st));
+    int h = 0;
+    BFVM_CUDA(cudaMemcpyAsync(&h, status.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
+    BFVM_CUDA(cudaStreamSynchronize(st));
+    float ms = 0;
+    BFVM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    *gave_up = h;
+    *waited_ms = ms;
+  });
+}
+
 int bfvm_set_slab_planes(bfvm_solver* m, int planes) {
   return SOLVER_CALL(m, {
     require(planes >= 0, "planes must be >= 0");

@@ -261,6 +261,17 @@ class Solver:
         return tuple(ms)
 
 
+def selftest_bounded_wait(device: int = 0, limit_ns: int = 2_000_000):
+    """Runs the error path of the TMA sweeps' bounded waits on `device`: a
+    kernel waits on a barrier that nothing completes and gives up after
+    limit_ns.  Returns (gave_up, waited_ms); the device stays usable."""
+    _abi.load_library()
+    g = ctypes.c_int()
+    ms = ctypes.c_double()
+    call("bfvm_selftest_bounded_wait", device, limit_ns, ctypes.byref(g), ctypes.byref(ms))
+    return bool(g.value), ms.value
+
+
 def load_scenario(sv: Solver, scn) -> None:
     """Sets a Solver up from a workloads.Scenario, the way a reference driver
     would: resize, densities and coefficients, initial field, bulk rates,

@@ -244,6 +244,15 @@ BFVM_API int bfvm_get_sweep_kernel(bfvm_solver* m, int axis, int* kind);
 BFVM_API int bfvm_set_slab_planes(bfvm_solver* m, int planes);
 BFVM_API int bfvm_get_slab_planes(bfvm_solver* m, int* planes);
 
+/* Self-test of the TMA sweeps' error path on `device`: a kernel waits on a
+ * barrier that nothing completes, with the sweeps' bounded wait limited to
+ * limit_ns (1 us .. 2 s); the wait gives up and the kernel returns with its
+ * status set, as a sweep that gave up waiting for a copy would.
+ * *gave_up = 1 when the status came back set, *waited_ms = the kernel's
+ * time.  The device stays usable afterwards. */
+BFVM_API int bfvm_selftest_bounded_wait(int device, int64_t limit_ns, int* gave_up,
+                                        double* waited_ms);
+
 /* Times bfvm_step's kernels with CUDA events on the solver's stream, averaged
  * over nsteps steps: ms[4] = source kernels (bulk + cells), x sweep (with its
  * Dirichlet prologue/epilogue), y sweep, z sweep.  With slabs

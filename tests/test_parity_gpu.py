@@ -444,3 +444,20 @@ def test_tuner_picks_a_slab_thickness():
         sv.step(scn.dt, 3)
         got = sv.get_densities()
     assert np.all(rel_err(got, O.oracle_run(scn, 3, 7)) <= TOL64), k
+
+
+# ---- error path of the bounded waits (no GPU fault involved) ----
+
+def test_bounded_wait_gives_up_and_the_device_stays_usable():
+    """A kernel waits, with the sweeps' bounded wait, on a barrier that
+    nothing completes: it must give up after the limit, report it through the
+    status word, and leave the context usable for a normal step."""
+    from biofvm_b200.solver import selftest_bounded_wait
+
+    gave_up, ms = selftest_bounded_wait(0, 3_000_000)  # 3 ms
+    assert gave_up
+    assert 2.5 <= ms < 1000.0, ms
+    scn = W.mixed_small(shape=(20, 18, 16), S=2, n_agents=100, seed=99)
+    assert np.all(rel_err(run_gpu(scn, 2, 7, path=PATH_TMA), O.oracle_run(scn, 2, 7)) <= TOL64)
+    with pytest.raises(BfvmError):
+        selftest_bounded_wait(0, 10)  # below the 1 us floor

@@ -7,7 +7,7 @@
 // step is bulk -> cells -> Dirichlet, x sweep, Dirichlet, y sweep,
 // Dirichlet, z sweep (BioFVM_solvers.cpp:175-273).
 //
-// Scheduling.  The instances are packed, in the order they were added, into
+// Scheduling.  The instances are packed, first fit in decreasing size, into
 // groups whose density fields together stay within a byte budget (by
 // default a fraction of the L2 cache), and all n steps of one group run
 // before the next group starts: a group small enough for L2 keeps its fields
@@ -54,7 +54,6 @@ struct BatchConfig {
 
 // Device descriptors of one group, all in one buffer.
 struct GroupPlan {
-  int first_inst = 0, n_inst = 0;  // members b->inst[first_inst ..]
   int64_t field_bytes = 0;
   size_t off_sweep[3] = {0, 0, 0}, off_bulk = 0, off_cells = 0, off_dir = 0;
   int n_sweep[3] = {0, 0, 0}, n_bulk = 0, n_cells = 0, n_dir = 0;
@@ -75,6 +74,7 @@ struct bfvm_batch {
   // current plan
   std::vector<unsigned char> host_desc;  // descriptor bytes of every group
   std::vector<bfvm_rt::GroupPlan> groups;
+  std::vector<std::vector<bfvm_solver*>> group_members;  // per group, in plan order
   int ch[3] = {16, 16, 16}, threads[3] = {256, 256, 256};
   bfvm_rt::DevBuf d_desc;
   // cached graph and what it was captured for
@@ -164,19 +164,30 @@ BatchSweep<T> sweep_desc(const bfvm_solver* m, int a, int ch, int threads, int64
   return d;
 }
 
-// Instances packed in order into groups of at most `budget` field bytes (a
-// single instance larger than the budget is a group of its own).
+// Instances packed into groups of at most `budget` field bytes, first fit
+// in decreasing size (a single instance larger than the budget is a group
+// of its own): small instances share groups, so that a group's members can
+// run side by side.  Members are independent, so the order is free.
 std::vector<std::vector<bfvm_solver*>> make_groups(const bfvm_batch* b, int64_t budget) {
   std::vector<std::vector<bfvm_solver*>> g;
-  int64_t cur = 0;
-  for (bfvm_solver* m : b->inst) {
-    const int64_t bytes = (int64_t)(m->NS() * m->elem());
-    if (g.empty() || (budget > 0 && cur + bytes > budget)) {
+  if (budget <= 0) {
+    g.push_back(b->inst);
+    return g;
+  }
+  std::vector<bfvm_solver*> order(b->inst);
+  auto bytes = [](const bfvm_solver* m) { return (int64_t)(m->NS() * m->elem()); };
+  std::stable_sort(order.begin(), order.end(),
+                   [&](const bfvm_solver* x, const bfvm_solver* y) { return bytes(x) > bytes(y); });
+  std::vector<int64_t> used;
+  for (bfvm_solver* m : order) {
+    size_t k = 0;
+    while (k < g.size() && used[k] + bytes(m) > budget) ++k;
+    if (k == g.size()) {
       g.emplace_back();
-      cur = 0;
+      used.push_back(0);
     }
-    g.back().push_back(m);
-    cur += bytes;
+    g[k].push_back(m);
+    used[k] += bytes(m);
   }
   return g;
 }
@@ -188,13 +199,10 @@ void build_plan(bfvm_batch* b) {
   std::vector<unsigned char>& buf = b->host_desc;
   buf.clear();
   b->groups.clear();
-  int next_inst = 0;
+  b->group_members = groups;
   for (auto& members : groups) {
     GroupPlan G;
     std::memset(&G, 0, sizeof G);
-    G.first_inst = next_inst;
-    G.n_inst = (int)members.size();
-    next_inst += G.n_inst;
     for (bfvm_solver* m : members) G.field_bytes += (int64_t)(m->NS() * m->elem());
     for (int a = 0; a < 3; ++a) {
       align_to(buf, 64);
@@ -390,21 +398,21 @@ cudaGraphExec_t capture(bfvm_batch* b, double dt, int nsteps, int flags, int axe
   if (branches) warm_instances(b, dt, flags);
   BFVM_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
   try {
-    for (const GroupPlan& G : b->groups) {
+    for (size_t gi = 0; gi < b->groups.size(); ++gi) {
+      const GroupPlan& G = b->groups[gi];
       if (branches) {
         // fork: every member's own stream joins the capture after the work
         // captured so far; join: the batch stream waits for every member
+        const std::vector<bfvm_solver*>& members = b->group_members[gi];
         BFVM_CUDA(cudaEventRecord(b->ev, b->stream));
-        for (int i = G.first_inst; i < G.first_inst + G.n_inst; ++i)
-          BFVM_CUDA(cudaStreamWaitEvent(b->inst[i]->stream, b->ev, 0));
-        for (int i = G.first_inst; i < G.first_inst + G.n_inst; ++i) {
-          bfvm_solver* m = b->inst[i];
+        for (bfvm_solver* m : members) BFVM_CUDA(cudaStreamWaitEvent(m->stream, b->ev, 0));
+        for (bfvm_solver* m : members) {
           const int64_t before = m->launches;
           for (int it = 0; it < nsteps; ++it) enqueue_instance_step(m, dt, flags, axes);
           *kernels += m->launches - before;
         }
-        for (int i = G.first_inst; i < G.first_inst + G.n_inst; ++i) {
-          BFVM_CUDA(cudaEventRecord(b->ev, b->inst[i]->stream));
+        for (bfvm_solver* m : members) {
+          BFVM_CUDA(cudaEventRecord(b->ev, m->stream));
           BFVM_CUDA(cudaStreamWaitEvent(b->stream, b->ev, 0));
         }
         continue;

@@ -220,6 +220,27 @@ def test_long_lines_multiple_boxes():
         assert np.all(rel_err(p, ref) <= TOL64), path
 
 
+@pytest.mark.parametrize("shape", [(1024, 2, 3), (3, 1024, 2), (2, 3, 1024)],
+                         ids=["x", "y", "z"])
+def test_longest_lines(shape):
+    """Lines of 1024 points, the longest an axis may have (32 chunks of 32
+    points), on every kernel path."""
+    scn = W.mixed_small(shape=shape, S=2, n_agents=200, seed=sum(shape) + 1)
+    ref = O.oracle_run(scn, 2, 7)
+    for path in PATHS:
+        p = run_gpu(scn, 2, 7, path=path)
+        assert np.all(rel_err(p, ref) <= TOL64), path
+
+
+def test_lines_past_the_limit_are_rejected():
+    with Solver(0) as sv:
+        sv.resize_densities(1)
+        with pytest.raises(BfvmError) as e:
+            sv.resize_space(0, 10250, 0, 10, 0, 10, 10)  # 1025 points along x
+        assert "1024-point" in str(e.value)
+        sv.resize_space(0, 10240, 0, 10, 0, 10, 10)  # 1024: accepted
+
+
 @pytest.mark.slow
 def test_lod_256_full_size_two_steps():
     """The full 256^3 x 10 workload with 100k agents: two fused steps against

@@ -280,6 +280,23 @@ __global__ void bulk_kernel(T* __restrict__ p, int S, int64_t E, const int64_t* 
   p[q] = (T)bulk_update((double)p[q], st[t], su[t], dt);
 }
 
+// The same update with the coefficient rows shared between voxels: voxel
+// e's (S*T, U+S) for density s are tab[(row[e]*S + s)*2 + {0,1}] (the table
+// is small and stays in L1), so the stream is the density itself plus 8 B
+// per listed voxel.
+template <typename T>
+__global__ void bulk_rows_kernel(T* __restrict__ p, int S, int64_t E,
+                                 const int* __restrict__ voxel, const int* __restrict__ row,
+                                 const double* __restrict__ tab, double dt) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= E * S) return;
+  const int64_t e = t / S;
+  const int s = (int)(t - e * S);
+  const int64_t q = (int64_t)__ldg(voxel + e) * S + s;
+  const double* c = tab + ((int64_t)__ldg(row + e) * S + s) * 2;
+  p[q] = (T)bulk_update((double)p[q], __ldg(c), __ldg(c + 1), dt);
+}
+
 // simulate_cell_sources_and_sinks over the agents sorted by voxel (key[r] =
 // voxel of the r-th sorted agent, idx[r] = its position in the agent list;
 // the sort is stable).  One thread per (sorted agent, substrate): the thread

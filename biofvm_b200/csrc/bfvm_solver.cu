@@ -224,6 +224,44 @@ void build_bulk(bfvm_solver* m) {
   upload(m->d_bulk_vox, m->bulk_vox, st);
   upload(m->d_bulk_st, m->bulk_st, st);
   upload(m->d_bulk_su, m->bulk_su, st);
+  // shared coefficient rows (bitwise-equal rows once): worth it when they
+  // compress at least 4x and voxel indices fit int32
+  m->bulk_rows = 0;
+  if (m->N() < ((int64_t)1 << 31)) {
+    std::unordered_map<std::string, int> seen;
+    std::vector<int> vox32(E), row(E);
+    std::vector<double> tab;
+    const int64_t cap = std::max<int64_t>(1, E / 4);
+    std::string key((size_t)S * 2 * sizeof(double), '\0');
+    bool ok = true;
+    for (int64_t e = 0; e < E && ok; ++e) {
+      for (int s = 0; s < S; ++s) {
+        std::memcpy(&key[(size_t)s * 2 * sizeof(double)], &m->bulk_st[e * S + s], sizeof(double));
+        std::memcpy(&key[((size_t)s * 2 + 1) * sizeof(double)], &m->bulk_su[e * S + s],
+                    sizeof(double));
+      }
+      auto it = seen.find(key);
+      if (it == seen.end()) {
+        if ((int64_t)seen.size() >= cap) {
+          ok = false;
+          break;
+        }
+        it = seen.emplace(key, (int)seen.size()).first;
+        for (int s = 0; s < S; ++s) {
+          tab.push_back(m->bulk_st[e * S + s]);
+          tab.push_back(m->bulk_su[e * S + s]);
+        }
+      }
+      row[e] = it->second;
+      vox32[e] = (int)m->bulk_vox[e];
+    }
+    if (ok) {
+      upload(m->d_bulk_vox32, vox32, st);
+      upload(m->d_bulk_row, row, st);
+      upload(m->d_bulk_tab, tab, st);
+      m->bulk_rows = (int64_t)seen.size();
+    }
+  }
   const int ch = m->axis[0].ch, nc = (m->nx + ch - 1) / ch;
   std::vector<int64_t> line(E);
   std::vector<int> pos(E);
@@ -1068,9 +1106,14 @@ void bulk_standalone(bfvm_solver* m, double dt) {
   const int64_t E = (int64_t)m->bulk_vox.size();
   if (E == 0) return;
   const int64_t work = E * m->S;
-  bfvm::bulk_kernel<T><<<(unsigned)blocks_for(work, 256), 256, 0, m->stream>>>(
-      m->p.as<T>(), m->S, E, m->d_bulk_vox.as<int64_t>(), m->d_bulk_st.as<double>(),
-      m->d_bulk_su.as<double>(), dt);
+  if (m->bulk_rows > 0)
+    bfvm::bulk_rows_kernel<T><<<(unsigned)blocks_for(work, 256), 256, 0, m->stream>>>(
+        m->p.as<T>(), m->S, E, m->d_bulk_vox32.as<int>(), m->d_bulk_row.as<int>(),
+        m->d_bulk_tab.as<double>(), dt);
+  else
+    bfvm::bulk_kernel<T><<<(unsigned)blocks_for(work, 256), 256, 0, m->stream>>>(
+        m->p.as<T>(), m->S, E, m->d_bulk_vox.as<int64_t>(), m->d_bulk_st.as<double>(),
+        m->d_bulk_su.as<double>(), dt);
   check_launch(m);
 }
 

@@ -165,6 +165,11 @@ struct bfvm_solver {
   std::vector<double> bulk_st, bulk_su;
   bool bulk_dirty = true;
   bfvm_rt::DevBuf d_bulk_vox, d_bulk_st, d_bulk_su;
+  // the same list with its coefficient rows shared: voxel and row index
+  // (int32) per listed voxel, unique (S*T, U+S) rows [rows][S][2]; used by
+  // the stand-alone bulk kernel when the rows compress (bulk_rows > 0)
+  int64_t bulk_rows = 0;
+  bfvm_rt::DevBuf d_bulk_vox32, d_bulk_row, d_bulk_tab;
   bfvm_rt::DevSegList seg_bulk;
 
   // Dirichlet nodes in insertion order (BioFVM_microenvironment.h:102-103)

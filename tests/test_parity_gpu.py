@@ -70,6 +70,19 @@ def test_golden_cases(name, fused, path):
     assert np.all(np.isfinite(p))
 
 
+def test_bulk_with_shared_coefficient_rows_is_exact():
+    """A bulk region with one rate vector (the sphere of the headline
+    workload) runs the kernel that shares coefficient rows between voxels:
+    bulk steps alone must equal the oracle's bit for bit, and so must a
+    region where every voxel has its own rates (the per-voxel kernel)."""
+    scn = W.lod_cube(24, 3, 0, steps=3, seed=101, bulk_radius=80.0, name="bulk_rows")
+    assert len(scn.bulk_voxels) > 100
+    assert np.array_equal(run_gpu(scn, 3, STEP_BULK), O.oracle_run(scn, 3, STEP_BULK))
+    build, _, _, _ = CASES["small_bulk_only"]
+    scn2 = build()
+    assert np.array_equal(run_gpu(scn2, 3, STEP_BULK), O.oracle_run(scn2, 3, STEP_BULK))
+
+
 def test_dirichlet_alone_is_exact():
     scn = W.mixed_small(shape=(10, 9, 8), S=3, n_agents=0, seed=41)
     with Solver(0) as sv:

@@ -539,22 +539,27 @@ void launch_sweep(bfvm_solver* m, int ax, int fuse, double dt, int64_t z0 = 0, i
 
 // ---- TMA-fed persistent sweeps ---------------------------------------------
 
+// The driver's tensor-map encoder, looked up once (a static initialised by
+// the first caller; other threads wait for it; a failed lookup is retried).
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  if (!fn) {
+  static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
     void* ptr = nullptr;
     cudaDriverEntryPointQueryResult q;
     BFVM_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q));
     require(q == cudaDriverEntryPointSuccess && ptr != nullptr,
             "cuTensorMapEncodeTiled is not available from the driver", BFVM_ERR_CUDA);
-    fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(ptr);
-  }
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(ptr);
+  }();
   return fn;
 }
 
-// Raises the dynamic shared-memory limit of a kernel once per device.
+// Raises the dynamic shared-memory limit of a kernel once per device (solvers
+// on other host threads may launch the same kernels: the record is locked).
 void allow_smem(const void* kernel, int device, size_t bytes) {
+  static std::mutex mu;
   static std::unordered_map<const void*, uint64_t> done;  // kernel -> device bitmask
+  require(device >= 0 && device < 64, "device index out of range");
+  std::lock_guard<std::mutex> g(mu);
   uint64_t& mask = done[kernel];
   if (mask & (1ull << device)) return;
   BFVM_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -495,3 +495,53 @@ def test_bounded_wait_gives_up_and_the_device_stays_usable():
     assert np.all(rel_err(run_gpu(scn, 2, 7, path=PATH_TMA), O.oracle_run(scn, 2, 7)) <= TOL64)
     with pytest.raises(BfvmError):
         selftest_bounded_wait(0, 10)  # below the 1 us floor
+
+
+# ---- host threads, one solver each ----
+
+_THREADS_CHILD = r"""
+import sys, threading
+sys.path.insert(0, sys.argv[1])
+import numpy as np
+from biofvm_b200 import Solver, load_scenario
+from biofvm_b200 import workloads as W
+from biofvm_b200._abi import PATH_AUTO, PATH_TMA
+scns = [W.mixed_small(shape=(30 + 4 * i, 24, 20), S=2, n_agents=150, seed=200 + i) for i in range(4)]
+out = [None] * 4
+errs = []
+go = threading.Barrier(4)
+def work(i):
+    try:
+        with Solver(0) as sv:
+            load_scenario(sv, scns[i])
+            sv.set_kernel_path(PATH_TMA if i % 2 else PATH_AUTO)
+            go.wait()
+            sv.step(scns[i].dt, 3)
+            out[i] = sv.get_densities()
+    except Exception as e:
+        errs.append(repr(e))
+ts = [threading.Thread(target=work, args=(i,)) for i in range(4)]
+[t.start() for t in ts]
+[t.join() for t in ts]
+assert not errs, errs
+np.savez(sys.argv[2], *out)
+"""
+
+
+def test_host_threads_each_with_a_solver(tmp_path):
+    """Four host threads, each with its own solver, step at the same time
+    from a fresh process (so the library's first-use caches are filled
+    concurrently); every field must match the oracle."""
+    import os
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = tmp_path / "fields.npz"
+    r = subprocess.run([sys.executable, "-c", _THREADS_CHILD, root, str(out)],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    got = np.load(out)
+    for i in range(4):
+        scn = W.mixed_small(shape=(30 + 4 * i, 24, 20), S=2, n_agents=150, seed=200 + i)
+        assert np.all(rel_err(got[f"arr_{i}"], O.oracle_run(scn, 3, 7)) <= TOL64), i

@@ -359,6 +359,7 @@ def run_ours(args, world, rank, local):
                        "l2": "inputs (1.34 GB field) larger than L2; no flush",
                        "parallelism": f"instances x{world}" if world > 1 else "1 GPU"},
             "hbm_gbs_step": BYTES_PER_VS_STEP * N * S / (ms_step / 1e3) / 1e9,
+            "hbm_frac_step": BYTES_PER_VS_STEP * N * S / (ms_step / 1e3) / 1e9 / hbm,
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / hbm,
                          "traffic": traffic,

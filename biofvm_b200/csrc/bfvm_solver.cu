@@ -1228,6 +1228,9 @@ int bfvm_destroy(bfvm_solver* m) {
     m->d_bulk_vox.release();
     m->d_bulk_st.release();
     m->d_bulk_su.release();
+    m->d_bulk_vox32.release();
+    m->d_bulk_row.release();
+    m->d_bulk_tab.release();
     m->seg_bulk.release();
     m->d_dir_vox.release();
     m->d_dir_val.release();

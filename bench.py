@@ -571,10 +571,13 @@ def run_fp32(args, world, rank, local):
 def run_plain50(args, world, rank, local):
     """The small launch-bound workload: 50^3 voxels x 1 substrate, all-boundary
     Dirichlet 1.0, 1000 uptake agents, 100 steps.  Reports microseconds per
-    step for bfvm_step (kernel launches from the host) and for the same steps
-    replayed from a CUDA graph (a one-member bfvm_batch), and the reference
-    on the host cores for the same run."""
+    step for bfvm_step as a user calls it (the field fits one thread-block
+    cluster, so every step runs in one launch), for the sweep kernels launched
+    from the host (cluster steps off) and for the sweep kernels replayed from a
+    CUDA graph (a one-member bfvm_batch), and the reference on the host cores
+    for the same run."""
     import numpy as np
+    import torch
 
     from biofvm_b200 import STEP_ALL, Batch, Solver, load_scenario
     from biofvm_b200 import workloads as W
@@ -584,14 +587,36 @@ def run_plain50(args, world, rank, local):
     load_scenario(sv, scn)
     p0 = scn.initial_field()
     dt = scn.dt
+    stream = torch.cuda.ExternalStream(sv.stream, device=torch.device("cuda", local))
+
+    def timed(fn):
+        """Device time of fn() on the solver's stream (CUDA events), ms."""
+        sv.set_densities(p0)
+        sv.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        sv.synchronize()
+        return e0.elapsed_time(e1)
+
+    # cluster steps (a field this size fits one cluster)
+    sv.set_cluster_steps(True)
+    blocks = sv.get_cluster_steps()
     sv.step(dt, 3, STEP_ALL)
-    sv.set_densities(p0)
-    sv.synchronize()
-    t0 = time.perf_counter()
-    sv.step(dt, args.steps, STEP_ALL)
-    sv.synchronize()
-    t_loop = time.perf_counter() - t0
+    l0 = sv.launch_count
+    with ClockSampler(local) as clocks:
+        ms_cluster = timed(lambda: sv.step(dt, args.steps, STEP_ALL))
+    launches = sv.launch_count - l0
+    cluster_field = sv.get_densities()
+    # the sweep kernels, launched from the host
+    sv.set_cluster_steps(False)
+    sv.step(dt, 3, STEP_ALL)
+    ms_loop = timed(lambda: sv.step(dt, args.steps, STEP_ALL))
     ref = sv.get_densities()
+    # the sweep kernels replayed from a CUDA graph
     bt = Batch(local)
     bt.add(sv)
     sv.set_densities(p0)
@@ -599,13 +624,17 @@ def run_plain50(args, world, rank, local):
     bt.synchronize()
     sv.set_densities(p0)
     sv.synchronize()
-    with ClockSampler(local) as clocks:
-        t0 = time.perf_counter()
-        bt.step(dt, args.steps, STEP_ALL)
-        bt.synchronize()
-        t_graph = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    bt.step(dt, args.steps, STEP_ALL)
+    bt.synchronize()
+    t_graph = time.perf_counter() - t0
     got = sv.get_densities()
-    err = float((np.abs(got - ref).max(axis=0) / np.maximum(np.abs(ref).max(axis=0), 1e-300)).max())
+
+    def rel(a, b):
+        return float((np.abs(a - b).max(axis=0) / np.maximum(np.abs(b).max(axis=0), 1e-300)).max())
+
+    err = rel(got, ref)
+    err_cluster = rel(cluster_field, ref)
     groups, kernels = bt.plan()
     bt.close()
     sv.close()
@@ -625,15 +654,19 @@ def run_plain50(args, world, rank, local):
     if rank == 0:
         vs = scn.num_voxels * scn.S * args.steps
         line = {
-            "metric": METRIC + " (50^3 launch-bound case)", "value": vs * world / t_graph,
+            "metric": METRIC + " (50^3 launch-bound case)", "value": vs * world / (ms_cluster / 1e3),
             "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": 3,
-            "ms_per_step": 1e3 * t_graph / args.steps, "us_per_step": 1e6 * t_graph / args.steps,
+            "ms_per_step": ms_cluster / args.steps, "us_per_step": 1e3 * ms_cluster / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded)",
             "config": {"workload": "plain_50: 50^3 x 1 FP64, all-boundary Dirichlet 1.0, 1000 "
-                                   f"uptake agents, {args.steps} steps"},
-            "host_launched": {"us_per_step": 1e6 * t_loop / args.steps},
-            "graph": {"us_per_step": 1e6 * t_graph / args.steps, "kernels_per_call": kernels},
+                                   f"uptake agents, {args.steps} steps",
+                       "path": f"whole steps in one thread-block cluster of {blocks} blocks"},
+            "gpu_launches": int(launches),
+            "sweep_kernels_host_launched": {"us_per_step": 1e3 * ms_loop / args.steps},
+            "sweep_kernels_graph": {"us_per_step": 1e6 * t_graph / args.steps,
+                                    "kernels_per_call": kernels},
+            "max_rel_err_cluster_vs_sweep_kernels": err_cluster,
             "max_rel_err_graph_vs_host_launched": err,
             "cpu_baseline": cpu,
             "clocks": clocks.summary(),

@@ -16,6 +16,7 @@
 #include "bfvm.h"
 #include "bfvm_host_math.h"
 #include "bfvm_kernels.cuh"
+#include "bfvm_kernels_cluster.cuh"
 #include "bfvm_kernels_tma.cuh"
 #include <cub/device/device_radix_sort.cuh>
 #include <cudaTypedefs.h>
@@ -124,6 +125,10 @@ void thomas_setup(bfvm_solver* m, double dt) {
     m->h_cx[a] = cx;
     m->chunk_ch[a] = 0;
   }
+  m->cl_tab_ok = false;
+  m->setup_dt = dt;
+  m->setup_D = m->D;
+  m->setup_decay = m->decay;
   m->setup_done = true;
 }
 
@@ -1343,6 +1348,7 @@ int bfvm_resize_densities(bfvm_solver* m, int num_densities) {
   return SOLVER_CALL(m, {
     require(num_densities > 0, "need at least one density");
     m->S = num_densities;
+    m->setup_done = false;  // new densities: the next step sets the tables up
     m->D.assign(num_densities, 0.0);
     m->decay.assign(num_densities, 0.0);
     m->d_grad.release();
@@ -1406,6 +1412,27 @@ int bfvm_add_density(bfvm_solver* m, double diffusion_coefficient, double decay_
     }
     m->dir_dirty = m->bulk_dirty = true;
     m->ag_dirty = m->ag_seg_dirty = true;
+    // The reference keeps its Thomas tables after add_density (sized for the
+    // old count; its next solve reads past them).  Here the tables are
+    // rebuilt for S1 densities from the setup's own dt and coefficients, so
+    // the existing densities keep exactly the coefficients they had and the
+    // new one gets its own.
+    if (m->setup_done) {
+      m->setup_D.push_back(diffusion_coefficient);
+      m->setup_decay.push_back(decay_rate);
+      std::vector<double> D = m->setup_D, decay = m->setup_decay;
+      m->D.swap(D);
+      m->decay.swap(decay);
+      try {
+        thomas_setup(m, m->setup_dt);
+      } catch (...) {
+        m->D.swap(D);
+        m->decay.swap(decay);
+        throw;
+      }
+      m->D.swap(D);
+      m->decay.swap(decay);
+    }
   });
 }
 
@@ -1702,6 +1729,103 @@ int bfvm_apply_dirichlet_conditions(bfvm_solver* m) {
   });
 }
 
+namespace bfvm_rt {
+
+constexpr int kClusterMaxN = 64;                  // points per axis (registers per line)
+constexpr size_t kClusterSlabBytes = 200 * 1024;  // shared memory per block
+
+// Blocks of the cluster that holds the whole field (1, 2, 4 or 8), or 0 when
+// bfvm_step cannot run this solver's steps in one cluster.
+int cluster_blocks(const bfvm_solver* m) {
+  if (!m->cluster_steps || m->path != BFVM_PATH_AUTO || m->precision != BFVM_FP64 ||
+      m->lod_dims != 3 || !m->uniform || m->fuse_sources || m->slab_planes > 0)
+    return 0;
+  if (m->nx > kClusterMaxN || m->ny > kClusterMaxN || m->nz > kClusterMaxN) return 0;
+  for (int cl : {1, 2, 4, 8}) {
+    const int64_t pz = (m->nz + cl - 1) / cl;
+    if ((size_t)(pz * m->nx * m->ny * m->S) * sizeof(double) <= kClusterSlabBytes) return cl;
+  }
+  return 0;
+}
+
+// nsteps whole steps (bulk -> cells -> LOD_3D) in one cluster launch.
+void cluster_run(bfvm_solver* m, double dt, int nsteps, int flags, int cl) {
+  if (!m->cl_tab_ok) {
+    const int ns[3] = {m->nx, m->ny, m->nz};
+    for (int a = 0; a < 3; ++a) {
+      const size_t nS = (size_t)ns[a] * m->S;
+      std::vector<double> t(2 * nS + m->S);
+      std::copy(m->h_den[a].begin(), m->h_den[a].end(), t.begin());
+      std::copy(m->h_cx[a].begin(), m->h_cx[a].end(), t.begin() + nS);
+      std::copy(m->h_c1[a].begin(), m->h_c1[a].end(), t.begin() + 2 * nS);
+      upload(m->cl_tab[a], t, m->stream);
+    }
+    m->cl_tab_ok = true;
+  }
+  bfvm::ClusterStepArgs a{};
+  a.p = m->p.as<double>();
+  a.nx = m->nx;
+  a.ny = m->ny;
+  a.nz = m->nz;
+  a.S = m->S;
+  a.pz = (m->nz + cl - 1) / cl;
+  a.nsteps = nsteps;
+  a.dt = dt;
+  a.bulk = (flags & BFVM_STEP_BULK) && !m->bulk_vox.empty();
+  a.cells = (flags & BFVM_STEP_CELLS) && m->n_agents > 0;
+  a.diffusion = true;
+  const int ns[3] = {m->nx, m->ny, m->nz};
+  for (int ax = 0; ax < 3; ++ax) {
+    const double* t = m->cl_tab[ax].as<double>();
+    const size_t nS = (size_t)ns[ax] * m->S;
+    a.den[ax] = t;
+    a.cx[ax] = t + nS;
+    a.c1[ax] = t + 2 * nS;
+  }
+  a.nbulk = (int64_t)m->bulk_vox.size();
+  a.bulk_vox = m->d_bulk_vox.as<int64_t>();
+  a.bulk_st = m->d_bulk_st.as<double>();
+  a.bulk_su = m->d_bulk_su.as<double>();
+  a.nagents = m->n_agents;
+  a.ag_key = m->d_ag_key.as<uint64_t>();
+  a.ag_idx = m->d_ag_idx.as<int>();
+  a.ag_t1 = m->d_ag_t1.as<double>();
+  a.ag_t2 = m->d_ag_t2.as<double>();
+  a.ndir = m->dir_unique;
+  a.dir_vox = m->d_dir_vox.as<int64_t>();
+  a.dir_val = m->d_dir_val.as<double>();
+  const size_t smem = (size_t)a.pz * m->nx * m->ny * m->S * sizeof(double);
+  auto k = bfvm::cluster_steps_kernel<kClusterMaxN>;
+  allow_smem((const void*)k, m->device, smem);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)cl);
+  cfg.blockDim = dim3(256);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = m->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)cl;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  BFVM_CUDA(cudaLaunchKernelEx(&cfg, k, a));
+  check_launch(m);
+}
+
+}  // namespace bfvm_rt
+
+int bfvm_set_cluster_steps(bfvm_solver* m, int enable) {
+  return SOLVER_CALL(m, { m->cluster_steps = enable ? 1 : 0; });
+}
+
+int bfvm_get_cluster_steps(bfvm_solver* m, int* blocks) {
+  return SOLVER_CALL(m, {
+    require(blocks != nullptr, "null output pointer");
+    *blocks = cluster_blocks(m);
+  });
+}
+
 int bfvm_step(bfvm_solver* m, double dt, int nsteps, int flags) {
   return SOLVER_CALL(m, {
     require(nsteps >= 0, "negative step count");
@@ -1714,6 +1838,14 @@ int bfvm_step(bfvm_solver* m, double dt, int nsteps, int flags) {
         if (flags & BFVM_STEP_BULK) bulk_any(m, dt);
         if (flags & BFVM_STEP_CELLS) cells_any(m);
       }
+      return;
+    }
+    const int cl = cluster_blocks(m);
+    if (cl > 0 && nsteps > 0) {
+      check_lod_mesh(m);
+      if (!m->setup_done) thomas_setup(m, dt);
+      build_all(m);
+      cluster_run(m, dt, nsteps, flags, cl);
       return;
     }
     for (int it = 0; it < nsteps; ++it) step_once(m, dt, flags, nullptr);

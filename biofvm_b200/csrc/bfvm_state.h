@@ -150,8 +150,11 @@ struct bfvm_solver {
   int precision = BFVM_FP64;
   bfvm_rt::DevBuf p;
 
-  // Thomas coefficients (computed once, BioFVM_solvers.cpp:87,172)
+  // Thomas coefficients (computed once, BioFVM_solvers.cpp:87,172), with the
+  // dt and coefficients they were computed from
   bool setup_done = false;
+  double setup_dt = 0.0;
+  std::vector<double> setup_D, setup_decay;
   bfvm_rt::DevBuf coef[3];  // per axis: inv_den, fwd, bwd [n*S] then c1 [S], in the sweep precision
   std::vector<double> h_c1[3], h_den[3], h_cx[3];  // FP64 host copies per axis
   bfvm_rt::DevBuf chunk[3];     // per axis: chunk tables k1, kg, kc by slot (sweep precision)
@@ -198,6 +201,12 @@ struct bfvm_solver {
   int fuse_sources = 0;  // bulk/cell updates in the x sweep's prologue
   int lod_dims = 3;      // 2 while a LOD_2D step runs: sweeps of the z = 0 plane only
   int slab_planes = 0;   // x and y sweeps by slabs of this many z planes (0: whole field)
+  // whole steps of a small field in one thread-block cluster (bfvm_step under
+  // BFVM_PATH_AUTO): enabled flag, and the FP64 Thomas tables it reads per
+  // axis (den [n][S], cx [n][S], c1 [S]), rebuilt after each Thomas setup
+  int cluster_steps = 0;
+  bool cl_tab_ok = false;
+  bfvm_rt::DevBuf cl_tab[3];
   // cached tensor maps of the y and z sweeps (keyed by field pointer)
   CUtensorMap maps[3];
   const void* map_key[3] = {nullptr, nullptr, nullptr};

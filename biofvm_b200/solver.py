@@ -245,6 +245,17 @@ class Solver:
         call("bfvm_get_launch_count", self._h, ctypes.byref(n))
         return n.value
 
+    def set_cluster_steps(self, enable: bool) -> None:
+        """Whole steps of a small field in one thread-block cluster (on by
+        default under the AUTO kernel path)."""
+        call("bfvm_set_cluster_steps", self._h, 1 if enable else 0)
+
+    def get_cluster_steps(self) -> int:
+        """Blocks of the cluster that bfvm_step would use now (0: none)."""
+        b = ctypes.c_int()
+        call("bfvm_get_cluster_steps", self._h, ctypes.byref(b))
+        return b.value
+
     def set_slab_planes(self, planes: int) -> None:
         """x and y sweeps by slabs of `planes` z planes (0: whole axes)."""
         call("bfvm_set_slab_planes", self._h, planes)

@@ -82,7 +82,11 @@ BFVM_API int bfvm_get_mesh(bfvm_solver* m, int* nxyz, double* geom, int* flags);
  * S densities, all zero, D = decay = 0. */
 BFVM_API int bfvm_resize_densities(bfvm_solver* m, int num_densities);
 /* Microenvironment::add_density(name, units, D, decay)
- * (BioFVM_microenvironment.cpp:404-441): appends one zero density. */
+ * (BioFVM_microenvironment.cpp:404-441): appends one zero density.  After
+ * the Thomas setup (the first step) the coefficient tables are rebuilt for
+ * the new count from the setup's dt and coefficients: the existing densities
+ * keep theirs, the new one gets its own (the reference keeps tables sized for
+ * the old count there, and its next solve reads past them). */
 BFVM_API int bfvm_add_density(bfvm_solver* m, double diffusion_coefficient, double decay_rate);
 /* Microenvironment::set_density(index, name, units, D, decay)
  * (BioFVM_microenvironment.cpp:450-458) and the public
@@ -252,6 +256,17 @@ BFVM_API int bfvm_get_slab_planes(bfvm_solver* m, int* planes);
  * time.  The device stays usable afterwards. */
 BFVM_API int bfvm_selftest_bounded_wait(int device, int64_t limit_ns, int* gave_up,
                                         double* waited_ms);
+
+/* Whole steps of a small field in one thread-block cluster: under
+ * BFVM_PATH_AUTO, bfvm_step runs all its steps in one launch when the FP64
+ * field fits in the shared memory of a cluster of at most 8 blocks (about
+ * 1.6 MB) and no axis has more than 64 points.  The field stays in shared
+ * memory across the steps; z lines are solved through distributed shared
+ * memory; lines use the reference's own operation sequence (bit-exact).
+ * enable = 1 turns it on (off by default); bfvm_get_cluster_steps gives the
+ * cluster's block count for this solver now (0: not used). */
+BFVM_API int bfvm_set_cluster_steps(bfvm_solver* m, int enable);
+BFVM_API int bfvm_get_cluster_steps(bfvm_solver* m, int* blocks);
 
 /* Times bfvm_step's kernels with CUDA events on the solver's stream, averaged
  * over nsteps steps: ms[4] = source kernels (bulk + cells), x sweep (with its

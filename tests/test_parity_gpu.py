@@ -545,3 +545,83 @@ def test_host_threads_each_with_a_solver(tmp_path):
     for i in range(4):
         scn = W.mixed_small(shape=(30 + 4 * i, 24, 20), S=2, n_agents=150, seed=200 + i)
         assert np.all(rel_err(got[f"arr_{i}"], O.oracle_run(scn, 3, 7)) <= TOL64), i
+
+
+# ---- whole steps of a small field in one thread-block cluster ----
+
+@pytest.mark.parametrize("case", [
+    dict(shape=(50, 50, 50), S=1, n_agents=1000, dirichlet=True, bulk=False),
+    dict(shape=(33, 17, 9), S=4, n_agents=400, dirichlet=True, bulk=True),
+    dict(shape=(40, 40, 40), S=3, n_agents=2000, dirichlet=False, bulk=True),
+    dict(shape=(7, 1, 5), S=2, n_agents=50, dirichlet=True, bulk=True),
+    dict(shape=(64, 3, 64), S=2, n_agents=100, dirichlet=True, bulk=True),
+], ids=["50cube", "odd", "40cube-S3", "thin", "64-lines"])
+def test_cluster_steps_equal_the_reference_bit_for_bit(case):
+    """bfvm_step on a field that fits a cluster runs every step in one
+    launch, with the reference's own operation sequence: the field must equal
+    the oracle's (the reference restated in C) exactly."""
+    scn = W.mixed_small(seed=sum(case["shape"]) + case["S"], **case)
+    with Solver(0) as sv:
+        load_scenario(sv, scn)
+        sv.set_cluster_steps(True)
+        assert sv.get_cluster_steps() > 0
+        sv.step(scn.dt, 4)
+        p = sv.get_densities()
+    assert np.array_equal(p, O.oracle_run(scn, 4, 7))
+
+
+def test_cluster_steps_agree_with_the_sweep_kernels_and_can_be_turned_off():
+    scn = W.plain_50(steps=10)
+    with Solver(0) as sv:
+        load_scenario(sv, scn)
+        sv.set_cluster_steps(True)
+        blocks = sv.get_cluster_steps()
+        assert blocks in (1, 2, 4, 8)
+        sv.step(scn.dt, 10)
+        a = sv.get_densities()
+        sv.set_densities(scn.initial_field())
+        sv.set_cluster_steps(False)
+        assert sv.get_cluster_steps() == 0
+        sv.step(scn.dt, 10)
+        b = sv.get_densities()
+        sv.set_cluster_steps(True)
+        sv.set_kernel_path(PATH_TMA)
+        assert sv.get_cluster_steps() == 0  # only under the AUTO path
+    assert np.all(rel_err(a, b) <= TOL64)
+
+
+def test_cluster_steps_not_used_for_large_fields():
+    with Solver(0) as sv:
+        sv.set_cluster_steps(True)
+        sv.resize_densities(2)
+        sv.resize_space(0, 650, 0, 640, 0, 640, 10)  # 65 points along x
+        assert sv.get_cluster_steps() == 0
+        sv.resize_space(0, 640, 0, 640, 0, 640, 10)  # 64^3 x 2: 4 MB
+        assert sv.get_cluster_steps() == 0
+        sv.resize_space(0, 400, 0, 400, 0, 400, 10)  # 40^3 x 2: 1 MB
+        assert sv.get_cluster_steps() > 0
+
+
+def test_add_density_after_the_setup_matches_a_fresh_solver():
+    """After a step (Thomas setup done), add_density rebuilds the tables for
+    the new count: stepping on equals a solver that had every density from
+    the start (bit for bit, same kernels)."""
+    scn = W.mixed_small(shape=(20, 18, 16), S=2, n_agents=0, seed=46, dirichlet=False,
+                        bulk=False)
+    D3, l3 = 3e4, 0.2
+    with Solver(0) as a, Solver(0) as b:
+        load_scenario(a, scn)
+        a.step(scn.dt, 2)
+        a.add_density(D3, l3)
+        p = a.get_densities()
+        p[:, 2] = np.linspace(0.0, 1.0, p.shape[0])
+        a.set_densities(p)
+        b.resize_densities(3)
+        m = scn.mesh
+        b.resize_space(m.x0, m.x1, m.y0, m.y1, m.z0, m.z1, m.dx, m.dy, m.dz)
+        b.set_coefficients(np.append(scn.D, D3), np.append(scn.decay, l3))
+        b.set_densities(p)
+        for sv in (a, b):
+            sv.set_cluster_steps(False)
+            sv.step(scn.dt, 3)
+        assert np.array_equal(a.get_densities(), b.get_densities())

@@ -51,6 +51,13 @@ struct ClusterStepArgs {
   int64_t ndir;
   const int64_t* dir_vox;
   const double* dir_val;
+  // per block (at most 8): its Dirichlet nodes [dir_lo, dir_hi) and bulk
+  // entries [bulk_lo, bulk_hi) (both lists ascending in voxel); dir_staged:
+  // the block's Dirichlet nodes are copied to its shared memory after the
+  // field (values [n][S], then local voxel indices [n])
+  int dir_lo[8], dir_hi[8];
+  int64_t bulk_lo[8], bulk_hi[8];
+  bool dir_staged;
 };
 
 // One line of n points in this block's shared memory (stride apart),
@@ -125,39 +132,62 @@ __global__ void __launch_bounds__(256, 1) cluster_steps_kernel(const ClusterStep
     const int64_t lv = v - first;
     return (lv >= 0 && lv < (int64_t)nzr * plane) ? lv : -1;
   };
+  // this block's Dirichlet nodes, staged in shared memory when they fit
+  const int d0 = a.dir_lo[rank], nd = a.dir_hi[rank] - d0;
+  double* sdv = slab + (int64_t)a.pz * plane * S;  // [nd][S]
+  int* sdi = reinterpret_cast<int*>(sdv + (a.dir_staged ? (int64_t)nd * S : 0));  // [nd]
+  if (a.dir_staged) {
+    for (int64_t w = tid; w < (int64_t)nd * S; w += nt) sdv[w] = __ldg(a.dir_val + (int64_t)d0 * S + w);
+    for (int e = tid; e < nd; e += nt) sdi[e] = (int)(__ldg(a.dir_vox + d0 + e) - first);
+  }
   auto dirichlet = [&]() {
-    for (int64_t w = tid; w < a.ndir * S; w += nt) {
+    for (int64_t w = tid; w < (int64_t)nd * S; w += nt) {
       const int64_t e = w / S;
       const int s = (int)(w - e * S);
-      const int64_t lv = local(__ldg(a.dir_vox + e));
-      if (lv >= 0) slab[lv * S + s] = __ldg(a.dir_val + w);
+      if (a.dir_staged)
+        slab[(int64_t)sdi[e] * S + s] = sdv[w];
+      else
+        slab[(__ldg(a.dir_vox + d0 + e) - first) * S + s] =
+            __ldg(a.dir_val + (int64_t)(d0 + e) * S + s);
     }
   };
+  // this block's agents: the sorted keys in [first, first + nzr*plane)
+  __shared__ int64_t ag_range[2];
+  if (tid < 2) {
+    const uint64_t want = (uint64_t)(first + (tid ? (int64_t)nzr * plane : 0));
+    int64_t lo = 0, hi = a.nagents;  // first key >= want
+    while (lo < hi) {
+      const int64_t mid = (lo + hi) >> 1;
+      if (__ldg(a.ag_key + mid) < want)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    ag_range[tid] = lo;
+  }
   cluster.sync();
+  const int64_t a0 = ag_range[0], a1 = ag_range[1];
 
   for (int step = 0; step < a.nsteps; ++step) {
     // bulk -> cells (BioFVM_microenvironment.cpp:603-609, BioFVM_basic_agent.cpp:234-235)
     if (a.bulk)
-      for (int64_t w = tid; w < a.nbulk * S; w += nt) {
+      for (int64_t w = a.bulk_lo[rank] * S + tid; w < a.bulk_hi[rank] * S; w += nt) {
         const int64_t e = w / S;
         const int s = (int)(w - e * S);
-        const int64_t lv = local(__ldg(a.bulk_vox + e));
-        if (lv >= 0) {
-          double* q = slab + lv * S + s;
-          *q = bulk_update(*q, __ldg(a.bulk_st + w), __ldg(a.bulk_su + w), a.dt);
-        }
+        double* q = slab + (__ldg(a.bulk_vox + e) - first) * S + s;
+        *q = bulk_update(*q, __ldg(a.bulk_st + w), __ldg(a.bulk_su + w), a.dt);
       }
     __syncthreads();
     if (a.cells)
-      for (int64_t w = tid; w < a.nagents * S; w += nt) {
+      for (int64_t w = a0 * S + tid; w < a1 * S; w += nt) {
         const int64_t r = w / S;
         const int s = (int)(w - r * S);
         const uint64_t v = __ldg(a.ag_key + r);
-        if (r > 0 && __ldg(a.ag_key + r - 1) == v) continue;
+        if (r > a0 && __ldg(a.ag_key + r - 1) == v) continue;
         const int64_t lv = local((int64_t)v);
         if (lv < 0) continue;
         double x = slab[lv * S + s];
-        for (int64_t e = r; e < a.nagents && __ldg(a.ag_key + e) == v; ++e) {
+        for (int64_t e = r; e < a1 && __ldg(a.ag_key + e) == v; ++e) {
           const int64_t ai = __ldg(a.ag_idx + e);
           x = cell_update(x, __ldg(a.ag_t1 + ai * S + s), __ldg(a.ag_t2 + ai * S + s));
         }

@@ -298,6 +298,7 @@ void build_dirichlet(bfvm_solver* m) {
   std::sort(vox.begin(), vox.end());
   const int64_t E = (int64_t)vox.size();
   m->dir_unique = E;
+  m->dir_sorted = vox;
   if (E == 0) {
     m->seg_dir_x.present = m->seg_dir_y.present = false;
     m->dir_dirty = false;
@@ -567,10 +568,14 @@ void allow_smem(const void* kernel, int device, size_t bytes) {
   std::lock_guard<std::mutex> g(mu);
   uint64_t& mask = done[kernel];
   if (mask & (1ull << device)) return;
-  BFVM_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 227 * 1024));
+  // a block may have 227 KB in all: the kernel's static shared memory counts
+  cudaFuncAttributes fa;
+  BFVM_CUDA(cudaFuncGetAttributes(&fa, kernel));
+  const int limit = 227 * 1024 - (int)fa.sharedSizeBytes;
+  require(bytes <= (size_t)limit, "kernel needs more shared memory than a block may have",
+          BFVM_ERR_STATE);
+  BFVM_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, limit));
   mask |= 1ull << device;
-  (void)bytes;
 }
 
 constexpr size_t kSmemBudget = 224 * 1024;  // of the 227 KB a block may use
@@ -1732,7 +1737,8 @@ int bfvm_apply_dirichlet_conditions(bfvm_solver* m) {
 namespace bfvm_rt {
 
 constexpr int kClusterMaxN = 64;                  // points per axis (registers per line)
-constexpr size_t kClusterSlabBytes = 200 * 1024;  // shared memory per block
+constexpr size_t kClusterSlabBytes = 200 * 1024;  // field in shared memory per block
+constexpr size_t kClusterSmemMax = 224 * 1024;    // with the staged Dirichlet nodes
 
 // Blocks of the cluster that holds the whole field (1, 2, 4 or 8), or 0 when
 // bfvm_step cannot run this solver's steps in one cluster.
@@ -1794,7 +1800,26 @@ void cluster_run(bfvm_solver* m, double dt, int nsteps, int flags, int cl) {
   a.ndir = m->dir_unique;
   a.dir_vox = m->d_dir_vox.as<int64_t>();
   a.dir_val = m->d_dir_val.as<double>();
-  const size_t smem = (size_t)a.pz * m->nx * m->ny * m->S * sizeof(double);
+  // each block's Dirichlet nodes and bulk entries (both lists ascending in
+  // voxel) are contiguous: [lo, hi) per block; the Dirichlet nodes are staged
+  // in the block's shared memory for the whole launch when they fit
+  const int64_t plane = (int64_t)m->nx * m->ny;
+  int dir_max = 0;
+  for (int r = 0; r < cl; ++r) {
+    const int64_t v0 = std::min<int64_t>(m->nz, (int64_t)r * a.pz) * plane;
+    const int64_t v1 = std::min<int64_t>(m->nz, (int64_t)(r + 1) * a.pz) * plane;
+    const auto& dv = m->dir_sorted;
+    a.dir_lo[r] = (int)(std::lower_bound(dv.begin(), dv.end(), v0) - dv.begin());
+    a.dir_hi[r] = (int)(std::lower_bound(dv.begin(), dv.end(), v1) - dv.begin());
+    dir_max = std::max(dir_max, a.dir_hi[r] - a.dir_lo[r]);
+    const auto& bv = m->bulk_vox;
+    a.bulk_lo[r] = std::lower_bound(bv.begin(), bv.end(), v0) - bv.begin();
+    a.bulk_hi[r] = std::lower_bound(bv.begin(), bv.end(), v1) - bv.begin();
+  }
+  const size_t slab_bytes = (size_t)a.pz * m->nx * m->ny * m->S * sizeof(double);
+  const size_t dir_bytes = (size_t)dir_max * (m->S * sizeof(double) + sizeof(int));
+  a.dir_staged = slab_bytes + dir_bytes <= kClusterSmemMax;
+  const size_t smem = slab_bytes + (a.dir_staged ? dir_bytes : 0) + 16;
   auto k = bfvm::cluster_steps_kernel<kClusterMaxN>;
   allow_smem((const void*)k, m->device, smem);
   cudaLaunchConfig_t cfg = {};

@@ -180,6 +180,7 @@ struct bfvm_solver {
   std::vector<double> dir_val;
   bool dir_dirty = true;
   int64_t dir_unique = 0;
+  std::vector<int64_t> dir_sorted;  // the unique nodes as uploaded (ascending)
   bfvm_rt::DevBuf d_dir_vox, d_dir_val;
   bfvm_rt::DevSegList seg_dir_x, seg_dir_y;
 

@@ -263,8 +263,10 @@ BFVM_API int bfvm_selftest_bounded_wait(int device, int64_t limit_ns, int* gave_
  * 1.6 MB) and no axis has more than 64 points.  The field stays in shared
  * memory across the steps; z lines are solved through distributed shared
  * memory; lines use the reference's own operation sequence (bit-exact).
- * enable = 1 turns it on (off by default); bfvm_get_cluster_steps gives the
- * cluster's block count for this solver now (0: not used). */
+ * enable = 1 turns it on (off by default: it is a bit-exact mode, slower
+ * than the sweep kernels -- 103 vs 25 us per step at 50^3 on a B200);
+ * bfvm_get_cluster_steps gives the cluster's block count for this solver
+ * now (0: not used). */
 BFVM_API int bfvm_set_cluster_steps(bfvm_solver* m, int enable);
 BFVM_API int bfvm_get_cluster_steps(bfvm_solver* m, int* blocks);
 

@@ -675,6 +675,63 @@ def run_plain50(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_gradients(args, world, rank, local):
+    """Microenvironment::compute_all_gradient_vectors on the device field
+    (BioFVM_microenvironment.cpp:702-787) at 256^3 voxels x 10 substrates FP64:
+    central differences along each axis into [N][S][3] FP64.  Algorithmic
+    bytes: the field read once (8 B/VS) and three gradients written (24 B/VS);
+    timed with CUDA events on the solver's stream over the calls."""
+    import numpy as np
+    import torch
+
+    from biofvm_b200 import Solver
+
+    n = args.size if "--size" in sys.argv else 256
+    S = args.substrates if "--substrates" in sys.argv else 10
+    sv = Solver(local)
+    sv.resize_densities(S)
+    sv.resize_space(0, n * 10.0, 0, n * 10.0, 0, n * 10.0, 10.0)
+    rng = np.random.default_rng(12350)
+    sv.set_densities(rng.random((n ** 3, S)))
+    stream = torch.cuda.ExternalStream(sv.stream, device=torch.device("cuda", local))
+    for _ in range(max(3, args.warmup)):
+        sv.compute_all_gradient_vectors()
+    sv.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    l0 = sv.launch_count
+    with ClockSampler(local) as clocks:
+        barrier(world)
+        e0.record(stream)
+        for _ in range(args.steps):
+            sv.compute_all_gradient_vectors()
+        e1.record(stream)
+        e1.synchronize()
+    launches = sv.launch_count - l0
+    ms = max_over_ranks(e0.elapsed_time(e1), world) / args.steps
+    sv.close()
+    if rank == 0:
+        hbm, peak_kind = peaks()
+        vs = n ** 3 * S
+        achieved = 32.0 * vs / (ms / 1e3) / 1e9
+        line = {
+            "metric": "voxel-substrate gradients/s (compute_all_gradient_vectors)",
+            "value": vs * world / (ms / 1e3), "unit": "voxel-substrate gradients/s",
+            "n_gpus": world, "steps": args.steps, "warmup": max(3, args.warmup),
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": f"gradients: {n}^3 voxels x {S} substrates FP64",
+                       "l2": "field and gradients larger than L2; no flush"},
+            "roofline": {"bound": "hbm", "kernel": "gradient_rows_kernel", "achieved": achieved,
+                         "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": None,
+                         "algorithmic_bytes_per_launch": 32 * vs},
+            "gpu_launches": int(launches),
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+
+
 def run_adjoint(args, world, rank, local):
     """The adjoint workload: 128^3 voxels x 4 substrates FP64, 20k agents,
     200 steps with checkpoints every 20.  Loss = 1/2 |p_T - target|^2, the
@@ -771,12 +828,14 @@ def main():
     ap.add_argument("--size", type=int, default=256, help="cube edge in voxels (default 256)")
     ap.add_argument("--substrates", type=int, default=10)
     ap.add_argument("--agents", type=int, default=100_000)
-    ap.add_argument("--workload", choices=["lod256", "plain50", "batched", "fp32", "adjoint"],
+    ap.add_argument("--workload",
+                    choices=["lod256", "plain50", "batched", "fp32", "adjoint", "gradients"],
                     default="lod256",
                     help="lod256: the headline line (default); batched: 64 independent "
                          "instances vs looped plain solves; fp32: FP32 sweeps at 512^3 x 8 "
                          "with 1M agents against FP64; adjoint: gradients at 128^3 x 4, 200 "
-                         "steps; plain50: the 50^3 launch-bound case, host-launched vs graph")
+                         "steps; plain50: the 50^3 launch-bound case, host-launched vs graph; "
+                         "gradients: compute_all_gradient_vectors at 256^3 x 10")
     ap.add_argument("--instances", type=int, default=64)
     args = ap.parse_args()
     if args.workload == "batched" and "--steps" not in sys.argv:
@@ -798,6 +857,8 @@ def main():
             run_fp32(args, world, rank, local)
         elif args.workload == "adjoint":
             run_adjoint(args, world, rank, local)
+        elif args.workload == "gradients":
+            run_gradients(args, world, rank, local)
         elif args.workload == "plain50":
             run_plain50(args, world, rank, local)
         else:

@@ -392,6 +392,43 @@ __global__ void gradient_kernel(const T* __restrict__ p, int nx, int ny, int nz,
     out[2] = __ddiv_rn(__dsub_rn((double)p[t + jz], (double)p[t - jz]), two_dz);
 }
 
+// The same central differences with the grid laid over the mesh: block
+// (bx, j, k) covers 256 consecutive (i, s) elements of row (j, k), so a thread
+// finds its point with one 32-bit division by S instead of 64-bit divisions
+// of a flat index (rows: gridDim.y = ny, gridDim.z = nz).
+// The block's 256 x 3 results are staged in shared memory and written back
+// as contiguous runs (components at an axis end keep their old value, read
+// back only there).  Blocks of 256 threads.
+template <typename T>
+__global__ void __launch_bounds__(256) gradient_rows_kernel(
+    const T* __restrict__ p, int nx, int ny, int nz, int S, double two_dx, double two_dy,
+    double two_dz, double* __restrict__ g) {
+  __shared__ double buf[3 * 256];
+  const int e0 = blockIdx.x * 256;
+  const int e = e0 + threadIdx.x;  // (i, s) within the row
+  const int count = min(256, nx * S - e0);
+  const int j = blockIdx.y, k = blockIdx.z;
+  const int64_t row0 = ((int64_t)k * ny + j) * nx * S;  // first element of the row
+  if (threadIdx.x < count) {
+    const int i = e / S;
+    const int64_t t = row0 + e;
+    const int64_t jx = S, jy = (int64_t)nx * S, jz = (int64_t)nx * ny * S;
+    double* b = buf + 3 * threadIdx.x;
+    b[0] = (i > 0 && i < nx - 1)
+               ? __ddiv_rn(__dsub_rn((double)p[t + jx], (double)p[t - jx]), two_dx)
+               : g[3 * t];
+    b[1] = (j > 0 && j < ny - 1)
+               ? __ddiv_rn(__dsub_rn((double)p[t + jy], (double)p[t - jy]), two_dy)
+               : g[3 * t + 1];
+    b[2] = (k > 0 && k < nz - 1)
+               ? __ddiv_rn(__dsub_rn((double)p[t + jz], (double)p[t - jz]), two_dz)
+               : g[3 * t + 2];
+  }
+  __syncthreads();
+  double* out = g + 3 * (row0 + e0);
+  for (int c = threadIdx.x; c < 3 * count; c += 256) out[c] = buf[c];
+}
+
 template <typename Dst, typename Src>
 __global__ void convert_kernel(Dst* __restrict__ dst, const Src* __restrict__ src, int64_t count) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;

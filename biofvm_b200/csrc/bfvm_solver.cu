@@ -1890,14 +1890,19 @@ int bfvm_compute_all_gradient_vectors(bfvm_solver* m) {
     // the reference divides by 2*dx, 2*dy, 2*dz (:704-713)
     const double two_dx = m->dx * 2.0, two_dy = m->dy * 2.0, two_dz = m->dz * 2.0;
     const int64_t work = m->NS();
-    if (m->precision == BFVM_FP64)
-      bfvm::gradient_kernel<double><<<(unsigned)blocks_for(work, 256), 256, 0, m->stream>>>(
-          m->p.as<double>(), m->nx, m->ny, m->nz, m->S, two_dx, two_dy, two_dz,
-          m->d_grad.as<double>());
-    else
-      bfvm::gradient_kernel<float><<<(unsigned)blocks_for(work, 256), 256, 0, m->stream>>>(
-          m->p.as<float>(), m->nx, m->ny, m->nz, m->S, two_dx, two_dy, two_dz,
-          m->d_grad.as<double>());
+    const bool rows = m->ny <= 65535 && m->nz <= 65535 && (int64_t)m->nx * m->S < (1 << 30);
+    const dim3 rgrid((unsigned)blocks_for((int64_t)m->nx * m->S, 256), m->ny, m->nz);
+    with_types(m, [&](auto t, auto) {
+      using T = decltype(t);
+      if (rows)
+        bfvm::gradient_rows_kernel<T><<<rgrid, 256, 0, m->stream>>>(
+            m->p.as<T>(), m->nx, m->ny, m->nz, m->S, two_dx, two_dy, two_dz,
+            m->d_grad.as<double>());
+      else
+        bfvm::gradient_kernel<T><<<(unsigned)blocks_for(work, 256), 256, 0, m->stream>>>(
+            m->p.as<T>(), m->nx, m->ny, m->nz, m->S, two_dx, two_dy, two_dz,
+            m->d_grad.as<double>());
+    });
     check_launch(m);
   });
 }

@@ -675,6 +675,74 @@ def run_plain50(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_lod2d(args, world, rank, local):
+    """diffusion_decay_solver__constant_coefficients_LOD_2D
+    (BioFVM_solvers.cpp:278-427) on a 1024 x 1024 x 32 FP64 plane (268 MB,
+    larger than L2; lines are at most 1024 points) (dx = 10,
+    D log-uniform in [1e3, 1e5], decay uniform in [0.01, 1], dt = 0.01):
+    the x and y sweeps of the plane with the Dirichlet overwrites fused.
+    Algorithmic bytes 32 B/VS per step (two sweeps, one read and one write of
+    the field each); CUDA events on the solver's stream."""
+    import numpy as np
+    import torch
+
+    from biofvm_b200 import Solver
+
+    n = args.size if "--size" in sys.argv else 1024
+    S = args.substrates if "--substrates" in sys.argv else 32
+    rng = np.random.default_rng(12351)
+    sv = Solver(local)
+    sv.resize_densities(S)
+    sv.resize_space(0, n * 10.0, 0, n * 10.0, -5.0, 5.0, 10.0)
+    sv.set_coefficients(np.exp(rng.uniform(np.log(1e3), np.log(1e5), S)),
+                        rng.uniform(0.01, 1.0, S))
+    sv.set_densities(rng.random((n * n, S)))
+    stream = torch.cuda.ExternalStream(sv.stream, device=torch.device("cuda", local))
+    dt = 0.01
+    for _ in range(max(3, args.warmup)):
+        sv.simulate_diffusion_decay_2d(dt)
+    # the sweep kernels timed on this plane (after the first step fixed the
+    # LOD_2D Thomas coefficients; the field is restored)
+    tuned = sv.tune_sweeps(dt, 3) if not args.no_tune else []
+    sv.set_slab_planes(0)
+    sv.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    l0 = sv.launch_count
+    with ClockSampler(local) as clocks:
+        barrier(world)
+        e0.record(stream)
+        for _ in range(args.steps):
+            sv.simulate_diffusion_decay_2d(dt)
+        e1.record(stream)
+        e1.synchronize()
+    launches = sv.launch_count - l0
+    ms = max_over_ranks(e0.elapsed_time(e1), world) / args.steps
+    sv.close()
+    if rank == 0:
+        hbm, peak_kind = peaks()
+        vs = n * n * S
+        achieved = 32.0 * vs / (ms / 1e3) / 1e9
+        line = {
+            "metric": METRIC + " (LOD_2D)", "value": vs * world / (ms / 1e3), "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": max(3, args.warmup),
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": f"lod2d: {n}^2 voxels x {S} substrates FP64",
+                       "l2": "field larger than L2; no flush"},
+            "tuned_sweeps": [{"axis": "xy"[i], "kernel": ["default", "register", "tma",
+                                                          "direct"][k],
+                              "chunk": ch, "columns": tw} for i, (k, ch, tw, _) in
+                             enumerate(tuned[:2])],
+            "roofline": {"bound": "hbm", "kernel": "x and y sweeps of the plane",
+                         "achieved": achieved, "peak": hbm, "peak_kind": peak_kind,
+                         "unit": "GB/s", "frac": achieved / hbm, "traffic": None},
+            "gpu_launches": int(launches),
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+
+
 def run_gradients(args, world, rank, local):
     """Microenvironment::compute_all_gradient_vectors on the device field
     (BioFVM_microenvironment.cpp:702-787) at 256^3 voxels x 10 substrates FP64:
@@ -829,13 +897,15 @@ def main():
     ap.add_argument("--substrates", type=int, default=10)
     ap.add_argument("--agents", type=int, default=100_000)
     ap.add_argument("--workload",
-                    choices=["lod256", "plain50", "batched", "fp32", "adjoint", "gradients"],
+                    choices=["lod256", "plain50", "batched", "fp32", "adjoint", "gradients",
+                             "lod2d"],
                     default="lod256",
                     help="lod256: the headline line (default); batched: 64 independent "
                          "instances vs looped plain solves; fp32: FP32 sweeps at 512^3 x 8 "
                          "with 1M agents against FP64; adjoint: gradients at 128^3 x 4, 200 "
                          "steps; plain50: the 50^3 launch-bound case, host-launched vs graph; "
-                         "gradients: compute_all_gradient_vectors at 256^3 x 10")
+                         "gradients: compute_all_gradient_vectors at 256^3 x 10; lod2d: the "
+                         "LOD_2D solver on a 1024^2 x 32 plane")
     ap.add_argument("--instances", type=int, default=64)
     args = ap.parse_args()
     if args.workload == "batched" and "--steps" not in sys.argv:
@@ -857,6 +927,8 @@ def main():
             run_fp32(args, world, rank, local)
         elif args.workload == "adjoint":
             run_adjoint(args, world, rank, local)
+        elif args.workload == "lod2d":
+            run_lod2d(args, world, rank, local)
         elif args.workload == "gradients":
             run_gradients(args, world, rank, local)
         elif args.workload == "plain50":

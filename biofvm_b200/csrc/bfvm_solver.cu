@@ -526,9 +526,15 @@ void launch_sweep(bfvm_solver* m, int ax, int fuse, double dt, int64_t z0 = 0, i
     a.col0 = z0 * per_plane;
     a.ncols = z1 * per_plane;
   }
-  dim3 block(A.tw, a.nchunks);
-  dim3 grid((unsigned)blocks_for(a.ncols - a.col0, A.tw));
-  const size_t smem = 4 * sizeof(CT) * (size_t)A.tw * a.nchunks;
+  // columns per block: the axis's choice, narrowed to the block size the
+  // kernel is compiled for (a fallback from another kernel may bring a wider one)
+  int tw = A.tw;
+  while (tw > 1 && tw * a.nchunks > bfvm::sweep_max_threads(A.ch)) tw /= 2;
+  require(tw * a.nchunks <= bfvm::sweep_max_threads(A.ch), "line too long for the sweep kernel",
+          BFVM_ERR_STATE);
+  dim3 block(tw, a.nchunks);
+  dim3 grid((unsigned)blocks_for(a.ncols - a.col0, tw));
+  const size_t smem = 4 * sizeof(CT) * (size_t)tw * a.nchunks;
   int mode = bfvm::kSweepPlain;
   if (fuse & (bfvm::kFuseBulk | bfvm::kFuseCells | bfvm::kFuseDirPro))
     mode = bfvm::kSweepFull;
@@ -601,8 +607,9 @@ struct LinesPlan {
 };
 
 // y (ax = 1) or z (ax = 2) sweep as a 3-D tensor [outer][n][C].  Tiles are
-// 16 columns wide in FP64 and 32 in FP32 (128-byte rows); the ring gets as
-// many stages as keep two blocks per SM, else one block with more stages.
+// 16 columns wide in FP64 and 32 in FP32 (128-byte rows), half that for lines
+// of 17-32 chunks; the ring gets as many stages as keep two blocks per SM,
+// else one block with more stages.
 LinesPlan plan_lines(const bfvm_solver* m, int ax) {
   LinesPlan L;
   const int64_t es = (int64_t)m->elem();
@@ -618,7 +625,8 @@ LinesPlan plan_lines(const bfvm_solver* m, int ax) {
   L.ch = m->axis[ax].ch;
   L.nc = (L.n + L.ch - 1) / L.ch;
   L.w = (m->math_elem() == 8) ? 16 : 32;
-  if (L.nc > 16) return L;
+  if (L.nc > 32 || (L.nc > 16 && L.ch < 32)) return L;
+  if (L.nc > 16) L.w /= 2;  // 513-1024 points: half-width tiles, 32 chunks
   L.box_n = std::min(L.n, 256);
   L.nboxes = (L.n + L.box_n - 1) / L.box_n;
   const int64_t ctiles = (L.C + L.w - 1) / L.w;
@@ -724,10 +732,11 @@ RowsPlan plan_rows(const bfvm_solver* m) {
   return P;
 }
 
-template <typename T, typename CT, int CH, int ST, bool DIR, bool TAB, int MAXNC>
+template <typename T, typename CT, int CH, int ST, bool DIR, bool TAB, int MAXNC, int W>
 void launch_lines_nc(const CUtensorMap& map, const bfvm::LinesArgs<T, CT>& a, int ntiles,
                      dim3 block, size_t smem, bfvm_solver* m) {
-  constexpr int W = sizeof(CT) == 8 ? 16 : 32;
+  require((int)block.x == W && (int)block.y <= MAXNC, "line kernel launch shape",
+          BFVM_ERR_STATE);
   auto k = bfvm::lod_lines_tma_kernel<T, CH, W, ST, DIR, TAB, MAXNC, CT>;
   allow_smem((const void*)k, m->device, smem);
   int per_sm = 0;
@@ -738,17 +747,24 @@ void launch_lines_nc(const CUtensorMap& map, const bfvm::LinesArgs<T, CT>& a, in
 }
 
 // Lines of up to 8 chunks of 32 points take the kernel compiled for 8 chunks
-// (more registers per thread); longer lines the one for 16.
+// (more registers per thread); up to 16 chunks the one for 16; lines of 17 to
+// 32 chunks of 32 points (513-1024 points) the one for 32 chunks with tiles of
+// half the width (the same threads per block and registers per thread).
 template <typename T, typename CT, int CH, int ST, bool DIR, bool TAB>
 void launch_lines_inst(const CUtensorMap& map, const bfvm::LinesArgs<T, CT>& a, int ntiles,
                        dim3 block, size_t smem, bfvm_solver* m) {
+  constexpr int WF = sizeof(CT) == 8 ? 16 : 32;  // 128-byte tile rows
   if constexpr (CH >= 32) {
+    if (block.y > 16) {
+      launch_lines_nc<T, CT, CH, ST, DIR, TAB, 32, WF / 2>(map, a, ntiles, block, smem, m);
+      return;
+    }
     if (block.y <= 8) {
-      launch_lines_nc<T, CT, CH, ST, DIR, TAB, 8>(map, a, ntiles, block, smem, m);
+      launch_lines_nc<T, CT, CH, ST, DIR, TAB, 8, WF>(map, a, ntiles, block, smem, m);
       return;
     }
   }
-  launch_lines_nc<T, CT, CH, ST, DIR, TAB, 16>(map, a, ntiles, block, smem, m);
+  launch_lines_nc<T, CT, CH, ST, DIR, TAB, 16, WF>(map, a, ntiles, block, smem, m);
 }
 
 template <typename T, typename CT, int CH, int ST, bool TAB>
@@ -2076,10 +2092,9 @@ void tune_sweeps(bfvm_solver* m, double dt, int reps) {
         if (nc > 64) continue;
         for (int tw : {32, 16, 8})
           if (nc * tw <= bfvm::sweep_max_threads(ch)) cand.push_back({BFVM_PATH_GENERIC, ch, tw});
-        if (nc <= 16) {
-          cand.push_back({BFVM_PATH_TMA, ch, 16});
-          cand.push_back({BFVM_PATH_DIRECT, ch, 16});
-        }
+        // the line kernel (y, z) also takes 17-32 chunks of 32 points
+        if (nc <= 16 || (ax > 0 && ch == 32 && nc <= 32)) cand.push_back({BFVM_PATH_TMA, ch, 16});
+        if (nc <= 16) cand.push_back({BFVM_PATH_DIRECT, ch, 16});
       }
       Axis best = m->axis[ax];
       float best_ms = 1e30f;

@@ -67,6 +67,15 @@ void copy_field(bfvm_solver* m, void* dst, const void* src) {
   BFVM_CUDA(cudaMemcpyAsync(dst, src, field_bytes(m), cudaMemcpyDeviceToDevice, m->stream));
 }
 
+// Sweeps write to another field while it is alive (out-of-place solves).
+struct OutSwap {
+  bfvm_solver* m;
+  OutSwap(bfvm_solver* mm, void* out) : m(mm) { m->sweep_out = out; }
+  ~OutSwap() { m->sweep_out = nullptr; }
+  OutSwap(const OutSwap&) = delete;
+  OutSwap& operator=(const OutSwap&) = delete;
+};
+
 // One forward step on the current field with every solve output kept:
 // x, y, z receive the field after the x, y and z solves.
 void step_keeping_solves(bfvm_solver* m, double dt, int flags, const void* in, unsigned char* x,
@@ -82,6 +91,19 @@ void step_keeping_solves(bfvm_solver* m, double dt, int flags, const void* in, u
     }
     dirichlet_standalone<double>(m);
     sweep(m, 0, 0, dt);
+  }
+  if (m->dir_unique == 0) {
+    // no Dirichlet node to overwrite between the solves: the y and z solves
+    // read the previous solve's output and write the next slot (no copies)
+    {
+      FieldSwap f(m, x);
+      OutSwap o(m, y);
+      sweep(m, 1, 0, dt);
+    }
+    FieldSwap f(m, y);
+    OutSwap o(m, z);
+    sweep(m, 2, 0, dt);
+    return;
   }
   copy_field(m, y, x);
   {

@@ -67,6 +67,7 @@ struct SegList {
 template <typename T, typename CT = T>
 struct SweepArgs {
   T* p;
+  T* out;                // where the solved lines go (p: in place)
   int64_t col0;          // first column of this launch (a slab of planes)
   int64_t ncols;         // end of the launch's columns (all (line, substrate) columns)
   int64_t C;             // columns per outer block
@@ -259,9 +260,10 @@ __global__ void __launch_bounds__(sweep_max_threads(CH), MINB)
   if (MODE != kSweepPlain && active && (a.fuse & kFuseDirEpi))
     apply_dirichlet_seg<CT, CH>(v, a.dir_epi, seg, k0, S, s);
 
+  T* dst = a.out + (ptr - a.p);
 #pragma unroll
   for (int m = 0; m < CH; ++m)
-    if (m < len) ptr[m * ls] = (T)v[m];
+    if (m < len) dst[m * ls] = (T)v[m];
 }
 
 // ---------------------------------------------------------------------------

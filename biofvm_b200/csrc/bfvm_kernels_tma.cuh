@@ -116,6 +116,7 @@ __device__ __forceinline__ size_t chunk_row(const ChunkCoef<T>& cc, int c, int s
 template <typename T, typename CT = T>
 struct LinesArgs {
   T* p;
+  T* out;          // where the solved lines go (p: in place; the map reads p)
   int64_t C;       // contiguous columns per outer block (< 2^31)
   int n;           // points per line
   int64_t ls;      // element stride between points
@@ -135,6 +136,7 @@ struct LinesArgs {
 template <typename T, typename CT = T>
 struct RowsArgs {
   T* p;
+  T* out;  // where the solved rows go (p: in place)
   int64_t rows;  // ny * nz
   int n;         // nx
   int S;
@@ -342,7 +344,7 @@ __global__ void __launch_bounds__(W * MAXNC)
       const int64_t seg = (vcol / S) * a.nchunks + c;
       apply_dirichlet_seg<CT, CH>(v, a.dir_epi, seg, k0, S, s);
     }
-    T* ptr = a.p + (int64_t)outer * a.os + col + (int64_t)k0 * a.ls;
+    T* ptr = a.out + (int64_t)outer * a.os + col + (int64_t)k0 * a.ls;
 #pragma unroll
     for (int m = 0; m < CH; ++m) {
       if (m < lenA) *ptr = (T)v[m];
@@ -491,7 +493,7 @@ __global__ void __launch_bounds__(MAXT, rows_min_blocks(CH, MAXT))
     if (a.fuse & kFuseDirEpi) apply_dirichlet_seg<CT, CH>(v, a.dir, seg, k0, S, s);
     // straight to global memory: the lanes of a warp write the S densities of
     // consecutive rows at one point
-    T* out = a.p + row * (int64_t)row_elems + (int64_t)k0 * S + s;
+    T* out = a.out + row * (int64_t)row_elems + (int64_t)k0 * S + s;
 #pragma unroll
     for (int m = 0; m < CH; ++m)
       if (m < lenA) out[(int64_t)m * S] = (T)v[m];
@@ -512,6 +514,7 @@ __global__ void __launch_bounds__(MAXT, rows_min_blocks(CH, MAXT))
 template <typename T, typename CT = T>
 struct DirectArgs {
   T* p;
+  T* out;                // where the solved lines go (p: in place)
   int64_t col0;          // first column of this launch (a slab of planes)
   int64_t ncols;         // end of the launch's (line, density) columns
   int64_t C;             // columns per outer block
@@ -614,10 +617,11 @@ __global__ void __launch_bounds__(512) lod_sweep_direct_kernel(const DirectArgs<
   chunk_fix<false, CT, CH>(v, lenA, a.cc.kg + row, S, cf, cb);
   if (MODE != kSweepPlain && (a.fuse & kFuseDirEpi))
     apply_dirichlet_seg<CT, CH>(v, a.dir_epi, seg, k0, S, s);
+  T* dst = a.out + (ptr - a.p);
 #pragma unroll
   for (int m = 0; m < CH; ++m) {
-    if (m < lenA) *ptr = (T)v[m];
-    ptr += ls;
+    if (m < lenA) *dst = (T)v[m];
+    dst += ls;
   }
 }
 

@@ -487,6 +487,7 @@ void launch_sweep(bfvm_solver* m, int ax, int fuse, double dt, int64_t z0 = 0, i
   const int64_t nx = m->nx, ny = m->ny, nz = m->nz;
   bfvm::SweepArgs<T, CT> a{};
   a.p = m->p.as<T>();
+  a.out = m->sweep_out ? static_cast<T*>(m->sweep_out) : a.p;
   a.S = S;
   a.dt = dt;
   a.coef = coef_view<CT>(m, ax);
@@ -817,6 +818,7 @@ void launch_lines(bfvm_solver* m, int ax, const LinesPlan& L, bool dir, int64_t 
   }
   bfvm::LinesArgs<T, CT> a{};
   a.p = m->p.as<T>();
+  a.out = m->sweep_out ? static_cast<T*>(m->sweep_out) : a.p;
   a.C = L.C;
   a.n = L.n;
   a.ls = L.ls;
@@ -892,6 +894,7 @@ bool launch_direct(bfvm_solver* m, int ax, int fuse, double dt, int64_t z0 = 0,
   const int64_t nblocks = (a.ncols - a.col0 + W - 1) / W;
   if (W * nc > 512 || nblocks >= ((int64_t)1 << 31)) return false;
   a.p = m->p.as<T>();
+  a.out = m->sweep_out ? static_cast<T*>(m->sweep_out) : a.p;
   a.S = (int)S;
   a.nchunks = nc;
   a.cc = chunk_view<CT>(m, ax);
@@ -952,6 +955,7 @@ void launch_rows(bfvm_solver* m, const RowsPlan& P, int fuse, double dt, int64_t
                  int64_t z1 = -1) {
   bfvm::RowsArgs<T, CT> a{};
   a.p = m->p.as<T>();
+  a.out = m->sweep_out ? static_cast<T*>(m->sweep_out) : a.p;
   a.rows = (int64_t)m->ny * (m->lod_dims == 2 ? 1 : m->nz);
   a.n = m->nx;
   a.S = m->S;

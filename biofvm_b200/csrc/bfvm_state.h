@@ -202,6 +202,7 @@ struct bfvm_solver {
   int fuse_sources = 0;  // bulk/cell updates in the x sweep's prologue
   int lod_dims = 3;      // 2 while a LOD_2D step runs: sweeps of the z = 0 plane only
   int slab_planes = 0;   // x and y sweeps by slabs of this many z planes (0: whole field)
+  void* sweep_out = nullptr;  // sweeps write here instead of in place (the adjoint's recompute)
   // whole steps of a small field in one thread-block cluster (bfvm_step under
   // BFVM_PATH_AUTO): enabled flag, and the FP64 Thomas tables it reads per
   // axis (den [n][S], cx [n][S], c1 [S]), rebuilt after each Thomas setup

@@ -356,7 +356,9 @@ def run_ours(args, world, rank, local):
             "config": {"workload": f"{scn.name}: {args.size}^3 voxels x {S} substrates FP64, "
                                    f"{scn.num_agents} agents, bulk sphere r=500um, dt=0.01",
                        "voxels": N, "substrates": S, "agents": scn.num_agents,
-                       "l2": "inputs (1.34 GB field) larger than L2; no flush",
+                       "l2": (f"inputs ({N * S * 8 / 1e9:.2f} GB field) larger than L2; no flush"
+                              if N * S * 8 > 126e6 else
+                              f"field ({N * S * 8 / 1e6:.0f} MB) fits in L2; no flush"),
                        "parallelism": f"instances x{world}" if world > 1 else "1 GPU"},
             "hbm_gbs_step": BYTES_PER_VS_STEP * N * S / (ms_step / 1e3) / 1e9,
             "hbm_frac_step": BYTES_PER_VS_STEP * N * S / (ms_step / 1e3) / 1e9 / hbm,

@@ -40,8 +40,11 @@ std::vector<int> segment_offsets(int64_t nlines, int nchunks, int ch,
 
 // Chunk length CH (points per thread) and block width TW (columns per block)
 // per axis; a block is TW x NC threads with NC = ceil(n/CH) <= 512/TW.  The y
-// and z sweeps of long lines take CH = 32 (fewer chunks to join per line), x
-// keeps CH = 16 for its register kernel.
+// and z sweeps of long lines take CH = 32 (fewer chunks to join per line).
+// x takes the row kernel with CH = 32 where it was measured faster than the
+// register kernel (S >= 4 densities and rows of >= 96 points: 0.85 -> 0.75 ms
+// at 256^3 x 10 FP64, 4.4 -> 2.7 ms at 384^3 x 10, 0.66 -> 0.43 ms at
+// 256^3 x 10 FP32), else the register kernel with CH = 8 or 16.
 void choose_axes(bfvm_solver* m) {
   const int ns[3] = {m->nx, m->ny, m->nz};
   for (int a = 0; a < 3; ++a) {
@@ -64,6 +67,14 @@ void choose_axes(bfvm_solver* m) {
             "axis with " + std::to_string(n) + " points exceeds the 1024-point line limit");
     m->axis[a].ch = ch;
     m->axis[a].tw = tw;
+    if (a == 0 && m->S >= 4 && n >= 96 && (int64_t)m->S * ((n + 31) / 32) <= 256 &&
+        ((int64_t)n * m->S * m->elem()) % 16 == 0) {
+      m->axis[a].ch = 32;
+      m->axis[a].kind = BFVM_PATH_TMA;
+      tw = 32;
+      while (tw > 8 && (n + 31) / 32 * tw > bfvm::sweep_max_threads(32)) tw /= 2;
+      m->axis[a].tw = tw;
+    }
   }
 }
 
@@ -706,12 +717,16 @@ RowsPlan plan_rows(const bfvm_solver* m) {
   P.pitch = pitch;
   const size_t extra = 8 * 4 + 16 + 128;
   const size_t tab = table_bytes(m, 0);
-  // Two blocks per SM of at most 256 threads (room for each thread's chunk
-  // in registers), a 2-stage ring of R rows, the chunk tables in shared
-  // memory when they fit; else one block of up to 512 threads.
+  // Blocks of at most 256 threads (room for each thread's chunk in
+  // registers), a 2-stage ring of R rows, the chunk tables in shared memory
+  // when they fit; else one block of up to 512 threads.  Half the shared
+  // memory per block where the kernel is compiled for two blocks per SM
+  // (chunks of up to 16 points), all of it where one block fills the
+  // register file (32-point chunks).
   for (int maxt : {256, 512}) {
     if (cols > maxt) continue;
-    const size_t budget = (maxt == 256) ? 113 * 1024 : kSmemBudget;
+    const size_t budget =
+        bfvm::rows_min_blocks(P.ch, maxt) == 2 ? 113 * 1024 : kSmemBudget;
     for (int staged = 1; staged >= 0; --staged) {
       if (staged && tab == 0) continue;
       for (int R = (int)std::min<int64_t>(maxt / cols, rows); R >= 1; --R) {
@@ -1390,6 +1405,7 @@ int bfvm_resize_densities(bfvm_solver* m, int num_densities) {
     m->bulk_dirty = true;
     m->n_agents = 0;
     m->ag_dirty = m->ag_seg_dirty = true;
+    choose_axes(m);  // the x kernel depends on the number of densities
   });
 }
 
@@ -1437,6 +1453,7 @@ int bfvm_add_density(bfvm_solver* m, double diffusion_coefficient, double decay_
     }
     m->dir_dirty = m->bulk_dirty = true;
     m->ag_dirty = m->ag_seg_dirty = true;
+    choose_axes(m);  // the x kernel depends on the number of densities
     // The reference keeps its Thomas tables after add_density (sized for the
     // old count; its next solve reads past them).  Here the tables are
     // rebuilt for S1 densities from the setup's own dt and coefficients, so

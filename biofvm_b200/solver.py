@@ -211,6 +211,13 @@ class Solver:
             out.append((k.value, cfg[0], cfg[1], cfg[2]))
         return out
 
+    def get_sweep_kernel(self, axis: int) -> int:
+        """The kernel `axis` sweeps with under PATH_AUTO: 0 for the default
+        (the register kernel), else a PATH_* value."""
+        k = ctypes.c_int()
+        call("bfvm_get_sweep_kernel", self._h, axis, ctypes.byref(k))
+        return k.value
+
     def set_sweep_config(self, axis: int, chunk: int, columns: int, min_blocks: int = 1) -> None:
         call("bfvm_set_sweep_config", self._h, axis, chunk, columns, min_blocks)
 

@@ -245,6 +245,49 @@ def test_longest_lines(shape):
         assert np.all(rel_err(p, ref) <= TOL64), path
 
 
+@pytest.mark.parametrize("shape,S,kind", [((96, 20, 12), 4, PATH_TMA), ((160, 12, 10), 5, PATH_TMA),
+                                          ((96, 20, 12), 1, 0), ((64, 20, 12), 6, 0)],
+                         ids=["rows96x4", "rows160x5", "register_S1", "register_n64"])
+def test_default_x_kernel(shape, S, kind):
+    """Untuned, x sweeps with the row kernel at 32-point chunks when there are
+    at least 4 densities and rows of at least 96 points, else with the
+    register kernel; either way the step matches the oracle, fused and per
+    call."""
+    scn = W.mixed_small(shape=shape, S=S, n_agents=300, seed=sum(shape) + S)
+    ref = O.oracle_run(scn, 3, 7)
+    with Solver(0) as sv:
+        load_scenario(sv, scn)
+        assert sv.get_sweep_kernel(0) == kind
+        if kind:
+            assert sv.get_sweep_config(0)[0] == 32
+    for fused in (True, False):
+        p = run_gpu(scn, 3, 7, fused=fused)
+        assert np.all(rel_err(p, ref) <= TOL64), fused
+
+
+def test_default_x_kernel_follows_added_densities():
+    """Densities added after the mesh (the usual driver order) move x to the
+    row kernel once there are 4; the step still matches the oracle."""
+    scn = W.mixed_small(shape=(128, 10, 8), S=4, n_agents=100, seed=5, dirichlet=False,
+                        bulk=False)
+    ref = O.oracle_run(scn, 2, 7)
+    m = scn.mesh
+    with Solver(0) as sv:
+        sv.resize_densities(1)
+        sv.resize_space(m.x0, m.x1, m.y0, m.y1, m.z0, m.z1, m.dx, m.dy, m.dz)
+        assert sv.get_sweep_kernel(0) == 0
+        for _ in range(3):
+            sv.add_density(0.0, 0.0)
+        assert sv.get_sweep_kernel(0) == PATH_TMA
+        sv.set_coefficients(scn.D, scn.decay)
+        sv.set_densities(scn.p0)
+        v, t1, t2 = scn.agent_arrays()
+        sv.set_agents(v, t1, t2)
+        sv.step(scn.dt, 2, 7)
+        p = sv.get_densities()
+    assert np.all(rel_err(p, ref) <= TOL64)
+
+
 def test_lines_past_the_limit_are_rejected():
     with Solver(0) as sv:
         sv.resize_densities(1)

@@ -573,11 +573,11 @@ def run_fp32(args, world, rank, local):
 def run_plain50(args, world, rank, local):
     """The small launch-bound workload: 50^3 voxels x 1 substrate, all-boundary
     Dirichlet 1.0, 1000 uptake agents, 100 steps.  Reports microseconds per
-    step for bfvm_step as a user calls it (the field fits one thread-block
-    cluster, so every step runs in one launch), for the sweep kernels launched
-    from the host (cluster steps off) and for the sweep kernels replayed from a
-    CUDA graph (a one-member bfvm_batch), and the reference on the host cores
-    for the same run."""
+    step for bfvm_step as a user calls it (the sweep kernels, launched from
+    the host), for the sweep kernels replayed from a CUDA graph (a one-member
+    bfvm_batch), for the opt-in modes that run all steps in one launch (grid
+    steps: a cooperative launch; cluster steps: one thread-block cluster,
+    bit-exact), and the reference on the host cores for the same run."""
     import numpy as np
     import torch
 
@@ -611,6 +611,15 @@ def run_plain50(args, world, rank, local):
         ms_loop = timed(lambda: sv.step(dt, args.steps, STEP_ALL))
     launches = sv.launch_count - l0
     ref = sv.get_densities()
+    # the same steps in one cooperative launch (opt-in)
+    sv.set_grid_steps(True)
+    grid_blocks = sv.get_grid_steps()
+    sv.step(dt, 3, STEP_ALL)
+    l0 = sv.launch_count
+    ms_grid = timed(lambda: sv.step(dt, args.steps, STEP_ALL))
+    grid_launches = sv.launch_count - l0
+    grid_field = sv.get_densities()
+    sv.set_grid_steps(False)
     # the same steps in one thread-block cluster (opt-in; bit-exact)
     sv.set_cluster_steps(True)
     blocks = sv.get_cluster_steps()
@@ -637,6 +646,7 @@ def run_plain50(args, world, rank, local):
 
     err = rel(got, ref)
     err_cluster = rel(cluster_field, ref)
+    err_grid = rel(grid_field, ref)
     groups, kernels = bt.plan()
     bt.close()
     sv.close()
@@ -665,10 +675,13 @@ def run_plain50(args, world, rank, local):
                                    f"uptake agents, {args.steps} steps",
                        "path": "sweep kernels launched from the host (bfvm_step default)"},
             "gpu_launches": int(launches),
+            "grid_steps_opt_in": {"us_per_step": 1e3 * ms_grid / args.steps,
+                                  "blocks": grid_blocks, "launches": int(grid_launches)},
             "sweep_kernels_graph": {"us_per_step": 1e6 * t_graph / args.steps,
                                     "kernels_per_call": kernels},
             "cluster_steps_bit_exact": {"us_per_step": 1e3 * ms_cluster / args.steps,
                                         "blocks": blocks},
+            "max_rel_err_grid_steps_vs_sweep_kernels": err_grid,
             "max_rel_err_cluster_vs_sweep_kernels": err_cluster,
             "max_rel_err_graph_vs_host_launched": err,
             "cpu_baseline": cpu,

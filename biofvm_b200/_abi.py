@@ -93,6 +93,8 @@ SIGNATURES = {
     "bfvm_selftest_bounded_wait": (c_int, [c_int, c_int64, _IP, _DP]),
     "bfvm_set_cluster_steps": (c_int, [_P, c_int]),
     "bfvm_get_cluster_steps": (c_int, [_P, _IP]),
+    "bfvm_set_grid_steps": (c_int, [_P, c_int]),
+    "bfvm_get_grid_steps": (c_int, [_P, _IP]),
     "bfvm_profile_step": (c_int, [_P, c_double, c_int, c_int, _DP]),
     "bfvm_tune_sweeps": (c_int, [_P, c_double, c_int]),
     "bfvm_get_sweep_kernel": (c_int, [_P, c_int, _IP]),

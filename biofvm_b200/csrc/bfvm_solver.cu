@@ -17,6 +17,7 @@
 #include "bfvm_host_math.h"
 #include "bfvm_kernels.cuh"
 #include "bfvm_kernels_cluster.cuh"
+#include "bfvm_kernels_grid.cuh"
 #include "bfvm_kernels_tma.cuh"
 #include <cub/device/device_radix_sort.cuh>
 #include <cudaTypedefs.h>
@@ -137,6 +138,7 @@ void thomas_setup(bfvm_solver* m, double dt) {
     m->chunk_ch[a] = 0;
   }
   m->cl_tab_ok = false;
+  m->gr_tab_ok = false;
   m->setup_dt = dt;
   m->setup_D = m->D;
   m->setup_decay = m->decay;
@@ -1295,6 +1297,9 @@ int bfvm_destroy(bfvm_solver* m) {
     adjoint_release(m);
     for (auto& c : m->chunk) c.release();
     for (auto& c : m->chunk_slots) c.release();
+    for (auto& c : m->cl_tab) c.release();
+    for (auto& c : m->gr_tab) c.release();
+    m->d_grid_maps.release();
     cudaStreamDestroy(m->stream);
     delete m;
   });
@@ -1875,7 +1880,130 @@ void cluster_run(bfvm_solver* m, double dt, int nsteps, int flags, int cl) {
   check_launch(m);
 }
 
+constexpr int kGridMaxN = 64;              // points per axis (registers per line)
+constexpr int64_t kGridMaxVS = 1 << 20;    // voxel-densities: past this the sweep kernels win
+constexpr int kGridThreads = 128;
+constexpr size_t kGridSmem = (size_t)kGridThreads * kGridMaxN * sizeof(double);  // a column each
+
+// Blocks of the cooperative launch that runs this solver's steps in one
+// launch, or 0 when bfvm_step uses the sweep kernels (or the cluster).
+int grid_blocks(bfvm_solver* m) {
+  if (!m->grid_steps || m->path != BFVM_PATH_AUTO || m->precision != BFVM_FP64 ||
+      m->lod_dims != 3 || !m->uniform || m->fuse_sources || m->slab_planes > 0)
+    return 0;
+  if (m->nx > kGridMaxN || m->ny > kGridMaxN || m->nz > kGridMaxN) return 0;
+  if ((int64_t)m->NS() > kGridMaxVS || cluster_blocks(m) > 0) return 0;
+  if (m->grid_per_sm == 0) {
+    int coop = 0;
+    BFVM_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, m->device));
+    int per_sm = 0;
+    if (coop) {
+      allow_smem((const void*)bfvm::grid_steps_kernel, m->device, kGridSmem);
+      BFVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &per_sm, bfvm::grid_steps_kernel, kGridThreads, kGridSmem));
+    }
+    m->grid_per_sm = per_sm > 0 ? per_sm : -1;
+  }
+  if (m->grid_per_sm < 0) return 0;
+  const int64_t N = (int64_t)m->nx * m->ny * m->nz;
+  const int64_t items =
+      std::max({N / m->nx, N / m->ny, N / m->nz}) * m->S;  // (line, density) per phase
+  return (int)std::min<int64_t>((items + kGridThreads - 1) / kGridThreads,
+                                (int64_t)m->grid_per_sm * m->num_sms);
+}
+
+// nsteps whole steps (bulk -> cells -> LOD_3D) in one cooperative launch.
+void grid_run(bfvm_solver* m, double dt, int nsteps, int flags, int blocks) {
+  const int S = m->S;
+  if (!m->gr_tab_ok) {
+    const int ns[3] = {m->nx, m->ny, m->nz};
+    for (int a = 0; a < 3; ++a) {
+      const size_t nS = (size_t)ns[a] * S;
+      std::vector<double> t(2 * nS + S);
+      for (size_t i = 0; i < nS; ++i) t[i] = 1.0 / m->h_den[a][i];
+      std::copy(m->h_cx[a].begin(), m->h_cx[a].end(), t.begin() + nS);
+      std::copy(m->h_c1[a].begin(), m->h_c1[a].end(), t.begin() + 2 * nS);
+      upload(m->gr_tab[a], t, m->stream);
+    }
+    m->gr_tab_ok = true;
+  }
+  // scratch: Dirichlet values [N][S] (doubles first), line masks of the x, y
+  // and z lines, bulk and agent maps [N] each
+  const int64_t N = m->N();
+  const int64_t lx = N / m->nx, ly = N / m->ny, lz = N / m->nz;
+  const size_t field_b = (size_t)N * S * sizeof(double);
+  const size_t masks_b = (size_t)(lx + ly + lz) * sizeof(uint64_t);
+  m->d_grid_maps.ensure(field_b + masks_b + (size_t)2 * N * sizeof(int));
+  unsigned char* base = m->d_grid_maps.as<unsigned char>();
+  double* dir_field = reinterpret_cast<double*>(base);
+  unsigned long long* mx = reinterpret_cast<unsigned long long*>(base + field_b);
+  unsigned long long* my = mx + lx;
+  unsigned long long* mz = my + ly;
+  int* maps = reinterpret_cast<int*>(base + field_b + masks_b);
+  BFVM_CUDA(cudaMemsetAsync(mx, 0, masks_b, m->stream));
+  BFVM_CUDA(cudaMemsetAsync(maps, 0xFF, (size_t)2 * N * sizeof(int), m->stream));
+  const int64_t nbulk = (int64_t)m->bulk_vox.size();
+  const int64_t most = std::max({nbulk, m->n_agents, m->dir_unique});
+  if (most > 0) {
+    bfvm::grid_maps_kernel<<<(unsigned)blocks_for(most, 256), 256, 0, m->stream>>>(
+        maps, maps + N, nbulk, m->d_bulk_vox.as<int64_t>(), m->n_agents,
+        m->d_ag_key.as<uint64_t>(), m->dir_unique, m->d_dir_vox.as<int64_t>(),
+        m->d_dir_val.as<double>(), mx, my, mz, dir_field, m->nx, m->ny, S);
+    check_launch(m);
+  }
+  bfvm::GridStepArgs a{};
+  a.p = m->p.as<double>();
+  a.nx = m->nx;
+  a.ny = m->ny;
+  a.nz = m->nz;
+  a.S = S;
+  a.nsteps = nsteps;
+  a.dt = dt;
+  a.bulk = (flags & BFVM_STEP_BULK) && nbulk > 0;
+  a.cells = (flags & BFVM_STEP_CELLS) && m->n_agents > 0;
+  const int ns[3] = {m->nx, m->ny, m->nz};
+  for (int ax = 0; ax < 3; ++ax) {
+    const double* t = m->gr_tab[ax].as<double>();
+    const size_t nS = (size_t)ns[ax] * S;
+    a.rd[ax] = t;
+    a.cx[ax] = t + nS;
+    a.c1[ax] = t + 2 * nS;
+  }
+  a.bulk_map = maps;
+  a.ag_map = maps + N;
+  a.dirichlet = m->dir_unique > 0;
+  a.dir_mask[0] = mx;
+  a.dir_mask[1] = my;
+  a.dir_mask[2] = mz;
+  a.dir_field = dir_field;
+  a.nbulk = nbulk;
+  a.bulk_vox = m->d_bulk_vox.as<int64_t>();
+  a.bulk_st = m->d_bulk_st.as<double>();
+  a.bulk_su = m->d_bulk_su.as<double>();
+  a.nagents = m->n_agents;
+  a.ag_key = m->d_ag_key.as<uint64_t>();
+  a.ag_idx = m->d_ag_idx.as<int>();
+  a.ag_t1 = m->d_ag_t1.as<double>();
+  a.ag_t2 = m->d_ag_t2.as<double>();
+  void* params[] = {&a};
+  BFVM_CUDA(cudaLaunchCooperativeKernel((const void*)bfvm::grid_steps_kernel,
+                                        dim3((unsigned)blocks), dim3(kGridThreads), params,
+                                        kGridSmem, m->stream));
+  check_launch(m);
+}
+
 }  // namespace bfvm_rt
+
+int bfvm_set_grid_steps(bfvm_solver* m, int enable) {
+  return SOLVER_CALL(m, { m->grid_steps = enable ? 1 : 0; });
+}
+
+int bfvm_get_grid_steps(bfvm_solver* m, int* blocks) {
+  return SOLVER_CALL(m, {
+    require(blocks != nullptr, "null output pointer");
+    *blocks = grid_blocks(m);
+  });
+}
 
 int bfvm_set_cluster_steps(bfvm_solver* m, int enable) {
   return SOLVER_CALL(m, { m->cluster_steps = enable ? 1 : 0; });
@@ -1908,6 +2036,14 @@ int bfvm_step(bfvm_solver* m, double dt, int nsteps, int flags) {
       if (!m->setup_done) thomas_setup(m, dt);
       build_all(m);
       cluster_run(m, dt, nsteps, flags, cl);
+      return;
+    }
+    const int gb = nsteps > 0 ? grid_blocks(m) : 0;
+    if (gb > 0) {
+      check_lod_mesh(m);
+      if (!m->setup_done) thomas_setup(m, dt);
+      build_all(m);
+      grid_run(m, dt, nsteps, flags, gb);
       return;
     }
     for (int it = 0; it < nsteps; ++it) step_once(m, dt, flags, nullptr);

@@ -252,6 +252,18 @@ class Solver:
         call("bfvm_get_launch_count", self._h, ctypes.byref(n))
         return n.value
 
+    def set_grid_steps(self, enable: bool) -> None:
+        """Whole steps of a small FP64 field (<= 2^20 voxel-densities, <= 64
+        points per axis) in one cooperative launch under PATH_AUTO (off by
+        default: slower than the sweep kernels at 50^3)."""
+        call("bfvm_set_grid_steps", self._h, 1 if enable else 0)
+
+    def get_grid_steps(self) -> int:
+        """Blocks of the cooperative launch bfvm_step would use now (0: none)."""
+        b = ctypes.c_int()
+        call("bfvm_get_grid_steps", self._h, ctypes.byref(b))
+        return b.value
+
     def set_cluster_steps(self, enable: bool) -> None:
         """Whole steps of a small field in one thread-block cluster (on by
         default under the AUTO kernel path)."""

@@ -270,6 +270,22 @@ BFVM_API int bfvm_selftest_bounded_wait(int device, int64_t limit_ns, int* gave_
 BFVM_API int bfvm_set_cluster_steps(bfvm_solver* m, int enable);
 BFVM_API int bfvm_get_cluster_steps(bfvm_solver* m, int* blocks);
 
+/* Whole steps of a small field in one cooperative launch over all SMs: under
+ * BFVM_PATH_AUTO, bfvm_step runs all its steps in one launch when the FP64
+ * field has at most 2^20 voxel-densities and no axis has more than 64
+ * points (and the cluster mode above is not in use).  Each step is three
+ * phases of whole lines solved in registers (x with the bulk, cell and
+ * Dirichlet updates applied as the lines are loaded, then y, then z, each
+ * with the Dirichlet values) separated by grid-wide barriers; the lines
+ * multiply by precomputed reciprocals of the Thomas denominators (within
+ * 1e-15 of the reference's divisions).  Off by default: one thread per
+ * line leaves too little parallelism (59 vs 25 us per step at 50^3 x 1 on a
+ * B200, of which 5.6 us are the four grid barriers).  enable = 1 turns it
+ * on; bfvm_get_grid_steps gives the launch's block count for this solver
+ * now (0: not used). */
+BFVM_API int bfvm_set_grid_steps(bfvm_solver* m, int enable);
+BFVM_API int bfvm_get_grid_steps(bfvm_solver* m, int* blocks);
+
 /* Times bfvm_step's kernels with CUDA events on the solver's stream, averaged
  * over nsteps steps: ms[4] = source kernels (bulk + cells), x sweep (with its
  * Dirichlet prologue/epilogue), y sweep, z sweep.  With slabs

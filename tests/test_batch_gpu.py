@@ -179,6 +179,7 @@ def plain_solves(scns, steps, flags=STEP_ALL):
     for scn in scns:
         with Solver(0) as sv:
             load_scenario(sv, scn)
+            sv.set_grid_steps(False)  # the sweep kernels, as the batch's branches
             sv.step(scn.dt, steps, flags)
             out.append(sv.get_densities())
     return out
@@ -230,6 +231,8 @@ def test_branches_see_member_changes_between_calls():
     r1, r2 = Solver(0), Solver(0)
     load_scenario(r1, a)
     load_scenario(r2, c)
+    for sv in (r1, r2):
+        sv.set_grid_steps(False)  # the sweep kernels, as the batch's branches
     with Batch(0) as bt:
         bt.set_mode(BATCH_BRANCHES)
         bt.add(s1)

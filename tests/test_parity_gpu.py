@@ -466,6 +466,7 @@ def _run_slabs(scn, steps, planes, path=PATH_AUTO, flags=7, precision=64):
             sv.set_precision(precision)
         sv.set_slab_planes(planes)
         assert sv.get_slab_planes() == planes
+        sv.set_grid_steps(False)  # whole-axis runs use the sweep kernels too
         sv.step(scn.dt, steps, flags)
         return sv.get_densities()
 
@@ -643,6 +644,107 @@ def test_cluster_steps_not_used_for_large_fields():
         assert sv.get_cluster_steps() == 0
         sv.resize_space(0, 400, 0, 400, 0, 400, 10)  # 40^3 x 2: 1 MB
         assert sv.get_cluster_steps() > 0
+
+
+GRID_CASES = [
+    dict(shape=(50, 50, 50), S=1, n_agents=1000, dirichlet=True, bulk=True),
+    dict(shape=(23, 17, 31), S=3, n_agents=400, dirichlet=True, bulk=True),
+    dict(shape=(40, 40, 40), S=5, n_agents=2000, dirichlet=True, bulk=True),
+    dict(shape=(64, 3, 64), S=2, n_agents=100, dirichlet=True, bulk=True),
+    dict(shape=(1, 64, 2), S=4, n_agents=50, dirichlet=False, bulk=True),
+]
+GRID_IDS = ["50cube", "odd", "40cube-S5", "thin", "one-point-x"]
+
+
+@pytest.mark.parametrize("case", GRID_CASES, ids=GRID_IDS)
+def test_grid_steps_match_the_oracle_and_the_sweep_kernels(case):
+    """With grid steps on, bfvm_step on a small FP64 field runs every step in
+    one cooperative launch (a thread per line, Dirichlet values applied as
+    lines load, sources in a phase of their own):
+    within 1e-12 of the oracle and of the sweep kernels, agents sharing
+    voxels included."""
+    scn = W.mixed_small(seed=sum(case["shape"]) + 3 * case["S"], **case)
+    ref = O.oracle_run(scn, 4, 7)
+    with Solver(0) as sv:
+        load_scenario(sv, scn)
+        assert sv.get_grid_steps() == 0  # opt-in
+        sv.set_grid_steps(True)
+        assert sv.get_grid_steps() > 0
+        sv.step(scn.dt, 4)
+        a = sv.get_densities()
+        sv.set_densities(scn.initial_field())
+        sv.set_grid_steps(False)
+        assert sv.get_grid_steps() == 0
+        sv.step(scn.dt, 4)
+        b = sv.get_densities()
+    assert np.all(rel_err(a, ref) <= TOL64)
+    assert np.all(rel_err(a, b) <= TOL64)
+
+
+@pytest.mark.parametrize("flags", [STEP_DIFFUSION, STEP_BULK | STEP_DIFFUSION,
+                                   STEP_CELLS | STEP_DIFFUSION],
+                         ids=["diffusion", "bulk+diffusion", "cells+diffusion"])
+def test_grid_steps_with_some_parts_of_the_step(flags):
+    scn = W.mixed_small(shape=(30, 20, 10), S=2, n_agents=300, seed=91)
+    ref = O.oracle_run(scn, 3, flags)
+    with Solver(0) as sv:
+        load_scenario(sv, scn)
+        sv.set_grid_steps(True)
+        assert sv.get_grid_steps() > 0
+        sv.step(scn.dt, 3, flags)
+        p = sv.get_densities()
+    assert np.all(rel_err(p, ref) <= TOL64)
+
+
+def test_grid_steps_follow_changes_between_calls():
+    """Agents, bulk rates and Dirichlet nodes changed between bfvm_step calls
+    are seen by the next cooperative launch (its voxel maps are rebuilt per
+    call)."""
+    scn = W.mixed_small(shape=(24, 20, 16), S=2, n_agents=200, seed=92)
+    scn2 = W.mixed_small(shape=(24, 20, 16), S=2, n_agents=300, seed=93)
+    with Solver(0) as sv:
+        load_scenario(sv, scn)
+        sv.set_grid_steps(True)
+        assert sv.get_grid_steps() > 0
+        sv.step(scn.dt, 2)
+        mid = sv.get_densities()
+        v, t1, t2 = scn2.agent_arrays()
+        sv.set_agents(v, t1, t2)
+        sv.set_bulk_rates_sparse(scn2.bulk_voxels, scn2.bulk_supply, scn2.bulk_target,
+                                 scn2.bulk_uptake)
+        sv.step(scn.dt, 2)
+        p = sv.get_densities()
+    scn2.p0 = mid
+    scn2.dirichlet_voxels, scn2.dirichlet_values = scn.dirichlet_voxels, scn.dirichlet_values
+    scn2.D, scn2.decay = scn.D, scn.decay
+    assert np.all(rel_err(p, O.oracle_run(scn2, 2, 7)) <= TOL64)
+
+
+def test_grid_steps_eligibility():
+    with Solver(0) as sv:
+        sv.resize_densities(1)
+        sv.resize_space(0, 500, 0, 500, 0, 500, 10)  # 50^3 x 1 (fits a cluster)
+        assert sv.get_grid_steps() == 0  # opt-in
+        sv.set_grid_steps(True)
+        assert sv.get_grid_steps() > 0
+        sv.set_cluster_steps(True)  # the bit-exact cluster mode comes first
+        assert sv.get_cluster_steps() > 0 and sv.get_grid_steps() == 0
+        sv.set_cluster_steps(False)
+        sv.resize_densities(2)
+        sv.set_kernel_path(PATH_TMA)  # only under the AUTO path
+        assert sv.get_grid_steps() == 0
+        sv.set_kernel_path(PATH_AUTO)
+        sv.set_precision(32)  # FP64 only
+        assert sv.get_grid_steps() == 0
+        sv.set_precision(64)
+        sv.resize_space(0, 650, 0, 640, 0, 640, 10)  # 65 points along x
+        assert sv.get_grid_steps() == 0
+        sv.resize_densities(5)
+        sv.resize_space(0, 640, 0, 640, 0, 640, 10)  # 64^3 x 5 > 2^20
+        assert sv.get_grid_steps() == 0
+        sv.resize_densities(4)
+        sv.resize_space(0, 640, 0, 640, 0, 640, 10)  # 64^3 x 4 = 2^20
+        assert sv.get_grid_steps() > 0
 
 
 def test_add_density_after_the_setup_matches_a_fresh_solver():

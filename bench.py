@@ -573,11 +573,11 @@ def run_fp32(args, world, rank, local):
 def run_plain50(args, world, rank, local):
     """The small launch-bound workload: 50^3 voxels x 1 substrate, all-boundary
     Dirichlet 1.0, 1000 uptake agents, 100 steps.  Reports microseconds per
-    step for bfvm_step as a user calls it (the sweep kernels, launched from
-    the host), for the sweep kernels replayed from a CUDA graph (a one-member
-    bfvm_batch), for the opt-in modes that run all steps in one launch (grid
-    steps: a cooperative launch; cluster steps: one thread-block cluster,
-    bit-exact), and the reference on the host cores for the same run."""
+    step for bfvm_step as a user calls it (a field this small runs all its
+    steps in one cooperative launch: grid steps), for the sweep kernels
+    launched from the host (grid steps off) and replayed from a CUDA graph (a
+    one-member bfvm_batch), for the opt-in bit-exact thread-block-cluster
+    mode, and the reference on the host cores for the same run."""
     import numpy as np
     import torch
 
@@ -604,22 +604,21 @@ def run_plain50(args, world, rank, local):
         sv.synchronize()
         return e0.elapsed_time(e1)
 
-    # bfvm_step as it runs by default: the sweep kernels, launched from the host
+    # bfvm_step as it runs by default: every step in one cooperative launch
+    grid_blocks = sv.get_grid_steps()
     sv.step(dt, 3, STEP_ALL)
     l0 = sv.launch_count
     with ClockSampler(local) as clocks:
         ms_loop = timed(lambda: sv.step(dt, args.steps, STEP_ALL))
     launches = sv.launch_count - l0
-    ref = sv.get_densities()
-    # the same steps in one cooperative launch (opt-in)
-    sv.set_grid_steps(True)
-    grid_blocks = sv.get_grid_steps()
+    grid_field = sv.get_densities()
+    # the sweep kernels, launched from the host (seven kernels per step)
+    sv.set_grid_steps(False)
     sv.step(dt, 3, STEP_ALL)
     l0 = sv.launch_count
-    ms_grid = timed(lambda: sv.step(dt, args.steps, STEP_ALL))
-    grid_launches = sv.launch_count - l0
-    grid_field = sv.get_densities()
-    sv.set_grid_steps(False)
+    ms_sweep = timed(lambda: sv.step(dt, args.steps, STEP_ALL))
+    sweep_launches = sv.launch_count - l0
+    ref = sv.get_densities()
     # the same steps in one thread-block cluster (opt-in; bit-exact)
     sv.set_cluster_steps(True)
     blocks = sv.get_cluster_steps()
@@ -673,10 +672,11 @@ def run_plain50(args, world, rank, local):
             "data": "synthetic (seeded)",
             "config": {"workload": "plain_50: 50^3 x 1 FP64, all-boundary Dirichlet 1.0, 1000 "
                                    f"uptake agents, {args.steps} steps",
-                       "path": "sweep kernels launched from the host (bfvm_step default)"},
+                       "path": "bfvm_step default: all steps in one cooperative launch "
+                               f"of {grid_blocks} blocks (grid steps)"},
             "gpu_launches": int(launches),
-            "grid_steps_opt_in": {"us_per_step": 1e3 * ms_grid / args.steps,
-                                  "blocks": grid_blocks, "launches": int(grid_launches)},
+            "sweep_kernels_host_launched": {"us_per_step": 1e3 * ms_sweep / args.steps,
+                                            "launches": int(sweep_launches)},
             "sweep_kernels_graph": {"us_per_step": 1e6 * t_graph / args.steps,
                                     "kernels_per_call": kernels},
             "cluster_steps_bit_exact": {"us_per_step": 1e3 * ms_cluster / args.steps,

@@ -9,18 +9,17 @@
 //            and then its voxel's agents in list order
 //            (BioFVM_basic_agent.cpp:234-235); per agent voxel without a bulk
 //            entry its agents;
-//   x, y, z: each thread solves whole (line, density) items in its own
-//            column of shared memory (points blockDim.x elements apart, so
-//            the threads of a warp hit different banks); as a line is loaded, its Dirichlet nodes take their
-//            values (BioFVM_microenvironment.cpp:192-197, before each axis:
-//            BioFVM_solvers.cpp:177, 207, 241): a 64-bit mask per line marks
-//            the nodes, whose values sit in a field-shaped array.
-// Offsets are 32-bit: the path is for fields of at most 2^20 elements.
+//   x, y, z: tiles of TW lines x NC chunks of 8 points per block (as the
+//            register sweep kernel: chunk-local passes, the chunks' carries
+//            folded through shared memory, fix-ups); as a chunk is loaded, its
+//            Dirichlet nodes take their values (BioFVM_microenvironment.cpp:
+//            192-197, before each axis: BioFVM_solvers.cpp:177, 207, 241): a
+//            64-bit mask per line marks the nodes, whose values sit in a
+//            field-shaped array.
 // Every voxel lies on exactly one line per axis, so this equals the
-// reference's whole-field passes.  Lines are solved with the reference's
-// recurrence (BioFVM_solvers.cpp:186-200) using precomputed reciprocals of
-// the denominators (a multiply instead of a divide), within 1e-15 of the
-// divided form.
+// reference's whole-field passes.  Lines are solved with the sweep kernels'
+// per-point tables (1/denominator, forward and backward slopes), within
+// 1e-12 of the reference's divisions.
 #pragma once
 
 #include <cooperative_groups.h>
@@ -35,10 +34,8 @@ struct GridStepArgs {
   int nsteps;
   double dt;
   bool bulk, cells;
-  // per axis: 1/denominator [n][S], cx [n][S], c1 [S]
-  const double* rd[3];
-  const double* cx[3];
-  const double* c1[3];
+  // per axis: the sweep kernels' per-point tables [n][S] and c1 [S]
+  AxisCoef<double> coef[3];
   // per voxel: its bulk entry and its first agent in the sorted list, or -1
   const int* bulk_map;
   const int* ag_map;
@@ -100,68 +97,126 @@ __device__ __forceinline__ void grid_sources(const GridStepArgs& a, int64_t firs
   }
 }
 
-// The lines of one axis: each thread takes (line, density) items.
+constexpr int kGridChunk = 8;  // points per thread: lines of <= 64 points in <= 8 chunks
+
+// The lines of one axis in tiles of TW columns x NC chunks (TW = blockDim.x /
+// NC); columns are (line, density) pairs numbered as in lod_sweep_kernel.
+// sm holds 4 * blockDim.x values for the chunks' forward and backward carries.
 template <int AX>
-__device__ __forceinline__ void grid_axis(const GridStepArgs& a, double* col, int first,
-                                          int stride) {
+__device__ __forceinline__ void grid_axis(const GridStepArgs& a, double* sm) {
+  constexpr int CH = kGridChunk;
   const int S = a.S;
-  const int T = blockDim.x;  // shared-memory elements between a column's points
-  const int plane = a.nx * a.ny;
+  const int64_t plane = (int64_t)a.nx * a.ny;
   const int n = AX == 0 ? a.nx : (AX == 1 ? a.ny : a.nz);
-  const int st = (AX == 0 ? 1 : (AX == 1 ? a.nx : plane)) * S;  // field elements between points
-  const int items = plane * a.nz / n * S;
-  const double* __restrict__ rd = a.rd[AX];
-  const double* __restrict__ cx = a.cx[AX];
-  for (int l = first; l < items; l += stride) {
-    const int s = l % S;
-    const int line = l / S;
-    int base;  // voxel of point 0
-    if (AX == 0)
-      base = line * a.nx;
-    else if (AX == 1)
-      base = (line / a.nx) * plane + line % a.nx;
-    else
-      base = line;
-    double* q = a.p + base * S + s;
-    const double* dq = a.dir_field + base * S + s;
-    const unsigned long long nodes = a.dirichlet ? __ldg(a.dir_mask[AX] + line) : 0ull;
-    // branch-free loads (both values, then a select) so that they overlap
-    if (nodes == 0ull) {
-#pragma unroll 8
-      for (int k = 0; k < n; ++k) col[k * T] = q[k * st];
-    } else {
-#pragma unroll 8
-      for (int k = 0; k < n; ++k) {
-        const double x = q[k * st], d = __ldg(dq + k * st);
-        col[k * T] = ((nodes >> k) & 1ull) ? d : x;
+  const int64_t C = AX == 0 ? S : (AX == 1 ? (int64_t)a.nx * S : plane * S);
+  const int64_t outer_stride = AX == 0 ? (int64_t)a.nx * S : (AX == 1 ? plane * S : 0);
+  const int64_t ls = AX == 0 ? S : (AX == 1 ? (int64_t)a.nx * S : plane * S);
+  const int64_t ncols = plane * a.nz / n * S;
+  const int NC = (n + CH - 1) / CH;
+  const int TW = blockDim.x / NC;
+  const int tx = threadIdx.x % TW;
+  const int c = threadIdx.x / TW;  // chunk; threads past NC chunks idle
+  const bool in_tile = c < NC;
+  const int k0 = c * CH;
+  double* sQ = sm;  // [NC][TW] forward chunk end values
+  double* sP = sQ + NC * TW;
+  double* sX = sP + NC * TW;  // backward chunk start values
+  double* sR = sX + NC * TW;
+  const AxisCoef<double> cf = a.coef[AX];
+  const int64_t ntiles = (ncols + TW - 1) / TW;
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int64_t vcol = tile * TW + tx;
+    const bool active = in_tile && vcol < ncols;
+    const int len = active ? max(0, min(CH, n - k0)) : 0;
+    double* ptr = a.p;
+    const double* dptr = a.dir_field;
+    int s = 0;
+    unsigned long long nodes = 0ull;
+    if (active) {
+      const int64_t outer = vcol / C;
+      const int64_t col = vcol - outer * C;
+      const int64_t off = outer * outer_stride + col + (int64_t)k0 * ls;
+      ptr = a.p + off;
+      dptr = a.dir_field + off;
+      s = (int)(col % S);
+      if (a.dirichlet) nodes = __ldg(a.dir_mask[AX] + vcol / S) >> k0;
+    }
+    double v[CH];
+#pragma unroll
+    for (int m = 0; m < CH; ++m)
+      v[m] = (m < len) ? (((nodes >> m) & 1ull) ? __ldg(dptr + m * ls) : ptr[m * ls]) : 0.0;
+    const double* c_inv = cf.inv_den + (int64_t)k0 * S + s;
+    const double* c_fwd = cf.fwd + (int64_t)k0 * S + s;
+    const double* c_bwd = cf.bwd + (int64_t)k0 * S + s;
+    // forward elimination, chunk-local with carry-in 0
+    const double c1 = active ? __ldg(cf.c1 + s) : 0.0;
+    double q = 0.0, P = 1.0;
+#pragma unroll
+    for (int m = 0; m < CH; ++m) {
+      if (m < len) {
+        q = (v[m] + c1 * q) * __ldg(c_inv + m * S);
+        P = P * __ldg(c_fwd + m * S);
+        v[m] = q;
       }
     }
-    // forward: p_0 /= d_0; p_k = (p_k + c1 p_{k-1}) / d_k (as multiplies)
-    const double c1 = __ldg(a.c1[AX] + s);
-    double prev = col[0] * __ldg(rd + s);
-    col[0] = prev;
-#pragma unroll 8
-    for (int k = 1; k < n; ++k) {
-      prev = (col[k * T] + c1 * prev) * __ldg(rd + k * S + s);
-      col[k * T] = prev;
+    if (in_tile) {
+      sQ[c * TW + tx] = q;
+      sP[c * TW + tx] = P;
     }
-    // back: p_k -= cx_k p_{k+1}, straight to the field
-    q[(n - 1) * st] = prev;
-#pragma unroll 8
-    for (int k = n - 2; k >= 0; --k) {
-      prev = col[k * T] - __ldg(cx + k * S + s) * prev;
-      q[k * st] = prev;
+    __syncthreads();
+    if (c > 0 && len > 0) {
+      double carry = 0.0;
+      for (int cc = 0; cc < c; ++cc) carry = sP[cc * TW + tx] * carry + sQ[cc * TW + tx];
+      double Pm = 1.0;
+#pragma unroll
+      for (int m = 0; m < CH; ++m) {
+        if (m < len) {
+          Pm = Pm * __ldg(c_fwd + m * S);
+          v[m] = v[m] + Pm * carry;
+        }
+      }
     }
+    // back substitution, chunk-local with carry-in 0
+    double x = 0.0, R = 1.0;
+#pragma unroll
+    for (int m = CH - 1; m >= 0; --m) {
+      if (m < len) {
+        const double b = __ldg(c_bwd + m * S);
+        x = v[m] + b * x;
+        R = R * b;
+        v[m] = x;
+      }
+    }
+    if (in_tile) {
+      sX[c * TW + tx] = x;
+      sR[c * TW + tx] = R;
+    }
+    __syncthreads();
+    if (c < NC - 1 && len > 0) {
+      double carry = 0.0;
+      for (int cc = NC - 1; cc > c; --cc) carry = sR[cc * TW + tx] * carry + sX[cc * TW + tx];
+      double Rm = 1.0;
+#pragma unroll
+      for (int m = CH - 1; m >= 0; --m) {
+        if (m < len) {
+          Rm = Rm * __ldg(c_bwd + m * S);
+          v[m] = v[m] + Rm * carry;
+        }
+      }
+    }
+#pragma unroll
+    for (int m = 0; m < CH; ++m)
+      if (m < len) ptr[m * ls] = v[m];
+    __syncthreads();  // the carries of this tile are read before the next overwrites them
   }
 }
 
 // nsteps whole steps; launched cooperatively (every block resident) with
-// blockDim.x * (most points per axis) doubles of dynamic shared memory.
+// 4 * blockDim.x doubles of dynamic shared memory.
 __global__ void __launch_bounds__(128) grid_steps_kernel(const GridStepArgs a) {
   namespace cg = cooperative_groups;
   cg::grid_group grid = cg::this_grid();
-  extern __shared__ double grid_cols[];
-  double* col = grid_cols + threadIdx.x;
+  extern __shared__ double grid_carries[];
   const int first = blockIdx.x * blockDim.x + threadIdx.x;
   const int stride = gridDim.x * blockDim.x;
   for (int step = 0; step < a.nsteps; ++step) {
@@ -169,11 +224,11 @@ __global__ void __launch_bounds__(128) grid_steps_kernel(const GridStepArgs a) {
       grid_sources(a, first, stride);
       grid.sync();
     }
-    grid_axis<0>(a, col, first, stride);
+    grid_axis<0>(a, grid_carries);
     grid.sync();
-    grid_axis<1>(a, col, first, stride);
+    grid_axis<1>(a, grid_carries);
     grid.sync();
-    grid_axis<2>(a, col, first, stride);
+    grid_axis<2>(a, grid_carries);
     grid.sync();
   }
 }

@@ -138,7 +138,6 @@ void thomas_setup(bfvm_solver* m, double dt) {
     m->chunk_ch[a] = 0;
   }
   m->cl_tab_ok = false;
-  m->gr_tab_ok = false;
   m->setup_dt = dt;
   m->setup_D = m->D;
   m->setup_decay = m->decay;
@@ -1298,7 +1297,6 @@ int bfvm_destroy(bfvm_solver* m) {
     for (auto& c : m->chunk) c.release();
     for (auto& c : m->chunk_slots) c.release();
     for (auto& c : m->cl_tab) c.release();
-    for (auto& c : m->gr_tab) c.release();
     m->d_grid_maps.release();
     cudaStreamDestroy(m->stream);
     delete m;
@@ -1881,9 +1879,11 @@ void cluster_run(bfvm_solver* m, double dt, int nsteps, int flags, int cl) {
 }
 
 constexpr int kGridMaxN = 64;              // points per axis (registers per line)
-constexpr int64_t kGridMaxVS = 1 << 20;    // voxel-densities: past this the sweep kernels win
+// voxel-densities: measured faster than the sweep kernels up to 2^19 (18.7 vs
+// 26.7 us/step at 50^3 x 1, 24.8 vs 27.2 at 50^3 x 4), even at 2^20
+constexpr int64_t kGridMaxVS = 1 << 19;
 constexpr int kGridThreads = 128;
-constexpr size_t kGridSmem = (size_t)kGridThreads * kGridMaxN * sizeof(double);  // a column each
+constexpr size_t kGridSmem = (size_t)4 * kGridThreads * sizeof(double);  // chunk carries
 
 // Blocks of the cooperative launch that runs this solver's steps in one
 // launch, or 0 when bfvm_step uses the sweep kernels (or the cluster).
@@ -1905,28 +1905,23 @@ int grid_blocks(bfvm_solver* m) {
     m->grid_per_sm = per_sm > 0 ? per_sm : -1;
   }
   if (m->grid_per_sm < 0) return 0;
+  // tiles of the widest phase: TW = threads / chunks columns per tile
   const int64_t N = (int64_t)m->nx * m->ny * m->nz;
-  const int64_t items =
-      std::max({N / m->nx, N / m->ny, N / m->nz}) * m->S;  // (line, density) per phase
-  return (int)std::min<int64_t>((items + kGridThreads - 1) / kGridThreads,
-                                (int64_t)m->grid_per_sm * m->num_sms);
+  const int ns[3] = {m->nx, m->ny, m->nz};
+  int64_t tiles = 1;
+  for (int ax = 0; ax < 3; ++ax) {
+    const int nc = (ns[ax] + bfvm::kGridChunk - 1) / bfvm::kGridChunk;
+    const int64_t tw = kGridThreads / nc;
+    tiles = std::max(tiles, (N / ns[ax] * m->S + tw - 1) / tw);
+  }
+  const int64_t sources = ((int64_t)m->bulk_vox.size() + m->n_agents) * m->S;
+  const int64_t need = std::max(tiles, (sources + kGridThreads - 1) / kGridThreads);
+  return (int)std::min<int64_t>(need, (int64_t)m->grid_per_sm * m->num_sms);
 }
 
 // nsteps whole steps (bulk -> cells -> LOD_3D) in one cooperative launch.
 void grid_run(bfvm_solver* m, double dt, int nsteps, int flags, int blocks) {
   const int S = m->S;
-  if (!m->gr_tab_ok) {
-    const int ns[3] = {m->nx, m->ny, m->nz};
-    for (int a = 0; a < 3; ++a) {
-      const size_t nS = (size_t)ns[a] * S;
-      std::vector<double> t(2 * nS + S);
-      for (size_t i = 0; i < nS; ++i) t[i] = 1.0 / m->h_den[a][i];
-      std::copy(m->h_cx[a].begin(), m->h_cx[a].end(), t.begin() + nS);
-      std::copy(m->h_c1[a].begin(), m->h_c1[a].end(), t.begin() + 2 * nS);
-      upload(m->gr_tab[a], t, m->stream);
-    }
-    m->gr_tab_ok = true;
-  }
   // scratch: Dirichlet values [N][S] (doubles first), line masks of the x, y
   // and z lines, bulk and agent maps [N] each
   const int64_t N = m->N();
@@ -1961,14 +1956,7 @@ void grid_run(bfvm_solver* m, double dt, int nsteps, int flags, int blocks) {
   a.dt = dt;
   a.bulk = (flags & BFVM_STEP_BULK) && nbulk > 0;
   a.cells = (flags & BFVM_STEP_CELLS) && m->n_agents > 0;
-  const int ns[3] = {m->nx, m->ny, m->nz};
-  for (int ax = 0; ax < 3; ++ax) {
-    const double* t = m->gr_tab[ax].as<double>();
-    const size_t nS = (size_t)ns[ax] * S;
-    a.rd[ax] = t;
-    a.cx[ax] = t + nS;
-    a.c1[ax] = t + 2 * nS;
-  }
+  for (int ax = 0; ax < 3; ++ax) a.coef[ax] = coef_view<double>(m, ax);
   a.bulk_map = maps;
   a.ag_map = maps + N;
   a.dirichlet = m->dir_unique > 0;

@@ -210,13 +210,10 @@ struct bfvm_solver {
   bool cl_tab_ok = false;
   bfvm_rt::DevBuf cl_tab[3];
   // whole steps of a small field in one cooperative launch over all SMs
-  // (bfvm_step under BFVM_PATH_AUTO, opt-in): enabled flag, its per-axis tables
-  // (1/den [n][S], cx [n][S], c1 [S]), rebuilt after each Thomas setup, the
-  // dense voxel maps of bulk entries, agents and Dirichlet nodes [3][N], and
+  // (bfvm_step under BFVM_PATH_AUTO, on by default): enabled flag, the per-call
+  // scratch (Dirichlet values and line masks, bulk and agent voxel maps), and
   // the kernel's resident blocks per SM (0: not queried yet)
-  int grid_steps = 0;
-  bool gr_tab_ok = false;
-  bfvm_rt::DevBuf gr_tab[3];
+  int grid_steps = 1;
   bfvm_rt::DevBuf d_grid_maps;
   int grid_per_sm = 0;
   // cached tensor maps of the y and z sweeps (keyed by field pointer)

@@ -253,9 +253,9 @@ class Solver:
         return n.value
 
     def set_grid_steps(self, enable: bool) -> None:
-        """Whole steps of a small FP64 field (<= 2^20 voxel-densities, <= 64
-        points per axis) in one cooperative launch under PATH_AUTO (off by
-        default: slower than the sweep kernels at 50^3)."""
+        """Whole steps of a small FP64 field (<= 2^19 voxel-densities, <= 64
+        points per axis) in one cooperative launch under PATH_AUTO (on by
+        default); False gives back the sweep kernels."""
         call("bfvm_set_grid_steps", self._h, 1 if enable else 0)
 
     def get_grid_steps(self) -> int:

@@ -272,17 +272,15 @@ BFVM_API int bfvm_get_cluster_steps(bfvm_solver* m, int* blocks);
 
 /* Whole steps of a small field in one cooperative launch over all SMs: under
  * BFVM_PATH_AUTO, bfvm_step runs all its steps in one launch when the FP64
- * field has at most 2^20 voxel-densities and no axis has more than 64
- * points (and the cluster mode above is not in use).  Each step is three
- * phases of whole lines solved in registers (x with the bulk, cell and
- * Dirichlet updates applied as the lines are loaded, then y, then z, each
- * with the Dirichlet values) separated by grid-wide barriers; the lines
- * multiply by precomputed reciprocals of the Thomas denominators (within
- * 1e-15 of the reference's divisions).  Off by default: one thread per
- * line leaves too little parallelism (59 vs 25 us per step at 50^3 x 1 on a
- * B200, of which 5.6 us are the four grid barriers).  enable = 1 turns it
- * on; bfvm_get_grid_steps gives the launch's block count for this solver
- * now (0: not used). */
+ * field has at most 2^19 voxel-densities and no axis has more than 64
+ * points (and the cluster mode above is not in use).  Each step is a phase of
+ * bulk and cell updates, then one phase per axis in which blocks solve tiles
+ * of lines in 8-point chunks as the sweep kernels do (Dirichlet values applied
+ * as the chunks load), separated by grid-wide barriers.  On by default
+ * (18.7 vs 26.7 us per step at 50^3 x 1 on a B200, faster than the sweep
+ * kernels up to 2^19 voxel-densities); enable = 0 gives back the sweep
+ * kernels.  bfvm_get_grid_steps gives the launch's block count for this
+ * solver now (0: not used). */
 BFVM_API int bfvm_set_grid_steps(bfvm_solver* m, int enable);
 BFVM_API int bfvm_get_grid_steps(bfvm_solver* m, int* blocks);
 

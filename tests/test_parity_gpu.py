@@ -658,18 +658,16 @@ GRID_IDS = ["50cube", "odd", "40cube-S5", "thin", "one-point-x"]
 
 @pytest.mark.parametrize("case", GRID_CASES, ids=GRID_IDS)
 def test_grid_steps_match_the_oracle_and_the_sweep_kernels(case):
-    """With grid steps on, bfvm_step on a small FP64 field runs every step in
-    one cooperative launch (a thread per line, Dirichlet values applied as
-    lines load, sources in a phase of their own):
+    """bfvm_step on a small FP64 field runs every step in one cooperative
+    launch (chunked lines per tile, Dirichlet values applied as chunks load,
+    sources in a phase of their own):
     within 1e-12 of the oracle and of the sweep kernels, agents sharing
     voxels included."""
     scn = W.mixed_small(seed=sum(case["shape"]) + 3 * case["S"], **case)
     ref = O.oracle_run(scn, 4, 7)
     with Solver(0) as sv:
         load_scenario(sv, scn)
-        assert sv.get_grid_steps() == 0  # opt-in
-        sv.set_grid_steps(True)
-        assert sv.get_grid_steps() > 0
+        assert sv.get_grid_steps() > 0  # the default for a field this small
         sv.step(scn.dt, 4)
         a = sv.get_densities()
         sv.set_densities(scn.initial_field())
@@ -724,9 +722,7 @@ def test_grid_steps_eligibility():
     with Solver(0) as sv:
         sv.resize_densities(1)
         sv.resize_space(0, 500, 0, 500, 0, 500, 10)  # 50^3 x 1 (fits a cluster)
-        assert sv.get_grid_steps() == 0  # opt-in
-        sv.set_grid_steps(True)
-        assert sv.get_grid_steps() > 0
+        assert sv.get_grid_steps() > 0  # on by default
         sv.set_cluster_steps(True)  # the bit-exact cluster mode comes first
         assert sv.get_cluster_steps() > 0 and sv.get_grid_steps() == 0
         sv.set_cluster_steps(False)
@@ -739,12 +735,14 @@ def test_grid_steps_eligibility():
         sv.set_precision(64)
         sv.resize_space(0, 650, 0, 640, 0, 640, 10)  # 65 points along x
         assert sv.get_grid_steps() == 0
-        sv.resize_densities(5)
-        sv.resize_space(0, 640, 0, 640, 0, 640, 10)  # 64^3 x 5 > 2^20
+        sv.resize_densities(3)
+        sv.resize_space(0, 640, 0, 640, 0, 640, 10)  # 64^3 x 3 > 2^19
         assert sv.get_grid_steps() == 0
-        sv.resize_densities(4)
-        sv.resize_space(0, 640, 0, 640, 0, 640, 10)  # 64^3 x 4 = 2^20
+        sv.resize_densities(2)
+        sv.resize_space(0, 640, 0, 640, 0, 640, 10)  # 64^3 x 2 = 2^19
         assert sv.get_grid_steps() > 0
+        sv.set_grid_steps(False)
+        assert sv.get_grid_steps() == 0
 
 
 def test_add_density_after_the_setup_matches_a_fresh_solver():

@@ -4,7 +4,8 @@
 // more in kernel start-up than in work when every phase of a step is its own
 // launch (7 launches per step at 50^3 x 1).  Here every step runs inside one
 // launch over all SMs, as phases separated by grid-wide barriers of a
-// cooperative launch (all blocks are resident, so each barrier completes):
+// cooperative launch (all blocks are resident, so each barrier completes;
+// after the first step the sources ride on the z phase of the step before):
 //   sources: per bulk entry its update (BioFVM_microenvironment.cpp:603-609)
 //            and then its voxel's agents in list order
 //            (BioFVM_basic_agent.cpp:234-235); per agent voxel without a bulk
@@ -102,8 +103,12 @@ constexpr int kGridChunk = 8;  // points per thread: lines of <= 64 points in <=
 // The lines of one axis in tiles of TW columns x NC chunks (TW = blockDim.x /
 // NC); columns are (line, density) pairs numbered as in lod_sweep_kernel.
 // sm holds 4 * blockDim.x values for the chunks' forward and backward carries.
+// With sources_after (z only), each stored point first takes the next step's
+// bulk and cell updates: every voxel lies on exactly one z chunk, so the
+// thread that solved it is the only one to touch it before the next x phase.
 template <int AX>
-__device__ __forceinline__ void grid_axis(const GridStepArgs& a, double* sm) {
+__device__ __forceinline__ void grid_axis(const GridStepArgs& a, double* sm,
+                                          bool sources_after = false) {
   constexpr int CH = kGridChunk;
   const int S = a.S;
   const int64_t plane = (int64_t)a.nx * a.ny;
@@ -204,9 +209,31 @@ __device__ __forceinline__ void grid_axis(const GridStepArgs& a, double* sm) {
         }
       }
     }
+    if (AX == 2 && sources_after) {
+      const int64_t vox0 = vcol / S + (int64_t)k0 * plane;  // voxel of the chunk's point 0
 #pragma unroll
-    for (int m = 0; m < CH; ++m)
-      if (m < len) ptr[m * ls] = v[m];
+      for (int m = 0; m < CH; ++m) {
+        if (m < len) {
+          const int64_t vox = vox0 + m * plane;
+          double x = v[m];
+          if (a.bulk) {
+            const int e = __ldg(a.bulk_map + vox);
+            if (e >= 0)
+              x = bulk_update(x, __ldg(a.bulk_st + (int64_t)e * S + s),
+                              __ldg(a.bulk_su + (int64_t)e * S + s), a.dt);
+          }
+          if (a.cells) {
+            const int r = __ldg(a.ag_map + vox);
+            if (r >= 0) x = grid_cells(a, x, r, (uint64_t)vox, s);
+          }
+          ptr[m * ls] = x;
+        }
+      }
+    } else {
+#pragma unroll
+      for (int m = 0; m < CH; ++m)
+        if (m < len) ptr[m * ls] = v[m];
+    }
     __syncthreads();  // the carries of this tile are read before the next overwrites them
   }
 }
@@ -219,8 +246,11 @@ __global__ void __launch_bounds__(128) grid_steps_kernel(const GridStepArgs a) {
   extern __shared__ double grid_carries[];
   const int first = blockIdx.x * blockDim.x + threadIdx.x;
   const int stride = gridDim.x * blockDim.x;
+  const bool sources = a.bulk || a.cells;
   for (int step = 0; step < a.nsteps; ++step) {
-    if (a.bulk || a.cells) {
+    // the first step's sources get a phase of their own; later steps' were
+    // applied as the previous z phase stored its lines
+    if (sources && step == 0) {
       grid_sources(a, first, stride);
       grid.sync();
     }
@@ -228,7 +258,7 @@ __global__ void __launch_bounds__(128) grid_steps_kernel(const GridStepArgs a) {
     grid.sync();
     grid_axis<1>(a, grid_carries);
     grid.sync();
-    grid_axis<2>(a, grid_carries);
+    grid_axis<2>(a, grid_carries, sources && step + 1 < a.nsteps);
     grid.sync();
   }
 }

@@ -10,7 +10,7 @@
 //            and then its voxel's agents in list order
 //            (BioFVM_basic_agent.cpp:234-235); per agent voxel without a bulk
 //            entry its agents;
-//   x, y, z: tiles of TW lines x NC chunks of 8 points per block (as the
+//   x, y, z: tiles of TW lines x NC chunks of 4 or 8 points per block (as the
 //            register sweep kernel: chunk-local passes, the chunks' carries
 //            folded through shared memory, fix-ups); as a chunk is loaded, its
 //            Dirichlet nodes take their values (BioFVM_microenvironment.cpp:
@@ -98,18 +98,15 @@ __device__ __forceinline__ void grid_sources(const GridStepArgs& a, int64_t firs
   }
 }
 
-constexpr int kGridChunk = 8;  // points per thread: lines of <= 64 points in <= 8 chunks
-
 // The lines of one axis in tiles of TW columns x NC chunks (TW = blockDim.x /
 // NC); columns are (line, density) pairs numbered as in lod_sweep_kernel.
 // sm holds 4 * blockDim.x values for the chunks' forward and backward carries.
 // With sources_after (z only), each stored point first takes the next step's
 // bulk and cell updates: every voxel lies on exactly one z chunk, so the
 // thread that solved it is the only one to touch it before the next x phase.
-template <int AX>
+template <int AX, int CH>
 __device__ __forceinline__ void grid_axis(const GridStepArgs& a, double* sm,
                                           bool sources_after = false) {
-  constexpr int CH = kGridChunk;
   const int S = a.S;
   const int64_t plane = (int64_t)a.nx * a.ny;
   const int n = AX == 0 ? a.nx : (AX == 1 ? a.ny : a.nz);
@@ -238,8 +235,10 @@ __device__ __forceinline__ void grid_axis(const GridStepArgs& a, double* sm,
   }
 }
 
-// nsteps whole steps; launched cooperatively (every block resident) with
+// nsteps whole steps with CH-point chunks (4 or 8: lines of <= 64 points in
+// at most 16 or 8 chunks); launched cooperatively (every block resident) with
 // 4 * blockDim.x doubles of dynamic shared memory.
+template <int CH>
 __global__ void __launch_bounds__(128) grid_steps_kernel(const GridStepArgs a) {
   namespace cg = cooperative_groups;
   cg::grid_group grid = cg::this_grid();
@@ -254,11 +253,11 @@ __global__ void __launch_bounds__(128) grid_steps_kernel(const GridStepArgs a) {
       grid_sources(a, first, stride);
       grid.sync();
     }
-    grid_axis<0>(a, grid_carries);
+    grid_axis<0, CH>(a, grid_carries);
     grid.sync();
-    grid_axis<1>(a, grid_carries);
+    grid_axis<1, CH>(a, grid_carries);
     grid.sync();
-    grid_axis<2>(a, grid_carries, sources && step + 1 < a.nsteps);
+    grid_axis<2, CH>(a, grid_carries, sources && step + 1 < a.nsteps);
     grid.sync();
   }
 }

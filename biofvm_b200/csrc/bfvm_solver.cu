@@ -1885,42 +1885,64 @@ constexpr int64_t kGridMaxVS = 1 << 19;
 constexpr int kGridThreads = 128;
 constexpr size_t kGridSmem = (size_t)4 * kGridThreads * sizeof(double);  // chunk carries
 
+// Tiles of the widest phase of grid steps with ch-point chunks (TW = threads
+// / chunks columns per tile).
+int64_t grid_tiles(const bfvm_solver* m, int ch) {
+  const int64_t N = (int64_t)m->nx * m->ny * m->nz;
+  const int ns[3] = {m->nx, m->ny, m->nz};
+  int64_t tiles = 1;
+  for (int ax = 0; ax < 3; ++ax) {
+    const int nc = (ns[ax] + ch - 1) / ch;
+    const int64_t tw = kGridThreads / nc;
+    tiles = std::max(tiles, (N / ns[ax] * m->S + tw - 1) / tw);
+  }
+  return tiles;
+}
+
 // Blocks of the cooperative launch that runs this solver's steps in one
-// launch, or 0 when bfvm_step uses the sweep kernels (or the cluster).
-int grid_blocks(bfvm_solver* m) {
+// launch, or 0 when bfvm_step uses the sweep kernels (or the cluster).  *ch:
+// the chunk length, 4 when the widest phase fits one wave of resident blocks
+// (shorter chains, measured faster: 50^3 x 1 19.9 -> 17.8 us/step, 32^3 x 8
+// 21.5 -> 16.8), else 8 (50^3 x 4: 27.3 us/step, 33.4 with 4-point chunks in
+// two waves).
+int grid_blocks(bfvm_solver* m, int* ch = nullptr) {
   if (!m->grid_steps || m->path != BFVM_PATH_AUTO || m->precision != BFVM_FP64 ||
       m->lod_dims != 3 || !m->uniform || m->fuse_sources || m->slab_planes > 0)
     return 0;
   if (m->nx > kGridMaxN || m->ny > kGridMaxN || m->nz > kGridMaxN) return 0;
   if ((int64_t)m->NS() > kGridMaxVS || cluster_blocks(m) > 0) return 0;
-  if (m->grid_per_sm == 0) {
+  if (m->grid_per_sm[0] == 0) {
     int coop = 0;
     BFVM_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, m->device));
-    int per_sm = 0;
+    int per4 = 0, per8 = 0;
     if (coop) {
-      allow_smem((const void*)bfvm::grid_steps_kernel, m->device, kGridSmem);
+      allow_smem((const void*)bfvm::grid_steps_kernel<4>, m->device, kGridSmem);
+      allow_smem((const void*)bfvm::grid_steps_kernel<8>, m->device, kGridSmem);
       BFVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-          &per_sm, bfvm::grid_steps_kernel, kGridThreads, kGridSmem));
+          &per4, bfvm::grid_steps_kernel<4>, kGridThreads, kGridSmem));
+      BFVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &per8, bfvm::grid_steps_kernel<8>, kGridThreads, kGridSmem));
     }
-    m->grid_per_sm = per_sm > 0 ? per_sm : -1;
+    m->grid_per_sm[0] = per4 > 0 ? per4 : -1;
+    m->grid_per_sm[1] = per8 > 0 ? per8 : -1;
   }
-  if (m->grid_per_sm < 0) return 0;
-  // tiles of the widest phase: TW = threads / chunks columns per tile
-  const int64_t N = (int64_t)m->nx * m->ny * m->nz;
-  const int ns[3] = {m->nx, m->ny, m->nz};
-  int64_t tiles = 1;
-  for (int ax = 0; ax < 3; ++ax) {
-    const int nc = (ns[ax] + bfvm::kGridChunk - 1) / bfvm::kGridChunk;
-    const int64_t tw = kGridThreads / nc;
-    tiles = std::max(tiles, (N / ns[ax] * m->S + tw - 1) / tw);
+  const int64_t sources =
+      (((int64_t)m->bulk_vox.size() + m->n_agents) * m->S + kGridThreads - 1) / kGridThreads;
+  for (int i = 0; i < 2; ++i) {
+    const int c = i == 0 ? 4 : 8;
+    if (m->grid_per_sm[i] < 0) continue;
+    const int64_t wave = (int64_t)m->grid_per_sm[i] * m->num_sms;
+    const int64_t tiles = grid_tiles(m, c);
+    if (tiles <= wave || c == 8) {
+      if (ch) *ch = c;
+      return (int)std::min<int64_t>(std::max(tiles, sources), wave);
+    }
   }
-  const int64_t sources = ((int64_t)m->bulk_vox.size() + m->n_agents) * m->S;
-  const int64_t need = std::max(tiles, (sources + kGridThreads - 1) / kGridThreads);
-  return (int)std::min<int64_t>(need, (int64_t)m->grid_per_sm * m->num_sms);
+  return 0;
 }
 
 // nsteps whole steps (bulk -> cells -> LOD_3D) in one cooperative launch.
-void grid_run(bfvm_solver* m, double dt, int nsteps, int flags, int blocks) {
+void grid_run(bfvm_solver* m, double dt, int nsteps, int flags, int blocks, int ch) {
   const int S = m->S;
   // scratch: Dirichlet values [N][S] (doubles first), line masks of the x, y
   // and z lines, bulk and agent maps [N] each
@@ -1974,8 +1996,9 @@ void grid_run(bfvm_solver* m, double dt, int nsteps, int flags, int blocks) {
   a.ag_t1 = m->d_ag_t1.as<double>();
   a.ag_t2 = m->d_ag_t2.as<double>();
   void* params[] = {&a};
-  BFVM_CUDA(cudaLaunchCooperativeKernel((const void*)bfvm::grid_steps_kernel,
-                                        dim3((unsigned)blocks), dim3(kGridThreads), params,
+  const void* k = ch == 4 ? (const void*)bfvm::grid_steps_kernel<4>
+                          : (const void*)bfvm::grid_steps_kernel<8>;
+  BFVM_CUDA(cudaLaunchCooperativeKernel(k, dim3((unsigned)blocks), dim3(kGridThreads), params,
                                         kGridSmem, m->stream));
   check_launch(m);
 }
@@ -2026,12 +2049,13 @@ int bfvm_step(bfvm_solver* m, double dt, int nsteps, int flags) {
       cluster_run(m, dt, nsteps, flags, cl);
       return;
     }
-    const int gb = nsteps > 0 ? grid_blocks(m) : 0;
+    int gch = 8;
+    const int gb = nsteps > 0 ? grid_blocks(m, &gch) : 0;
     if (gb > 0) {
       check_lod_mesh(m);
       if (!m->setup_done) thomas_setup(m, dt);
       build_all(m);
-      grid_run(m, dt, nsteps, flags, gb);
+      grid_run(m, dt, nsteps, flags, gb, gch);
       return;
     }
     for (int it = 0; it < nsteps; ++it) step_once(m, dt, flags, nullptr);

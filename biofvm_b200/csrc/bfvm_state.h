@@ -212,10 +212,10 @@ struct bfvm_solver {
   // whole steps of a small field in one cooperative launch over all SMs
   // (bfvm_step under BFVM_PATH_AUTO, on by default): enabled flag, the per-call
   // scratch (Dirichlet values and line masks, bulk and agent voxel maps), and
-  // the kernel's resident blocks per SM (0: not queried yet)
+  // the kernels' resident blocks per SM (0: not queried yet)
   int grid_steps = 1;
   bfvm_rt::DevBuf d_grid_maps;
-  int grid_per_sm = 0;
+  int grid_per_sm[2] = {0, 0};  // 4- and 8-point chunk kernels (-1: not usable)
   // cached tensor maps of the y and z sweeps (keyed by field pointer)
   CUtensorMap maps[3];
   const void* map_key[3] = {nullptr, nullptr, nullptr};

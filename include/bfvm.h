@@ -275,10 +275,10 @@ BFVM_API int bfvm_get_cluster_steps(bfvm_solver* m, int* blocks);
  * field has at most 2^19 voxel-densities and no axis has more than 64
  * points (and the cluster mode above is not in use).  Each step is a phase of
  * bulk and cell updates, then one phase per axis in which blocks solve tiles
- * of lines in 8-point chunks as the sweep kernels do (Dirichlet values applied
+ * of lines in 4- or 8-point chunks as the sweep kernels do (Dirichlet values applied
  * as the chunks load), separated by grid-wide barriers; after the first
  * step the bulk and cell updates are applied as the previous z phase stores
- * its points.  On by default (18.0 vs 24.7 us per step at 50^3 x 1 on a
+ * its points.  On by default (17.7 vs 24.7 us per step at 50^3 x 1 on a
  * B200 with 1000 agents, faster than the sweep
  * kernels up to 2^19 voxel-densities); enable = 0 gives back the sweep
  * kernels.  bfvm_get_grid_steps gives the launch's block count for this

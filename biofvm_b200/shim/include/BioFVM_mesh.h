@@ -1,7 +1,8 @@
 // Host-side Cartesian mesh with BioFVM's names (BioFVM_mesh.h:49-188):
 // voxel centres, volumes, indices and nearest-voxel lookup by the reference's
-// formulas.  Only the Cartesian mesh of the transport path is provided; the
-// connectivity lists and voxel faces (unused by the LOD solver) are not built.
+// formulas, and each voxel's list of face-connected neighbours.  Only the
+// Cartesian mesh of the transport path is provided; voxel faces (unused by
+// the LOD solver) are not built.
 #ifndef __BioFVM_mesh_h__
 #define __BioFVM_mesh_h__
 
@@ -27,8 +28,12 @@ class General_Mesh {
   General_Mesh();
   std::vector<double> bounding_box;  // [xmin ymin zmin xmax ymax zmax]
   std::vector<Voxel> voxels;
-  std::vector<std::vector<int> > connected_voxel_indices;  // not built
+  // per voxel its face neighbours, in the order the reference connects them
+  // (BioFVM_mesh.cpp:873-915): x-1, x+1, y-1, y+1, z-1, z+1 where present
+  std::vector<std::vector<int> > connected_voxel_indices;
   bool is_position_valid(double x, double y, double z);
+  // adds j to voxel i's list and i to voxel j's (BioFVM_mesh.cpp:260-268)
+  void connect_voxels_indices_only(int i, int j, double SA);
   bool Cartesian_mesh;
   bool uniform_mesh;
   bool regular_mesh;

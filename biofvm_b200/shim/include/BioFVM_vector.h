@@ -42,8 +42,31 @@ void axpy(std::vector<double>* y, std::vector<double>& a, std::vector<double>& x
 void naxpy(std::vector<double>* y, double& a, std::vector<double>& x);
 void naxpy(std::vector<double>* y, std::vector<double>& a, std::vector<double>& x);
 
+// y = (y + a.*x) ./ d
+void axpy_div(std::vector<double>* y, std::vector<double>& a, std::vector<double>& x,
+              std::vector<double>& d);
+// y = y + a1.*x1 + a2.*x2
+void double_axpy(std::vector<double>* y, std::vector<double>& a1, std::vector<double>& a2,
+                 std::vector<double>& x1, std::vector<double>& x2);
+// y = y + a.*(x1 + x2)
+void double_axpy(std::vector<double>* y, std::vector<double>& a, std::vector<double>& x1,
+                 std::vector<double>& x2);
+// y = (y + a.*(x1 + x2)) ./ d
+void double_axpy_div(std::vector<double>* y, std::vector<double>& a, std::vector<double>& x1,
+                     std::vector<double>& x2, std::vector<double>& d);
+// y = (y + a1.*x1 + a2.*x2) ./ d
+void double_axpy_div(std::vector<double>* y, std::vector<double>& a1, std::vector<double>& a2,
+                     std::vector<double>& x1, std::vector<double>& x2, std::vector<double>& d);
+
+// Comma-separated values, each printed as %.7e.  vector_to_csv returns a new
+// char[] buffer (release with delete[]); vector_to_csv_safe replaces the
+// caller's buffer (delete[] of the old one) with a new one; the two-argument
+// vector_to_csv writes into the caller's buffer, which must hold 16 chars
+// per value plus one.
 void csv_to_vector(const char* buffer, std::vector<double>& vect);
 char* vector_to_csv(const std::vector<double>& vect);
+void vector_to_csv_safe(const std::vector<double>& vect, char*& buffer);
+void vector_to_csv(const std::vector<double>& vect, char*& buffer);
 }  // namespace BioFVM
 
 #endif

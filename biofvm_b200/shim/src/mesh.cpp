@@ -19,11 +19,18 @@ std::ostream& operator<<(std::ostream& os, const Voxel& v) {
 
 General_Mesh::General_Mesh()
     : bounding_box{-0.5, -0.5, -0.5, 0.5, 0.5, 0.5},
+      voxels(1),
+      connected_voxel_indices(1),
       Cartesian_mesh(false),
       uniform_mesh(false),
       regular_mesh(false),
       use_voxel_faces(false),
       units("none") {}
+
+void General_Mesh::connect_voxels_indices_only(int i, int j, double) {
+  connected_voxel_indices[i].push_back(j);
+  connected_voxel_indices[j].push_back(i);
+}
 
 bool General_Mesh::is_position_valid(double x, double y, double z) {
   // BioFVM_mesh.cpp:208-217
@@ -93,7 +100,25 @@ void Cartesian_Mesh::build_voxels() {
         v.mesh_index = (int)n;
         v.volume = dV;
       }
-  connected_voxel_indices.clear();
+  // the reference connects all x pairs, then all y pairs, then all z pairs,
+  // each pair (lower, upper) once, so every voxel's list reads x-1, x+1,
+  // y-1, y+1, z-1, z+1 (those that exist)
+  connected_voxel_indices.assign(nx * ny * nz, std::vector<int>());
+  const int jx = 1, jy = (int)nx, jz = (int)(nx * ny);
+  n = 0;
+  for (size_t k = 0; k < nz; ++k)
+    for (size_t j = 0; j < ny; ++j)
+      for (size_t i = 0; i < nx; ++i, ++n) {
+        std::vector<int>& c = connected_voxel_indices[n];
+        const int v = (int)n;
+        c.reserve(6);
+        if (i > 0) c.push_back(v - jx);
+        if (i + 1 < nx) c.push_back(v + jx);
+        if (j > 0) c.push_back(v - jy);
+        if (j + 1 < ny) c.push_back(v + jy);
+        if (k > 0) c.push_back(v - jz);
+        if (k + 1 < nz) c.push_back(v + jz);
+      }
 }
 
 void Cartesian_Mesh::resize(double x0, double x1, double y0, double y1, double z0, double z1,

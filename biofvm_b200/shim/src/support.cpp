@@ -144,14 +144,72 @@ void csv_to_vector(const char* buffer, std::vector<double>& vect) {
     p = end;
   }
 }
+// The values as "%.7e" separated by commas (BioFVM_vector.cpp:313-364).
+namespace {
+size_t csv_write(const std::vector<double>& vect, char* out) {
+  size_t pos = 0;
+  for (size_t i = 0; i < vect.size(); ++i)
+    pos += (size_t)std::sprintf(out + pos, i + 1 < vect.size() ? "%.7e," : "%.7e", vect[i]);
+  out[pos] = '\0';
+  return pos;
+}
+// room for one "%.7e," value: sign, digit, point, 7 digits, e, sign, up to 3
+// exponent digits, comma
+constexpr size_t kCsvDatum = 16;
+}  // namespace
+
 char* vector_to_csv(const std::vector<double>& vect) {
-  std::ostringstream os;
-  os << std::setprecision(17);
-  for (size_t i = 0; i < vect.size(); ++i) os << vect[i] << (i + 1 < vect.size() ? "," : "");
-  const std::string s = os.str();
-  char* out = static_cast<char*>(std::malloc(s.size() + 1));
-  std::memcpy(out, s.c_str(), s.size() + 1);
+  char* out = new char[kCsvDatum * vect.size() + 1];
+  csv_write(vect, out);
   return out;
+}
+
+void vector_to_csv_safe(const std::vector<double>& vect, char*& buffer) {
+  delete[] buffer;
+  buffer = new char[kCsvDatum * vect.size() + 1];
+  csv_write(vect, buffer);
+}
+
+void vector_to_csv(const std::vector<double>& vect, char*& buffer) { csv_write(vect, buffer); }
+
+// ---- fused elementwise updates (declared by BioFVM_vector.h:97-106) -------
+
+void axpy_div(std::vector<double>* y, std::vector<double>& a, std::vector<double>& x,
+              std::vector<double>& d) {
+  std::vector<double>& Y = *y;
+  for (size_t i = 0; i < Y.size(); ++i) {
+    Y[i] += a[i] * x[i];
+    Y[i] /= d[i];
+  }
+}
+
+void double_axpy(std::vector<double>* y, std::vector<double>& a1, std::vector<double>& a2,
+                 std::vector<double>& x1, std::vector<double>& x2) {
+  std::vector<double>& Y = *y;
+  for (size_t i = 0; i < Y.size(); ++i) {
+    Y[i] += a1[i] * x1[i];
+    Y[i] += a2[i] * x2[i];
+  }
+}
+
+void double_axpy(std::vector<double>* y, std::vector<double>& a, std::vector<double>& x1,
+                 std::vector<double>& x2) {
+  std::vector<double>& Y = *y;
+  for (size_t i = 0; i < Y.size(); ++i) Y[i] += a[i] * (x1[i] + x2[i]);
+}
+
+void double_axpy_div(std::vector<double>* y, std::vector<double>& a, std::vector<double>& x1,
+                     std::vector<double>& x2, std::vector<double>& d) {
+  double_axpy(y, a, x1, x2);
+  std::vector<double>& Y = *y;
+  for (size_t i = 0; i < Y.size(); ++i) Y[i] /= d[i];
+}
+
+void double_axpy_div(std::vector<double>* y, std::vector<double>& a1, std::vector<double>& a2,
+                     std::vector<double>& x1, std::vector<double>& x2, std::vector<double>& d) {
+  double_axpy(y, a1, a2, x1, x2);
+  std::vector<double>& Y = *y;
+  for (size_t i = 0; i < Y.size(); ++i) Y[i] /= d[i];
 }
 
 // ---- stopwatch (wall time) ----------------------------------------------

@@ -12,7 +12,9 @@ ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
 SHIM_INCLUDE = os.path.join(ROOT, "biofvm_b200", "shim", "include")
 DROPIN = os.path.join(ROOT, "biofvm_b200", "shim", "_build", "dropin", "examples")
 REFBIN = os.path.join(ROOT, "oracle", "_ref", "examples")
-REFERENCE_EXAMPLES = "/root/reference/examples"
+# the reference source tree (read only), named by BIOFVM_REFERENCE
+REFERENCE_EXAMPLES = os.path.join(os.environ.get("BIOFVM_REFERENCE", "/root/reference"),
+                                  "examples")
 
 # example -> command-line arguments (dt, t_max, dx where the example takes them)
 EXAMPLES = {
@@ -162,3 +164,39 @@ def test_multicellds_files_match_the_reference_build(tmp_path, data_matlab, mesh
         elif name.endswith(".mat"):
             assert np.array_equal(read_mat4(pa), read_mat4(fb[name])), name
     assert la == lb
+
+
+def test_mesh_connectivity_and_vector_helpers_match_the_reference_build():
+    """tests/dropin/mesh_vector_driver.cpp (host only): every voxel's list of
+    face neighbours after Cartesian_Mesh::resize (the default one-voxel mesh,
+    a 7 x 5 x 4 mesh, a mesh with a one-node axis) and the CSV helpers must
+    print the same text in both builds.  The fused elementwise helpers, which
+    the reference declares without defining, are checked against their
+    stated formulas."""
+    gpu = os.path.join(ROOT, "biofvm_b200", "shim", "_build", "dropin", "drivers",
+                       "mesh_vector_driver")
+    ref = os.path.join(ROOT, "oracle", "_ref", "drivers", "mesh_vector_driver")
+    if not (os.path.exists(gpu) and os.path.exists(ref)):
+        pytest.skip("driver binaries not built (they need the reference sources)")
+    out = {}
+    for tag, exe in (("ref", ref), ("gpu", gpu)):
+        r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+        assert r.returncode == 0, (tag, r.stderr[-2000:])
+        out[tag] = r.stdout.splitlines()
+    keep = ("C0", "C1", "C2", "S1", "S2", "S3", "B ")
+    a = [l for l in out["ref"] if l.startswith(keep)]
+    b = [l for l in out["gpu"] if l.startswith(keep)]
+    assert a and a == b
+    assert "C1 size 140" in a
+    v = {}
+    for line in out["gpu"]:
+        if line.startswith("V "):
+            _, name, x = line.split()
+            v.setdefault(name, []).append(float(x))
+    y, a1, a2 = np.array([1.0, 2, 3]), np.array([0.5, -1, 2]), np.array([3.0, 0.25, -0.5])
+    x1, x2, d = np.array([4.0, 5, -6]), np.array([-1.0, 2, 0.125]), np.array([2.0, 4, -8])
+    assert v["axpy_div"] == list((y + a1 * x1) / d)
+    assert v["double_axpy2"] == list(y + a1 * x1 + a2 * x2)
+    assert v["double_axpy1"] == list(y + a1 * (x1 + x2))
+    assert v["double_axpy_div1"] == list((y + a1 * (x1 + x2)) / d)
+    assert v["double_axpy_div2"] == list((y + a1 * x1 + a2 * x2) / d)

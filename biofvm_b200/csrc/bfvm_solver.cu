@@ -2491,6 +2491,13 @@ extern "C" int bfvm_get_voxel_densities_noalloc(bfvm_solver* m, int64_t count,
                                                 const int64_t* voxels, double* values) {
   return SOLVER_CALL(m, {
     require(count >= 0 && (count == 0 || (voxels && values)), "bad arguments");
+    // bound count before any product of it, so no size below wraps around
+    const size_t per_voxel = sizeof(int64_t) + (size_t)std::max(m->S, 1) * sizeof(double);
+    require((uint64_t)count <= kGatherScratchBytes / per_voxel,
+            "bfvm_get_voxel_densities_noalloc: " + std::to_string(count) + " voxels x " +
+                std::to_string(m->S) + " densities do not fit the " +
+                std::to_string(kGatherScratchBytes) +
+                "-byte static scratch (at most count*(8 + 8*S) bytes)");
     const size_t vox_bytes = ((size_t)count * sizeof(int64_t) + 255) & ~(size_t)255;
     const size_t val_bytes = (size_t)count * m->S * sizeof(double);
     require(vox_bytes + val_bytes <= kGatherScratchBytes,

@@ -14,15 +14,16 @@ with no data-path collective), so per-GPU work is fixed: weak scaling.  Time
 is the max over ranks of the device time.
 
 --impl reference times the unmodified BioFVM reference (compiled from its
-sources into oracle/_ref/) on this host's cores, on a bounded sample of the
-same workload, and prints the same metric.
+sources into oracle/_ref/) on this host's cores, on the same workload with the
+same --steps and --warmup, and prints the same metric.  The reference's
+layout of the 256^3 x 10 case takes about 26 GB of host memory; a host with
+less runs the 128^3 x 10 sample instead and says so in the line.
 """
 from __future__ import annotations
 
 import argparse
 import json
 import os
-import re
 import statistics
 import subprocess
 import sys
@@ -128,19 +129,25 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.samples)}
 
 
-def ncu_traffic(kernel_key: str):
-    """DRAM bytes per launch of the dominant kernel from the committed ncu
-    summary (a line `traffic_bytes_per_launch <kernel> <bytes> <units>`)."""
-    path = os.path.join(ROOT, "profiles", "lod_sweeps_lod256.md")
-    if not os.path.exists(path):
-        return None
-    pat = re.compile(r"traffic_bytes_per_launch\s+(\S+)\s+([0-9.eE+]+)")
-    with open(path) as f:
-        for line in f:
-            m = pat.search(line)
-            if m and m.group(1) == kernel_key:
-                return float(m.group(2))
-    return None
+TRAFFIC_PROFILE = os.path.join(ROOT, "profiles", "sweeps_traffic_lod256.json")
+
+
+def ncu_traffic(axis_key: str, kernel_kind: int):
+    """DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch
+    of the sweep kernel of an axis at the full 256^3 x 10 size, from the
+    one-pass ncu capture recorded in profiles/sweeps_traffic_lod256.json
+    (the capture's command is in the file).  None when the file lacks the
+    axis or the capture ran another kernel than the one timed here
+    (kernel_kind: the tuner's choice, a BFVM_PATH_* value, 0 = the default,
+    which the capture ran)."""
+    if not os.path.exists(TRAFFIC_PROFILE):
+        return None, None
+    with open(TRAFFIC_PROFILE) as f:
+        d = json.load(f)
+    k = d.get("launches", {}).get(axis_key)
+    if not k or (kernel_kind != 0 and kernel_kind != k.get("path")):
+        return None, None
+    return float(k["dram_bytes_read"]) + float(k["dram_bytes_write"]), k["kernel"]
 
 
 def dist_init(args):
@@ -180,28 +187,79 @@ def max_over_ranks(x: float, world: int) -> float:
 
 # ---------------------------------------------------------------------------
 
-def reference_sample(threads: int):
-    """A bounded sample of the headline workload for the CPU reference:
-    128^3 voxels x 10 substrates (1/8 of the voxels), agents at the same
-    density (12.5k), the bulk sphere at the same radius."""
+def host_memory_gb():
+    """(MemTotal, MemAvailable) of this host in GB, and the cgroup memory
+    limit that applies to this process (None when unlimited)."""
+    total = avail = None
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                k, v = line.split(":", 1)
+                if k == "MemTotal":
+                    total = int(v.split()[0]) / 1e6
+                elif k == "MemAvailable":
+                    avail = int(v.split()[0]) / 1e6
+    except OSError:
+        pass
+    limit = None
+    for path in ("/sys/fs/cgroup/memory.max", "/sys/fs/cgroup/memory/memory.limit_in_bytes"):
+        try:
+            with open(path) as f:
+                v = f.read().strip()
+            if v.isdigit() and int(v) < (1 << 60):
+                limit = int(v) / 1e9
+            break
+        except OSError:
+            continue
+    return total, avail, limit
+
+
+# Host memory the reference's layout takes at 256^3 x 10 with 100k agents
+# (a heap vector per voxel for the density, its double buffer and the three
+# bulk-rate temporaries, plus the mesh's voxels): 26.4 GB peak resident,
+# measured; with headroom for the rest of the process.
+REFERENCE_256_GB = 32.0
+
+
+def reference_scenario(sample: bool):
+    """The headline workload (256^3 x 10 FP64, 100k agents, the bulk sphere)
+    for the CPU reference; sample=True takes the 128^3 x 10 cube with agents
+    at the same density (12.5k), for hosts without the memory for the full
+    case."""
     from biofvm_b200 import workloads as W
 
-    return W.lod_cube(128, 10, 12_500, steps=1, name="lod_128_sample")
+    if sample:
+        return W.lod_cube(128, 10, 12_500, steps=1, name="lod_128_sample")
+    return W.lod_256(steps=1)
 
 
-def time_reference(steps: int, warmup: int, threads: int):
+def time_reference(steps: int, warmup: int, threads: int, sample: bool = False):
+    """The reference (compiled from its sources) on this host's cores: setup,
+    `warmup` untimed steps (the first allocates the bulk temporaries), then
+    `steps` timed steps (steady_clock around the loop)."""
     from oracle import oracle as O
 
     variant = "v3" if (O.reference_available("v3") and _host_has_avx2()) else "core2"
-    scn = reference_sample(threads)
+    scn = reference_scenario(sample)
     t0 = time.perf_counter()
     ref = O.Reference(scn, variant, threads=threads, cells_single_thread=False)
     setup = time.perf_counter() - t0
-    ref.run(warmup)
+    if warmup > 0:
+        ref.run(warmup)
     secs = ref.run(steps)
     ref.close()
     vs = scn.num_voxels * scn.S * steps / secs
     return vs, secs, setup, variant, scn
+
+
+def reference_fits():
+    """Whether this host can hold the reference's layout of the full
+    headline case, and the memory figures that decided it."""
+    total, avail, limit = host_memory_gb()
+    known = [x for x in (avail, limit, total) if x is not None]
+    room = min(known) if known else 0.0
+    return room >= REFERENCE_256_GB, {"mem_total_gb": total, "mem_available_gb": avail,
+                                      "cgroup_limit_gb": limit}
 
 
 def _host_has_avx2() -> bool:
@@ -213,28 +271,43 @@ def _host_has_avx2() -> bool:
         return False
 
 
+def reference_baseline(steps: int, warmup: int):
+    """cpu_baseline entry: the reference on every host core, on the full
+    headline workload when the host has the memory, else on the 128^3 sample
+    (said in `sample`)."""
+    threads = os.cpu_count() or 1
+    fits, mem = reference_fits()
+    vs, secs, setup, variant, scn = time_reference(steps, warmup, threads, sample=not fits)
+    what = (f"{scn.shape[0]}^3 x {scn.S} substrates, {scn.num_agents} agents, bulk sphere "
+            f"r=500um: " + ("the whole headline workload" if fits else
+                            "1/8 of the headline workload's voxels (host memory "
+                            f"{mem} below the {REFERENCE_256_GB} GB the full case needs)"))
+    return {"value": vs, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"{what}; {steps} timed steps after {warmup} warm-up; reference build "
+                      f"{variant} (OpenMP threads {threads})",
+            "ms_per_step": 1e3 * secs / steps, "setup_s": setup, "host_memory": mem,
+            "same_config": fits}, scn
+
+
 def run_reference_arm(args, world, rank):
     if rank != 0:
         return
-    threads = os.cpu_count() or 1
-    # a step of the sample is ~0.05-0.5 s on a many-core host; keep the run bounded
-    steps = max(1, min(args.steps, 20))
-    warmup = max(1, min(args.warmup, 3))
-    vs, secs, setup, variant, scn = time_reference(steps, warmup, threads)
-    sample = (f"{scn.shape[0]}^3 x {scn.S} substrates, {scn.num_agents} agents, {steps} timed "
-              f"steps after {warmup} warm-up (1/8 of the 256^3 workload's voxels, same density "
-              f"of agents); reference build {variant}; OpenMP threads {threads}")
+    cpu, scn = reference_baseline(args.steps, args.warmup)
+    full = cpu["same_config"]
     line = {
-        "impl": "reference", "metric": METRIC, "value": vs, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": steps, "warmup": warmup, "ms_per_step": 1e3 * secs / steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded)",
-        "config": {"workload": "lod_256 sample: lod_128 (256^3 x 10 FP64 workload at 1/8 the "
-                               "voxels)", "threads": threads},
-        "cpu_baseline": {"value": vs, "unit": UNIT, "cores": threads, "kind": "reference",
-                         "sample": sample},
-        "e2e": {"value": vs, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "setup_s": setup,
+        "impl": "reference", "metric": METRIC, "value": cpu["value"], "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": cpu["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": ("lod_256: 256^3 voxels x 10 substrates FP64, 100000 agents, "
+                                "bulk sphere r=500um, dt=0.01") if full else
+                   "lod_256 sample: lod_128 (256^3 x 10 FP64 workload at 1/8 the voxels)",
+                   "voxels": scn.num_voxels, "substrates": scn.S, "agents": scn.num_agents,
+                   "threads": cpu["cores"], "parallelism": "host cores (OpenMP)"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": cpu["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "setup_s": cpu["setup_s"],
     }
     print(json.dumps(line), flush=True)
 
@@ -297,7 +370,9 @@ def run_ours(args, world, rank, local):
     per["sources"] = ks
     hbm, peak_kind = peaks()
     achieved = sweeps_in[dom] * BYTES_PER_VS_SWEEP * N * S / (per[dom] / 1e3) / 1e9
-    traffic = ncu_traffic(dom)
+    dom_axis = {"x_sweep": 0, "y_sweep": 1, "z_sweep": 2}.get(dom)
+    traffic, traffic_kernel = (ncu_traffic(dom, tuned[dom_axis][0]) if dom_axis is not None
+                               else (None, None))
 
     # end to end through the C ABI with host buffers: every step uploads the
     # agents' voxels and secretion/uptake constants (as when agents move and
@@ -337,12 +412,12 @@ def run_ours(args, world, rank, local):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # the reference on this host's cores, on the same workload with the
+        # same steps and warm-up (after the device work, which it does not
+        # overlap)
         try:
-            threads = os.cpu_count() or 1
-            vs, secs, setup, variant, sscn = time_reference(3, 1, threads)
-            cpu = {"value": vs, "unit": UNIT, "cores": threads, "kind": "reference",
-                   "sample": f"{sscn.shape[0]}^3 x {sscn.S}, {sscn.num_agents} agents, 3 steps "
-                             f"(1/8 of the workload's voxels), reference build {variant}"}
+            sv.synchronize()
+            cpu, _ = reference_baseline(args.steps, args.warmup)
         except Exception as exc:  # reported, not fatal
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
                    "sample": f"unavailable: {exc}"}
@@ -364,7 +439,9 @@ def run_ours(args, world, rank, local):
             "hbm_frac_step": BYTES_PER_VS_STEP * N * S / (ms_step / 1e3) / 1e9 / hbm,
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / hbm,
-                         "traffic": traffic,
+                         "traffic": traffic, "traffic_kernel": traffic_kernel,
+                         "traffic_source": "profiles/sweeps_traffic_lod256.json (ncu, one "
+                                           "launch at 256^3 x 10)" if traffic else None,
                          "algorithmic_bytes_per_launch": sweeps_in[dom] * BYTES_PER_VS_SWEEP * N * S},
             "kernel_ms": per,
             "tuned_sweeps": [{"axis": "xyz"[i], "kernel": ["default", "register", "tma", "direct"][k],
@@ -426,9 +503,10 @@ def run_batched(args, world, rank, local):
         bt.add(sv)
     reset()
     t0 = time.perf_counter()
-    bt.tune(dt, STEP_ALL, 3)
+    bt.tune(dt, STEP_ALL, args.batch_trial_steps)
     t_tune = time.perf_counter() - t0
     cfg = bt.get_config()
+    pch = bt.get_persistent_chunk()
     # first call captures the graph; the timed call replays it
     reset()
     t0 = time.perf_counter()
@@ -444,6 +522,28 @@ def run_batched(args, world, rank, local):
         t_batch = max_over_ranks(time.perf_counter() - t0, world)
     groups, kernels = bt.plan()
     mode = bt.get_mode()
+    # every mode with the tuned group budget, for comparison (captured, then
+    # timed on a replay)
+    per_mode = {}
+    if args.batch_modes:
+        from biofvm_b200._abi import BATCH_BRANCHES, BATCH_FUSED, BATCH_PERSISTENT
+        for name, md in (("fused", BATCH_FUSED), ("branches", BATCH_BRANCHES),
+                         ("persistent", BATCH_PERSISTENT)):
+            bt.set_mode(md)
+            reset()
+            bt.step(dt, args.steps, STEP_ALL)
+            bt.synchronize()
+            reset()
+            t0 = time.perf_counter()
+            bt.step(dt, args.steps, STEP_ALL)
+            bt.synchronize()
+            t_m = time.perf_counter() - t0
+            per_mode[name] = {"seconds": t_m, "speedup_vs_looped_plain": t_plain / t_m,
+                              "groups_kernels": list(bt.plan())}
+        bt.set_mode(mode)
+        reset()
+        bt.step(dt, args.steps, STEP_ALL)  # the tuned mode's fields for the check below
+        bt.synchronize()
     err = 0.0
     for sv, ref in zip(sols, plain):
         p = sv.get_densities()
@@ -477,10 +577,12 @@ def run_batched(args, world, rank, local):
                                           t_plain_tuned, "seconds": t_plain_tuned},
             "batched_seconds": t_batch, "speedup_vs_looped_plain": t_plain / t_batch,
             "max_rel_err_vs_looped_plain": err,
-            "tuned": {"mode": ["fused", "branches"][mode], "chunk": cfg[0], "threads": cfg[1],
-                      "group_bytes": cfg[2], "tune_seconds": t_tune},
+            "tuned": {"mode": ["fused", "branches", "persistent"][mode], "chunk": cfg[0],
+                      "threads": cfg[1], "group_bytes": cfg[2], "persistent_chunk": pch,
+                      "tune_seconds": t_tune, "trial_steps": args.batch_trial_steps},
             "graph": {"groups": groups, "kernels_per_call": kernels,
                       "first_call_seconds": t_first},
+            "modes_with_tuned_budget": per_mode,
             "gpu_launches": kernels,
             "clocks": clocks.summary(),
         }
@@ -612,12 +714,22 @@ def run_plain50(args, world, rank, local):
         ms_loop = timed(lambda: sv.step(dt, args.steps, STEP_ALL))
     launches = sv.launch_count - l0
     grid_field = sv.get_densities()
+
+    def one_step_calls():
+        for _ in range(args.steps):
+            sv.step(dt, 1, STEP_ALL)
+
+    # one step per call, as the drop-in's simulate_diffusion_decay calls it
+    l0 = sv.launch_count
+    ms_loop_1 = timed(one_step_calls)
+    launches_1 = sv.launch_count - l0
     # the sweep kernels, launched from the host (seven kernels per step)
     sv.set_grid_steps(False)
     sv.step(dt, 3, STEP_ALL)
     l0 = sv.launch_count
     ms_sweep = timed(lambda: sv.step(dt, args.steps, STEP_ALL))
     sweep_launches = sv.launch_count - l0
+    ms_sweep_1 = timed(one_step_calls)
     ref = sv.get_densities()
     # the same steps in one thread-block cluster (opt-in; bit-exact)
     sv.set_cluster_steps(True)
@@ -677,6 +789,9 @@ def run_plain50(args, world, rank, local):
             "gpu_launches": int(launches),
             "sweep_kernels_host_launched": {"us_per_step": 1e3 * ms_sweep / args.steps,
                                             "launches": int(sweep_launches)},
+            "one_step_per_call": {"bfvm_step_default_us_per_step": 1e3 * ms_loop_1 / args.steps,
+                                  "launches": int(launches_1),
+                                  "sweep_kernels_us_per_step": 1e3 * ms_sweep_1 / args.steps},
             "sweep_kernels_graph": {"us_per_step": 1e6 * t_graph / args.steps,
                                     "kernels_per_call": kernels},
             "cluster_steps_bit_exact": {"us_per_step": 1e3 * ms_cluster / args.steps,
@@ -922,6 +1037,10 @@ def main():
                          "gradients: compute_all_gradient_vectors at 256^3 x 10; lod2d: the "
                          "LOD_2D solver on a 1024^2 x 32 plane")
     ap.add_argument("--instances", type=int, default=64)
+    ap.add_argument("--batch-trial-steps", type=int, default=10,
+                    help="steps per trial run of the batch tuner")
+    ap.add_argument("--batch-modes", action="store_true",
+                    help="batched: also time every batch mode with the tuned group budget")
     args = ap.parse_args()
     if args.workload == "batched" and "--steps" not in sys.argv:
         args.steps = 200
@@ -951,9 +1070,9 @@ def main():
         else:
             run_ours(args, world, rank, local)
     finally:
-        if world > 1:
-            import torch.distributed as dist
+        import torch.distributed as dist
 
+        if dist.is_available() and dist.is_initialized():
             dist.destroy_process_group()
 
 

@@ -145,6 +145,7 @@ struct RowsArgs {
   int64_t tile0;  // tiles tile0 .. ntiles-1 (a slab of rows)
   int64_t ntiles;
   int nchunks;
+  int tpc;        // threads per chunk: R*S, or R*S rounded up to a multiple of 32
   ChunkCoef<CT> cc;
   // (row, chunk) segment lists, as for lod_sweep_kernel
   SegList bulk, cells, dir;
@@ -152,6 +153,12 @@ struct RowsArgs {
   int fuse;
   int* status;
 };
+
+// Bytes from the start of dynamic shared memory to its first 128-byte
+// boundary.
+__device__ __forceinline__ uint32_t smem_pad128(const unsigned char* smem) {
+  return (128u - ((uint32_t)__cvta_generic_to_shared(smem) & 127u)) & 127u;
+}
 
 // ---- the chunk solve shared by both kernels --------------------------------
 
@@ -259,9 +266,10 @@ __global__ void __launch_bounds__(W * MAXNC)
   const int NC = blockDim.y;
   const int npad = a.box_n * a.nboxes;
   const size_t stage_elems = (size_t)npad * W;
-  // tensor copies need 128-B aligned shared-memory destinations
-  T* tiles =
-      reinterpret_cast<T*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~(uintptr_t)127);
+  // tensor copies need 128-B aligned shared-memory destinations; the pad is
+  // added to the shared array itself, so every pointer below stays a
+  // shared-memory pointer to the compiler
+  T* tiles = reinterpret_cast<T*>(smem_raw + smem_pad128(smem_raw));
   Pair<CT>* fold = reinterpret_cast<Pair<CT>*>(tiles + STAGES * stage_elems);  // 2 x [NC][W]
   uint64_t* full = reinterpret_cast<uint64_t*>(fold + 2 * NC * W);
   CT* sm_tab = reinterpret_cast<CT*>(full + 4);  // chunk tables (SMEM_TAB)
@@ -374,18 +382,25 @@ __global__ void __launch_bounds__(MAXT, rows_min_blocks(CH, MAXT))
   const size_t pitch = a.pitch;
   const size_t row_elems = (size_t)n * S;
   const size_t stage_elems = pitch * R;
-  T* tiles =
-      reinterpret_cast<T*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~(uintptr_t)127);
+  // 128-B aligned stages; the pad is added to the shared array itself, so
+  // every pointer below stays a shared-memory pointer to the compiler
+  const uint32_t pad = smem_pad128(smem_raw);
+  T* tiles = reinterpret_cast<T*>(smem_raw + pad);
   Pair<CT>* fold = reinterpret_cast<Pair<CT>*>(tiles + STAGES * stage_elems);  // 2 x [NC][FW]
-  uint64_t* full = reinterpret_cast<uint64_t*>(
-      (reinterpret_cast<uintptr_t>(fold + 2 * NC * FW) + 15) & ~(uintptr_t)15);
+  const size_t full_off =
+      (pad + (STAGES * stage_elems * sizeof(T) + 2 * NC * FW * sizeof(Pair<CT>)) + 15) &
+      ~(size_t)15;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + full_off);
   CT* sm_tab = reinterpret_cast<CT*>(full + 4);  // chunk tables (SMEM_TAB)
   int* sm_slot = reinterpret_cast<int*>(sm_tab + (SMEM_TAB ? a.cc.tab_elems : 0));
 
   const int tid = threadIdx.x;
   const int nthreads = blockDim.x;
-  const int fc = tid % FW;  // column in the tile
-  const int c = tid / FW;   // chunk
+  // a.tpc threads per chunk (FW, or FW rounded up to whole warps so that the
+  // lanes of a warp read one chunk: lanes of two chunks 32*CH*S elements
+  // apart would meet on the same banks); lanes past FW idle
+  const int fc = tid % a.tpc;  // column in the tile
+  const int c = tid / a.tpc;   // chunk
   const int r = fc / S;
   const int s = fc - r * S;
   const int k0 = c * CH;
@@ -472,7 +487,7 @@ __global__ void __launch_bounds__(MAXT, rows_min_blocks(CH, MAXT))
     CT qe, x0;
     chunk_local<SMEM_TAB, CT, CH>(v, lenA, k1, S, qe, x0);
     Pair<CT>* sF = fold + (i & 1) * NC * FW;
-    if (c < NC) st_fold(sF + c * FW + fc, qe, x0);
+    if (c < NC && fc < FW) st_fold(sF + c * FW + fc, qe, x0);
     // every thread has its chunk in registers: the stage can be refilled
     if (__syncthreads_or(!ok)) {
       if (tid == 0) drain_after_failure(full, STAGES, i, issued - i, a.status);

@@ -55,6 +55,7 @@ void choose_axes(bfvm_solver* m) {
       continue;
     m->axis[a].user = false;
     m->axis[a].kind = 0;
+    m->axis[a].stages = 0;
     int ch = (n <= 64) ? 8 : 16;
     if (a > 0 && n >= 128) ch = 32;
     while ((n + ch - 1) / ch > 16 && ch < 32) ch *= 2;
@@ -684,6 +685,7 @@ struct RowsPlan {
   bool ok = false;
   bool smem_tab = false;
   int ch = 0, nc = 0, R = 0, stages = 0, maxt = 256;
+  int tpc = 0;  // threads per chunk
   int64_t pitch = 0;
   size_t smem = 0;
 };
@@ -718,6 +720,9 @@ RowsPlan plan_rows(const bfvm_solver* m) {
   P.pitch = pitch;
   const size_t extra = 8 * 4 + 16 + 128;
   const size_t tab = table_bytes(m, 0);
+  // tiles in the ring: 2, or 3 (one more tile in flight while a tile is
+  // solved) where the axis asks for it
+  const int nst = m->axis[0].stages == 3 ? 3 : 2;
   // Blocks of at most 256 threads (room for each thread's chunk in
   // registers), a 2-stage ring of R rows, the chunk tables in shared memory
   // when they fit; else one block of up to 512 threads.  Half the shared
@@ -734,10 +739,14 @@ RowsPlan plan_rows(const bfvm_solver* m) {
         const size_t stage = (size_t)(R * pitch * es);
         const size_t fold = 4 * (size_t)P.nc * R * m->S * m->math_elem();  // two parities of (qe, x0)
         const size_t t = staged ? tab : 0;
-        const size_t smem = 2 * stage + fold + extra + t;
+        const size_t smem = nst * stage + fold + extra + t;
         if (smem > budget) continue;
         P.R = R;
-        P.stages = 2;
+        // whole warps per chunk when that still fits the block: the lanes
+        // of a warp then read one chunk (two chunks' rows would share banks)
+        const int fw = R * m->S, fw32 = (fw + 31) / 32 * 32;
+        P.tpc = fw32 * P.nc <= maxt ? fw32 : fw;
+        P.stages = nst;
         P.maxt = maxt;
         P.smem_tab = staged != 0;
         P.smem = smem;
@@ -940,9 +949,9 @@ bool launch_direct(bfvm_solver* m, int ax, int fuse, double dt, int64_t z0 = 0,
   return true;
 }
 
-template <typename T, typename CT, int CH, bool TAB, int MAXT>
+template <typename T, typename CT, int CH, bool TAB, int MAXT, int ST>
 void launch_rows_inst(const bfvm::RowsArgs<T, CT>& a, dim3 block, size_t smem, bfvm_solver* m) {
-  auto k = bfvm::lod_rows_tma_kernel<T, CH, 2, TAB, MAXT, CT>;
+  auto k = bfvm::lod_rows_tma_kernel<T, CH, ST, TAB, MAXT, CT>;
   allow_smem((const void*)k, m->device, smem);
   int per_sm = 0;
   BFVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, block.x * block.y, smem));
@@ -951,19 +960,27 @@ void launch_rows_inst(const bfvm::RowsArgs<T, CT>& a, dim3 block, size_t smem, b
   k<<<grid, block, smem, m->stream>>>(a);
 }
 
-template <typename T, typename CT, int CH>
-void launch_rows_ch(const bfvm::RowsArgs<T, CT>& a, const RowsPlan& P, dim3 block, bfvm_solver* m) {
+template <typename T, typename CT, int CH, int ST>
+void launch_rows_st(const bfvm::RowsArgs<T, CT>& a, const RowsPlan& P, dim3 block, bfvm_solver* m) {
   if (P.maxt == 256) {
     if (P.smem_tab)
-      launch_rows_inst<T, CT, CH, true, 256>(a, block, P.smem, m);
+      launch_rows_inst<T, CT, CH, true, 256, ST>(a, block, P.smem, m);
     else
-      launch_rows_inst<T, CT, CH, false, 256>(a, block, P.smem, m);
+      launch_rows_inst<T, CT, CH, false, 256, ST>(a, block, P.smem, m);
   } else {
     if (P.smem_tab)
-      launch_rows_inst<T, CT, CH, true, 512>(a, block, P.smem, m);
+      launch_rows_inst<T, CT, CH, true, 512, ST>(a, block, P.smem, m);
     else
-      launch_rows_inst<T, CT, CH, false, 512>(a, block, P.smem, m);
+      launch_rows_inst<T, CT, CH, false, 512, ST>(a, block, P.smem, m);
   }
+}
+
+template <typename T, typename CT, int CH>
+void launch_rows_ch(const bfvm::RowsArgs<T, CT>& a, const RowsPlan& P, dim3 block, bfvm_solver* m) {
+  if (P.stages == 3)
+    launch_rows_st<T, CT, CH, 3>(a, P, block, m);
+  else
+    launch_rows_st<T, CT, CH, 2>(a, P, block, m);
 }
 
 template <typename T, typename CT>
@@ -998,8 +1015,9 @@ void launch_rows(bfvm_solver* m, const RowsPlan& P, int fuse, double dt, int64_t
   a.cells = m->seg_cells.view();
   a.dir = m->seg_dir_x.view();
   a.status = m->d_status.as<int>();
-  // whole warps: threads past R*S*NC idle through the sweep
-  dim3 block((unsigned)((P.R * m->S * P.nc + 31) / 32 * 32));
+  a.tpc = P.tpc;
+  // whole warps: threads past tpc*NC idle through the sweep
+  dim3 block((unsigned)((P.tpc * P.nc + 31) / 32 * 32));
   switch (P.ch) {
     case 8: launch_rows_ch<T, CT, 8>(a, P, block, m); break;
     case 16: launch_rows_ch<T, CT, 16>(a, P, block, m); break;
@@ -2222,6 +2240,7 @@ int bfvm_set_sweep_config(bfvm_solver* m, int axis, int chunk, int columns, int 
     A.tw = columns;
     A.minb = min_blocks;
     A.kind = 0;
+    A.stages = 0;
     A.user = true;
   });
 }
@@ -2249,7 +2268,7 @@ void tune_sweeps(bfvm_solver* m, double dt, int reps) {
   BFVM_CUDA(cudaEventCreate(&e0));
   BFVM_CUDA(cudaEventCreate(&e1));
   struct Choice {
-    int kind, ch, tw;
+    int kind, ch, tw, stages;
   };
   const int ns[3] = {m->nx, m->ny, m->nz};
   const int fuses[3] = {bfvm::kFuseDirPro | bfvm::kFuseDirEpi, bfvm::kFuseDirEpi, 0};
@@ -2260,10 +2279,14 @@ void tune_sweeps(bfvm_solver* m, double dt, int reps) {
         const int nc = (ns[ax] + ch - 1) / ch;
         if (nc > 64) continue;
         for (int tw : {32, 16, 8})
-          if (nc * tw <= bfvm::sweep_max_threads(ch)) cand.push_back({BFVM_PATH_GENERIC, ch, tw});
+          if (nc * tw <= bfvm::sweep_max_threads(ch))
+            cand.push_back({BFVM_PATH_GENERIC, ch, tw, 0});
         // the line kernel (y, z) also takes 17-32 chunks of 32 points
-        if (nc <= 16 || (ax > 0 && ch == 32 && nc <= 32)) cand.push_back({BFVM_PATH_TMA, ch, 16});
-        if (nc <= 16) cand.push_back({BFVM_PATH_DIRECT, ch, 16});
+        if (nc <= 16 || (ax > 0 && ch == 32 && nc <= 32))
+          cand.push_back({BFVM_PATH_TMA, ch, 16, 0});
+        // the row kernel (x) with a ring of three tiles
+        if (ax == 0 && nc <= 16) cand.push_back({BFVM_PATH_TMA, ch, 16, 3});
+        if (nc <= 16) cand.push_back({BFVM_PATH_DIRECT, ch, 16, 0});
       }
       Axis best = m->axis[ax];
       float best_ms = 1e30f;
@@ -2274,6 +2297,7 @@ void tune_sweeps(bfvm_solver* m, double dt, int reps) {
         A.tw = c.tw;
         A.minb = 1;
         A.kind = c.kind;
+        A.stages = c.stages;
         A.user = true;
         build_all(m);
         sweep(m, ax, fuses[ax], dt);  // warm-up: tables and plans
@@ -2378,6 +2402,7 @@ int bfvm_get_sweep_config(bfvm_solver* m, int axis, int* config) {
     config[0] = m->axis[axis].ch;
     config[1] = m->axis[axis].tw;
     config[2] = m->axis[axis].minb;
+    config[3] = m->axis[axis].stages == 3 ? 3 : 2;
   });
 }
 

@@ -92,6 +92,7 @@ struct Axis {
   int tw = 32;  // columns per block
   int minb = 1; // resident blocks per SM the kernel is compiled for (1 or 2)
   int kind = 0; // kernel under BFVM_PATH_AUTO: 0 = default, else a BFVM_PATH_* value
+  int stages = 0;  // x row kernel: tiles in its shared-memory ring (0 = 2)
   bool user = false;  // set through bfvm_set_sweep_config or the tuner
 };
 

@@ -206,7 +206,7 @@ class Solver:
         for ax in range(3):
             k = ctypes.c_int()
             call("bfvm_get_sweep_kernel", self._h, ax, ctypes.byref(k))
-            cfg = (ctypes.c_int * 3)()
+            cfg = (ctypes.c_int * 4)()
             call("bfvm_get_sweep_config", self._h, ax, cfg)
             out.append((k.value, cfg[0], cfg[1], cfg[2]))
         return out
@@ -222,7 +222,8 @@ class Solver:
         call("bfvm_set_sweep_config", self._h, axis, chunk, columns, min_blocks)
 
     def get_sweep_config(self, axis: int):
-        cfg = (ctypes.c_int * 3)()
+        """(chunk, columns, min_blocks, row-kernel ring stages) of `axis`."""
+        cfg = (ctypes.c_int * 4)()
         call("bfvm_get_sweep_config", self._h, axis, cfg)
         return tuple(cfg)
 

@@ -197,7 +197,8 @@ BFVM_API int bfvm_set_precision(bfvm_solver* m, int precision);
  * default is chosen from the axis length; the autotuner sets this. */
 BFVM_API int bfvm_set_sweep_config(bfvm_solver* m, int axis, int chunk, int columns,
                                    int min_blocks);
-/* config[3] = chunk, columns, min_blocks */
+/* config[4] = chunk, columns, min_blocks, and the tiles in the x row
+ * kernel's shared-memory ring (2, or 3 where the tuner found it faster) */
 /* Which sweep kernels run (all compute the same sweep):
  *   BFVM_PATH_AUTO    (default) the register kernel for x, the TMA-fed
  *                     persistent kernel for y and z where the layout allows

@@ -147,6 +147,8 @@ void adjoint_forward(bfvm_solver* m, double dt, int nsteps, int flags, int k) {
   require(k >= 1, "checkpoint interval must be positive");
   require((flags & ~BFVM_STEP_ALL) == 0, "unknown step flags");
   require(m->S <= 256, "the adjoint supports at most 256 densities");
+  require(m->nx <= 1024 && m->ny <= 1024 && m->nz <= 1024,
+          "the adjoint supports lines of at most 1024 points");
   check_lod_mesh(m);
   if (!m->adj) m->adj = new AdjointTape;
   AdjointTape& T = *m->adj;

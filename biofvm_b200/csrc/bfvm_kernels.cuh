@@ -431,6 +431,43 @@ __global__ void __launch_bounds__(256) gradient_rows_kernel(
   for (int c = threadIdx.x; c < 3 * count; c += 256) out[c] = buf[c];
 }
 
+// Lines longer than the chunked kernels take (more than 1024 points): one
+// thread per (line, density) column runs the reference's Thomas sequence
+// (BioFVM_solvers.cpp:186-200: p_0 /= d_0; p_k = (p_k + c1 p_{k-1}) / d_k;
+// then p_k -= cx_k p_{k+1}), each operation rounded on its own, so the
+// result equals the reference's for an FP64 field.  Consecutive columns are
+// consecutive addresses for the y and z axes (the S densities of consecutive
+// rows for x).  The forward values are stored and read back by the backward
+// pass: two reads and two writes per element.  den, cx: [n][S]; c1: [S].
+template <typename T>
+__global__ void long_line_kernel(T* __restrict__ p, T* __restrict__ out, int64_t col0,
+                                 int64_t ncols, int64_t C, int64_t outer_stride,
+                                 int64_t line_stride, int n, int S,
+                                 const double* __restrict__ den, const double* __restrict__ cx,
+                                 const double* __restrict__ c1v) {
+  const int64_t vcol = col0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (vcol >= ncols) return;
+  const int64_t outer = vcol / C;
+  const int64_t col = vcol - outer * C;
+  const int s = (int)(col % S);
+  const int64_t off = outer * outer_stride + col;
+  const T* q = p + off;
+  T* o = out + off;
+  const double c1 = __ldg(c1v + s);
+  double prev = __ddiv_rn((double)q[0], __ldg(den + s));
+  o[0] = (T)prev;
+  for (int k = 1; k < n; ++k) {
+    prev = __ddiv_rn(__dadd_rn((double)q[k * line_stride], __dmul_rn(c1, prev)),
+                     __ldg(den + (int64_t)k * S + s));
+    o[k * line_stride] = (T)prev;
+  }
+  double next = prev;
+  for (int k = n - 2; k >= 0; --k) {
+    next = __dsub_rn((double)o[k * line_stride], __dmul_rn(__ldg(cx + (int64_t)k * S + s), next));
+    o[k * line_stride] = (T)next;
+  }
+}
+
 template <typename Dst, typename Src>
 __global__ void convert_kernel(Dst* __restrict__ dst, const Src* __restrict__ src, int64_t count) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;

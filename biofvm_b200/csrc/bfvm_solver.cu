@@ -46,6 +46,14 @@ std::vector<int> segment_offsets(int64_t nlines, int nchunks, int ch,
 // register kernel (S >= 4 densities and rows of >= 96 points: 0.85 -> 0.75 ms
 // at 256^3 x 10 FP64, 4.4 -> 2.7 ms at 384^3 x 10, 0.66 -> 0.43 ms at
 // 256^3 x 10 FP32), else the register kernel with CH = 8 or 16.
+// Lines of up to this many points run in the chunked kernels (the chunks of a
+// line in one block); longer lines run in long_line_kernel.
+constexpr int kChunkedMaxN = 1024;
+
+bool long_axis(const bfvm_solver* m, int a) {
+  return (a == 0 ? m->nx : (a == 1 ? m->ny : m->nz)) > kChunkedMaxN;
+}
+
 void choose_axes(bfvm_solver* m) {
   const int ns[3] = {m->nx, m->ny, m->nz};
   for (int a = 0; a < 3; ++a) {
@@ -65,8 +73,13 @@ void choose_axes(bfvm_solver* m) {
                               : bfvm::sweep_max_threads(ch);
     int tw = 32;
     while (tw > 8 && nc * tw > maxt) tw /= 2;
+    if (n > kChunkedMaxN) {  // the long-line kernel runs this axis
+      m->axis[a].ch = 32;
+      m->axis[a].tw = 1;
+      continue;
+    }
     require(nc * tw <= bfvm::sweep_max_threads(ch),
-            "axis with " + std::to_string(n) + " points exceeds the 1024-point line limit");
+            "axis with " + std::to_string(n) + " points: no sweep kernel shape fits");
     m->axis[a].ch = ch;
     m->axis[a].tw = tw;
     if (a == 0 && m->S >= 4 && n >= 96 && (int64_t)m->S * ((n + 31) / 32) <= 256 &&
@@ -1038,7 +1051,77 @@ void with_types(const bfvm_solver* m, F&& f) {
     f(float(), float());
 }
 
+// The FP64 Thomas tables as the reference holds them, per axis den [n][S],
+// cx [n][S], c1 [S] (rebuilt after each Thomas setup): read by the kernels
+// that run the reference's own operation sequence.
+void ensure_exact_tables(bfvm_solver* m) {
+  if (m->cl_tab_ok) return;
+  const int ns[3] = {m->nx, m->ny, m->nz};
+  for (int a = 0; a < 3; ++a) {
+    const size_t nS = (size_t)ns[a] * m->S;
+    std::vector<double> t(2 * nS + m->S);
+    std::copy(m->h_den[a].begin(), m->h_den[a].end(), t.begin());
+    std::copy(m->h_cx[a].begin(), m->h_cx[a].end(), t.begin() + nS);
+    std::copy(m->h_c1[a].begin(), m->h_c1[a].end(), t.begin() + 2 * nS);
+    upload(m->cl_tab[a], t, m->stream);
+  }
+  m->cl_tab_ok = true;
+}
+
+template <typename T>
+void dirichlet_standalone(bfvm_solver* m);
+template <typename T>
+void bulk_standalone(bfvm_solver* m, double dt);
+template <typename T>
+void cells_standalone(bfvm_solver* m);
+
+// A sweep of an axis longer than the chunked kernels take: the parts of the
+// step fused into the chunked sweeps run as their own kernels around it
+// (bulk, cells and the Dirichlet overwrite before, the Dirichlet overwrite
+// after), then long_line_kernel over the axis's columns (planes [z0, z1)
+// for x and y when z1 >= 0).
+template <typename T>
+void long_sweep(bfvm_solver* m, int ax, int fuse, int64_t z0, int64_t z1, double dt) {
+  ensure_exact_tables(m);
+  if (fuse & bfvm::kFuseBulk) bulk_standalone<T>(m, dt);
+  if (fuse & bfvm::kFuseCells) cells_standalone<T>(m);
+  if ((fuse & bfvm::kFuseDirPro) && m->dir_unique > 0) dirichlet_standalone<T>(m);
+  const int64_t S = m->S, nx = m->nx, ny = m->ny, nz = m->nz;
+  const int64_t nzp = (m->lod_dims == 2) ? 1 : nz;  // planes swept
+  int64_t C, os, ls, ncols, col0 = 0;
+  int n;
+  if (ax == 0) {
+    n = (int)nx, C = S, os = nx * S, ls = S, ncols = ny * nzp * S;
+  } else if (ax == 1) {
+    n = (int)ny, C = nx * S, os = nx * ny * S, ls = nx * S, ncols = nzp * nx * S;
+  } else {
+    n = (int)nz, C = nx * ny * S, os = 0, ls = nx * ny * S, ncols = nx * ny * S;
+  }
+  if (z1 >= 0 && ax < 2) {
+    const int64_t per_plane = (ax == 0 ? ny : nx) * S;
+    col0 = z0 * per_plane;
+    ncols = z1 * per_plane;
+  }
+  T* p = m->p.as<T>();
+  T* out = m->sweep_out ? static_cast<T*>(m->sweep_out) : p;
+  const double* t = m->cl_tab[ax].as<double>();
+  const int64_t nS = (int64_t)n * S;
+  if (ncols > col0) {
+    bfvm::long_line_kernel<T><<<(unsigned)blocks_for(ncols - col0, 128), 128, 0, m->stream>>>(
+        p, out, col0, ncols, C, os, ls, n, (int)S, t, t + nS, t + 2 * nS);
+    check_launch(m);
+  }
+  if ((fuse & bfvm::kFuseDirEpi) && m->dir_unique > 0) dirichlet_standalone<T>(m);
+}
+
 void sweep(bfvm_solver* m, int ax, int fuse, double dt, int64_t z0, int64_t z1) {
+  if (long_axis(m, ax)) {
+    if (m->precision == BFVM_FP64)
+      long_sweep<double>(m, ax, fuse, z0, z1, dt);
+    else
+      long_sweep<float>(m, ax, fuse, z0, z1, dt);
+    return;
+  }
   // under AUTO an axis may carry its own kernel choice (bfvm_tune_sweeps)
   const int path =
       (m->path == BFVM_PATH_AUTO && m->axis[ax].kind) ? m->axis[ax].kind : m->path;
@@ -1814,18 +1897,7 @@ int cluster_blocks(const bfvm_solver* m) {
 
 // nsteps whole steps (bulk -> cells -> LOD_3D) in one cluster launch.
 void cluster_run(bfvm_solver* m, double dt, int nsteps, int flags, int cl) {
-  if (!m->cl_tab_ok) {
-    const int ns[3] = {m->nx, m->ny, m->nz};
-    for (int a = 0; a < 3; ++a) {
-      const size_t nS = (size_t)ns[a] * m->S;
-      std::vector<double> t(2 * nS + m->S);
-      std::copy(m->h_den[a].begin(), m->h_den[a].end(), t.begin());
-      std::copy(m->h_cx[a].begin(), m->h_cx[a].end(), t.begin() + nS);
-      std::copy(m->h_c1[a].begin(), m->h_c1[a].end(), t.begin() + 2 * nS);
-      upload(m->cl_tab[a], t, m->stream);
-    }
-    m->cl_tab_ok = true;
-  }
+  ensure_exact_tables(m);
   bfvm::ClusterStepArgs a{};
   a.p = m->p.as<double>();
   a.nx = m->nx;
@@ -2274,6 +2346,7 @@ void tune_sweeps(bfvm_solver* m, double dt, int reps) {
   const int fuses[3] = {bfvm::kFuseDirPro | bfvm::kFuseDirEpi, bfvm::kFuseDirEpi, 0};
   try {
     for (int ax = 0; ax < 3; ++ax) {
+      if (long_axis(m, ax)) continue;  // one kernel runs it
       std::vector<Choice> cand;
       for (int ch : {8, 16, 32}) {
         const int nc = (ns[ax] + ch - 1) / ch;

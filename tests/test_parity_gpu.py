@@ -288,13 +288,70 @@ def test_default_x_kernel_follows_added_densities():
     assert np.all(rel_err(p, ref) <= TOL64)
 
 
-def test_lines_past_the_limit_are_rejected():
+LONG_SHAPES = [(2048, 3, 2), (3, 2048, 2), (2, 3, 2048), (4100, 2, 3), (2, 4100, 2),
+               (3, 2, 4100), (1025, 5, 4)]
+
+
+@pytest.mark.parametrize("shape", LONG_SHAPES, ids=["x2048", "y2048", "z2048", "x4100", "y4100",
+                                                    "z4100", "x1025"])
+@pytest.mark.parametrize("fused", [True, False], ids=["fused", "per_call"])
+def test_lines_longer_than_1024_points(shape, fused):
+    """Axes past the chunked kernels' 1024 points run one thread per column
+    with the reference's own operation sequence: the whole step (bulk,
+    agents, Dirichlet nodes) against the oracle."""
+    scn = W.mixed_small(shape=shape, S=2, n_agents=300, seed=sum(shape) + 3)
+    ref = O.oracle_run(scn, 3, 7)
+    p = run_gpu(scn, 3, 7, fused)
+    assert np.all(rel_err(p, ref) <= TOL64), rel_err(p, ref)
+
+
+def test_long_lines_fp32_and_slabs():
+    """An FP32 field on a 2048-point axis (FP64 arithmetic along it), and the
+    x and y sweeps by slabs of planes with a long x axis."""
+    scn = W.mixed_small(shape=(2048, 4, 6), S=3, n_agents=100, seed=41)
+    ref = O.oracle_run(scn, 3, 7)
     with Solver(0) as sv:
-        sv.resize_densities(1)
+        load_scenario(sv, scn)
+        sv.set_precision(32)
+        sv.set_densities(scn.initial_field())
+        sv.step(scn.dt, 3)
+        assert np.all(rel_err(sv.get_densities(), ref) <= TOL32)
+    with Solver(0) as sv:
+        load_scenario(sv, scn)
+        sv.set_slab_planes(2)
+        sv.step(scn.dt, 3)
+        assert np.all(rel_err(sv.get_densities(), ref) <= TOL64)
+
+
+def test_lod2d_plane_of_2048_squared():
+    """diffusion_decay_solver__constant_coefficients_LOD_2D on a 2048 x 2048
+    plane with Dirichlet nodes: both axes run the long-line kernel, which
+    follows the reference's operation sequence, so the plane equals the
+    oracle's bit for bit."""
+    scn = W.mixed_small(shape=(2048, 2048, 1), S=2, n_agents=0, seed=2048, bulk=False)
+    ref = O.oracle_lod2d_run(scn, 2)
+    with Solver(0) as sv:
+        load_scenario(sv, scn)
+        for _ in range(2):
+            sv.simulate_diffusion_decay_2d(scn.dt)
+        p = sv.get_densities()
+    assert np.array_equal(p, ref)
+
+
+def test_long_lines_tuner_and_adjoint_limits():
+    """The sweep tuner leaves a long axis to its one kernel; the adjoint
+    refuses lines past 1024 points."""
+    scn = W.mixed_small(shape=(1500, 6, 5), S=2, n_agents=50, seed=43)
+    ref = O.oracle_run(scn, 2, 7)
+    with Solver(0) as sv:
+        load_scenario(sv, scn)
+        sv.tune_sweeps(scn.dt, 1)
+        sv.step(scn.dt, 2)
+        assert np.all(rel_err(sv.get_densities(), ref) <= TOL64)
+        from biofvm_b200._abi import call
         with pytest.raises(BfvmError) as e:
-            sv.resize_space(0, 10250, 0, 10, 0, 10, 10)  # 1025 points along x
-        assert "1024-point" in str(e.value)
-        sv.resize_space(0, 10240, 0, 10, 0, 10, 10)  # 1024: accepted
+            call("bfvm_adjoint_forward", sv.handle, scn.dt, 2, 7, 1)
+        assert "1024 points" in str(e.value)
 
 
 @pytest.mark.slow

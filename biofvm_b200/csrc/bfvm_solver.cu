@@ -244,6 +244,7 @@ bfvm::ChunkCoef<T> chunk_view(bfvm_solver* m, int a) {
 
 void build_bulk(bfvm_solver* m) {
   if (!m->bulk_dirty) return;
+  ++m->lists_version;
   cudaStream_t st = m->stream;
   const int S = m->S;
   const int64_t E = (int64_t)m->bulk_vox.size();
@@ -312,6 +313,7 @@ void build_bulk(bfvm_solver* m) {
 
 void build_dirichlet(bfvm_solver* m) {
   if (!m->dir_dirty) return;
+  ++m->lists_version;
   cudaStream_t st = m->stream;
   const int S = m->S;
   // Nodes are applied in list order, so for a repeated voxel the last one
@@ -384,6 +386,7 @@ void build_dirichlet(bfvm_solver* m) {
 // list order, BioFVM_microenvironment.cpp:626-633).
 void build_agents(bfvm_solver* m) {
   if (!m->ag_dirty) return;
+  ++m->lists_version;
   const int64_t A = m->n_agents;
   m->ag_dirty = false;
   if (A == 0) return;
@@ -2040,6 +2043,7 @@ void grid_run(bfvm_solver* m, double dt, int nsteps, int flags, int blocks, int 
   const int64_t lx = N / m->nx, ly = N / m->ny, lz = N / m->nz;
   const size_t field_b = (size_t)N * S * sizeof(double);
   const size_t masks_b = (size_t)(lx + ly + lz) * sizeof(uint64_t);
+  const void* before = m->d_grid_maps.ptr;
   m->d_grid_maps.ensure(field_b + masks_b + (size_t)2 * N * sizeof(int));
   unsigned char* base = m->d_grid_maps.as<unsigned char>();
   double* dir_field = reinterpret_cast<double*>(base);
@@ -2047,11 +2051,19 @@ void grid_run(bfvm_solver* m, double dt, int nsteps, int flags, int blocks, int 
   unsigned long long* my = mx + lx;
   unsigned long long* mz = my + ly;
   int* maps = reinterpret_cast<int*>(base + field_b + masks_b);
-  BFVM_CUDA(cudaMemsetAsync(mx, 0, masks_b, m->stream));
-  BFVM_CUDA(cudaMemsetAsync(maps, 0xFF, (size_t)2 * N * sizeof(int), m->stream));
   const int64_t nbulk = (int64_t)m->bulk_vox.size();
+  // the maps are rebuilt only when a list changed since they were built (or
+  // the buffer moved, or the number of densities changed)
+  const bool rebuild = m->grid_maps_version != m->lists_version || before != m->d_grid_maps.ptr ||
+                       m->grid_maps_S != S;
+  if (rebuild) {
+    BFVM_CUDA(cudaMemsetAsync(mx, 0, masks_b, m->stream));
+    BFVM_CUDA(cudaMemsetAsync(maps, 0xFF, (size_t)2 * N * sizeof(int), m->stream));
+    m->grid_maps_version = m->lists_version;
+    m->grid_maps_S = S;
+  }
   const int64_t most = std::max({nbulk, m->n_agents, m->dir_unique});
-  if (most > 0) {
+  if (rebuild && most > 0) {
     bfvm::grid_maps_kernel<<<(unsigned)blocks_for(most, 256), 256, 0, m->stream>>>(
         maps, maps + N, nbulk, m->d_bulk_vox.as<int64_t>(), m->n_agents,
         m->d_ag_key.as<uint64_t>(), m->dir_unique, m->d_dir_vox.as<int64_t>(),

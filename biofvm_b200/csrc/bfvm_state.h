@@ -216,6 +216,11 @@ struct bfvm_solver {
   // the kernels' resident blocks per SM (0: not queried yet)
   int grid_steps = 1;
   bfvm_rt::DevBuf d_grid_maps;
+  // the device lists change: every rebuild of the bulk, Dirichlet or agent
+  // lists counts one; the grid-steps maps keep the count they were built at
+  int64_t lists_version = 0;
+  int64_t grid_maps_version = -1;
+  int grid_maps_S = 0;
   int grid_per_sm[2] = {0, 0};  // 4- and 8-point chunk kernels (-1: not usable)
   // cached tensor maps of the y and z sweeps (keyed by field pointer)
   CUtensorMap maps[3];

@@ -104,6 +104,8 @@ SIGNATURES = {
     "bfvm_adjoint_forward": (c_int, [_P, c_double, c_int, c_int, c_int]),
     "bfvm_adjoint_backward": (c_int, [_P, c_void_p, c_int, _DP, _DP, _DP, _DP, _DP]),
     "bfvm_adjoint_release": (c_int, [_P]),
+    "bfvm_set_z_slab": (c_int, [_P, c_int, _IP, c_int]),
+    "bfvm_zslab_fixup": (c_int, [_P, c_void_p]),
     "bfvm_batch_create": (c_int, [POINTER(c_void_p), c_int]),
     "bfvm_batch_destroy": (c_int, [_P]),
     "bfvm_batch_add": (c_int, [_P, _P]),

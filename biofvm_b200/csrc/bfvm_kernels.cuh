@@ -468,6 +468,51 @@ __global__ void long_line_kernel(T* __restrict__ p, T* __restrict__ out, int64_t
   }
 }
 
+// Joins the z slabs of a field split by planes over several solvers, after
+// each slab's z sweep ran with zero carries at its ends (x').  One thread
+// per (i, j, density) column of this slab.  planes [R][2][C]: every slab's
+// first and last local plane after its sweep (C = nx*ny*S values each);
+// cst [R][S][3] {P, Gs, R} per slab; pt [nz][S][2] {G, Rk} of this slab's
+// planes.  The forward value entering slab r folds the slabs before it
+// (Q = P Q + last), the solution on the first plane after this slab folds
+// the slabs after it from the far end (X = first + C Gs + R X); then
+// x_k = x'_k + C G_k + X Rk_k on every plane of this slab.
+template <int MAXR>
+__global__ void zslab_fixup_kernel(double* __restrict__ p, int64_t C, int S, int nz, int R,
+                                   int rank, const double* __restrict__ planes,
+                                   const double* __restrict__ cst,
+                                   const double* __restrict__ pt) {
+  const int64_t col = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= C) return;
+  const int s = (int)(col % S);
+  double carry_in[MAXR];
+  double Q = 0.0;
+#pragma unroll
+  for (int r = 0; r < MAXR; ++r) {
+    if (r < R) {
+      carry_in[r] = Q;
+      Q = __ldg(cst + ((int64_t)r * S + s) * 3) * Q + __ldg(planes + ((int64_t)r * 2 + 1) * C + col);
+    }
+  }
+  double X = 0.0;
+#pragma unroll
+  for (int r = MAXR - 1; r >= 0; --r) {
+    if (r < R && r > rank) {
+      const double* k = cst + ((int64_t)r * S + s) * 3;
+      X = __ldg(planes + (int64_t)r * 2 * C + col) + carry_in[r] * __ldg(k + 1) + __ldg(k + 2) * X;
+    }
+  }
+  double Cr = 0.0;
+#pragma unroll
+  for (int r = 0; r < MAXR; ++r)
+    if (r == rank) Cr = carry_in[r];
+  for (int k = 0; k < nz; ++k) {
+    const double* g = pt + ((int64_t)k * S + s) * 2;
+    double* q = p + (int64_t)k * C + col;
+    *q = *q + Cr * __ldg(g) + X * __ldg(g + 1);
+  }
+}
+
 template <typename Dst, typename Src>
 __global__ void convert_kernel(Dst* __restrict__ dst, const Src* __restrict__ src, int64_t count) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;

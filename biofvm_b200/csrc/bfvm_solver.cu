@@ -49,6 +49,8 @@ std::vector<int> segment_offsets(int64_t nlines, int nchunks, int ch,
 // Lines of up to this many points run in the chunked kernels (the chunks of a
 // line in one block); longer lines run in long_line_kernel.
 constexpr int kChunkedMaxN = 1024;
+// most slabs of a z-split field
+constexpr int kZSlabMaxRanks = 64;
 
 bool long_axis(const bfvm_solver* m, int a) {
   return (a == 0 ? m->nx : (a == 1 ? m->ny : m->nz)) > kChunkedMaxN;
@@ -94,6 +96,8 @@ void choose_axes(bfvm_solver* m) {
 }
 
 void clear_state_after_resize(bfvm_solver* m) {
+  m->zs_ranks = 0;  // a z slab is declared again for the new mesh
+  m->zs_bounds.clear();
   m->p.ensure(std::max<size_t>(m->NS() * m->elem(), 16));
   BFVM_CUDA(cudaMemsetAsync(m->p.ptr, 0, m->NS() * m->elem(), m->stream));
   m->setup_done = false;
@@ -116,14 +120,64 @@ void clear_state_after_resize(bfvm_solver* m) {
 // The reference shares one set of Thomas coefficients between its 3-D and
 // 2-D LOD solvers (diffusion_solver_setup_done): whichever runs first fixes
 // them.
+// z slab: the per-density constants that join the slabs of a z-split field
+// (every slab's P = prod a, Gs, R = prod c over its planes) and this slab's
+// per-plane G and Rk, from the global line's slopes a_k = c_k = -cx_k (the
+// forward and backward slopes are the same numbers), in FP64.  With x' the
+// slab-local solve (zero carries at both slab ends) and A_k the product of
+// a over the slab's planes up to k:
+//   G_k = A_k + c_k G_{k+1} (G past the slab 0), Rk_k = prod_{j>=k} c_j,
+//   x_k = x'_k + C G_k + X Rk_k
+// with C the true forward value before the slab and X the true solution on
+// the first plane after it.
+void zslab_tables(bfvm_solver* m, const std::vector<double>& gcx) {
+  const int S = m->S, R = m->zs_ranks, ntot = m->zs_bounds[R];
+  std::vector<double> cst((size_t)R * S * 3), pt((size_t)m->nz * S * 2);
+  for (int r = 0; r < R; ++r) {
+    const int g0 = m->zs_bounds[r], g1 = m->zs_bounds[r + 1];
+    for (int s = 0; s < S; ++s) {
+      auto a = [&](int k) { return -gcx[(size_t)k * S + s]; };
+      auto c = [&](int k) { return k + 1 < ntot ? -gcx[(size_t)k * S + s] : 0.0; };
+      std::vector<double> A(g1 - g0), G(g1 - g0 + 1, 0.0), Rk(g1 - g0 + 1, 1.0);
+      double prod = 1.0;
+      for (int k = g0; k < g1; ++k) A[k - g0] = prod = prod * a(k);
+      for (int k = g1 - 1; k >= g0; --k) {
+        G[k - g0] = A[k - g0] + c(k) * G[k - g0 + 1];
+        Rk[k - g0] = c(k) * Rk[k - g0 + 1];
+      }
+      cst[((size_t)r * S + s) * 3 + 0] = prod;
+      cst[((size_t)r * S + s) * 3 + 1] = G[0];
+      cst[((size_t)r * S + s) * 3 + 2] = Rk[0];
+      if (r == m->zs_rank)
+        for (int k = g0; k < g1; ++k) {
+          pt[((size_t)(k - g0) * S + s) * 2 + 0] = G[k - g0];
+          pt[((size_t)(k - g0) * S + s) * 2 + 1] = Rk[k - g0];
+        }
+    }
+  }
+  upload(m->zs_const, cst, m->stream);
+  upload(m->zs_pt, pt, m->stream);
+}
+
 void thomas_setup(bfvm_solver* m, double dt) {
   const int ns[3] = {m->nx, m->ny, m->nz};
   for (int a = 0; a < 3; ++a) {
     const int n = ns[a], S = m->S;
     std::vector<double> c1(S), den((size_t)n * S), cx((size_t)n * S);
-    // The reference uses mesh.dx for every axis (BioFVM_solvers.cpp:112-113).
-    bfvm::thomas_axis(n, S, m->dx, dt, m->D.data(), m->decay.data(), c1.data(), den.data(),
-                      cx.data(), m->lod_dims);
+    if (a == 2 && m->zs_ranks > 0) {
+      // a z slab: the rows of the whole line's coefficients for its planes
+      const int ntot = m->zs_bounds[m->zs_ranks], z0 = m->zs_bounds[m->zs_rank];
+      std::vector<double> gden((size_t)ntot * S), gcx((size_t)ntot * S);
+      bfvm::thomas_axis(ntot, S, m->dx, dt, m->D.data(), m->decay.data(), c1.data(),
+                        gden.data(), gcx.data(), m->lod_dims);
+      std::copy(gden.begin() + (size_t)z0 * S, gden.begin() + (size_t)(z0 + n) * S, den.begin());
+      std::copy(gcx.begin() + (size_t)z0 * S, gcx.begin() + (size_t)(z0 + n) * S, cx.begin());
+      zslab_tables(m, gcx);
+    } else {
+      // The reference uses mesh.dx for every axis (BioFVM_solvers.cpp:112-113).
+      bfvm::thomas_axis(n, S, m->dx, dt, m->D.data(), m->decay.data(), c1.data(), den.data(),
+                        cx.data(), m->lod_dims);
+    }
     std::vector<double> tab((size_t)3 * n * S + S);
     for (size_t i = 0; i < (size_t)n * S; ++i) {
       const int s = (int)(i % S);
@@ -2132,6 +2186,9 @@ int bfvm_get_cluster_steps(bfvm_solver* m, int* blocks) {
 int bfvm_step(bfvm_solver* m, double dt, int nsteps, int flags) {
   return SOLVER_CALL(m, {
     require(nsteps >= 0, "negative step count");
+    require(m->zs_ranks == 0 || nsteps <= 1 || !(flags & BFVM_STEP_DIFFUSION),
+            "a z slab takes one diffusion step per call (bfvm_zslab_fixup joins the slabs "
+            "after each)");
     require((flags & ~BFVM_STEP_ALL) == 0, "unknown step flags");
     if (!(flags & BFVM_STEP_DIFFUSION)) {
       // No sweep to fuse into: the per-voxel kernels alone.
@@ -2209,6 +2266,51 @@ int bfvm_device_gradients(bfvm_solver* m, void** ptr) {
     require(ptr != nullptr, "null output pointer");
     ensure_gradients(m);
     *ptr = m->d_grad.ptr;
+  });
+}
+
+int bfvm_set_z_slab(bfvm_solver* m, int nranks, const int* bounds, int rank) {
+  return SOLVER_CALL(m, {
+    require(nranks >= 0 && nranks <= kZSlabMaxRanks,
+            "nranks must be in [0, " + std::to_string(kZSlabMaxRanks) + "]");
+    if (nranks == 0) {
+      m->zs_ranks = 0;
+      m->zs_bounds.clear();
+      m->setup_done = false;
+      return;
+    }
+    require(bounds != nullptr && rank >= 0 && rank < nranks, "bad arguments");
+    require(bounds[0] == 0, "the first slab starts at plane 0");
+    for (int r = 0; r < nranks; ++r)
+      require(bounds[r + 1] > bounds[r], "every slab holds at least one plane");
+    require(bounds[rank + 1] - bounds[rank] == m->nz,
+            "this solver's mesh must have its slab's " +
+                std::to_string(bounds[rank + 1] - bounds[rank]) + " planes (it has " +
+                std::to_string(m->nz) + ")");
+    m->zs_ranks = nranks;
+    m->zs_rank = rank;
+    m->zs_bounds.assign(bounds, bounds + nranks + 1);
+    m->setup_done = false;  // the z coefficients are the whole line's rows
+  });
+}
+
+int bfvm_zslab_fixup(bfvm_solver* m, const double* planes) {
+  return SOLVER_CALL(m, {
+    require(m->zs_ranks > 0, "not a z slab (bfvm_set_z_slab)", BFVM_ERR_STATE);
+    require(m->setup_done, "no step ran yet", BFVM_ERR_STATE);
+    require(m->precision == BFVM_FP64, "z slabs are FP64", BFVM_ERR_STATE);
+    require(planes != nullptr, "null planes");
+    const int64_t C = (int64_t)m->nx * m->ny * m->S;
+    const unsigned grid = (unsigned)blocks_for(C, 128);
+    const double* cst = m->zs_const.as<double>();
+    const double* pt = m->zs_pt.as<double>();
+    if (m->zs_ranks <= 8)
+      bfvm::zslab_fixup_kernel<8><<<grid, 128, 0, m->stream>>>(
+          m->p.as<double>(), C, m->S, m->nz, m->zs_ranks, m->zs_rank, planes, cst, pt);
+    else
+      bfvm::zslab_fixup_kernel<kZSlabMaxRanks><<<grid, 128, 0, m->stream>>>(
+          m->p.as<double>(), C, m->S, m->nz, m->zs_ranks, m->zs_rank, planes, cst, pt);
+    check_launch(m);
   });
 }
 

@@ -227,6 +227,17 @@ struct bfvm_solver {
   const void* map_key[3] = {nullptr, nullptr, nullptr};
   int map_w[3] = {0, 0, 0};
 
+  // z slab of a field split by z planes over several solvers (one per GPU):
+  // this solver holds global planes [zs_bounds[zs_rank], zs_bounds[zs_rank+1])
+  // of zs_bounds[zs_ranks] planes (zs_ranks = 0: not split).  Its z sweep
+  // uses the global line's Thomas rows for its planes; bfvm_zslab_fixup
+  // joins the slabs with the per-density constants of every slab
+  // (zs_const [ranks][S][3]: P, Gs, R) and of its own planes
+  // (zs_pt [nz][S][2]: G, Rk), built with the Thomas set-up.
+  int zs_ranks = 0, zs_rank = 0;
+  std::vector<int> zs_bounds;
+  bfvm_rt::DevBuf zs_const, zs_pt;
+
   // gradient vectors [N][S][3] FP64 (allocated and zeroed on first use)
   bfvm_rt::DevBuf d_grad;
 

@@ -179,6 +179,25 @@ BFVM_API int bfvm_apply_dirichlet_conditions(bfvm_solver* m);
  * kernels per step; flags selects the parts (BFVM_STEP_*). */
 BFVM_API int bfvm_step(bfvm_solver* m, double dt, int nsteps, int flags);
 
+/* ---- one field split by z planes over several solvers (no counterpart in
+ * the reference, which holds a Microenvironment in one process) ----------
+ *
+ * The solver's mesh holds planes [bounds[rank], bounds[rank+1]) of a field
+ * of bounds[nranks] planes (bounds[0] = 0; every slab at least one plane;
+ * its mesh must have bounds[rank+1] - bounds[rank] planes along z).  x and y
+ * lines lie in one plane and are solved by the slab alone; the z sweep of a
+ * bfvm_step solves the slab's segment of every z line with the whole line's
+ * Thomas rows and zero carries at the slab's ends.  After each step, every
+ * slab's first and last plane are gathered from every solver (an all-gather
+ * over NCCL by the caller) into a device array planes [nranks][2][nx*ny*S]
+ * (first plane, then last, per slab, in rank order), and bfvm_zslab_fixup
+ * joins the slabs: the result equals the unsplit solve to rounding.  A slab
+ * steps one diffusion step per bfvm_step call.  nranks = 0 ends the split;
+ * a resize ends it too.  FP64 fields; at most 64 slabs.  Call before the
+ * first step (the Thomas set-up is redone). */
+BFVM_API int bfvm_set_z_slab(bfvm_solver* m, int nranks, const int* bounds, int rank);
+BFVM_API int bfvm_zslab_fixup(bfvm_solver* m, const double* planes);
+
 /* The reference computes the Thomas coefficients on the first diffusion call
  * and never again (diffusion_solver_setup_done, BioFVM_solvers.cpp:87,172),
  * so later changes of dt, D or decay are ignored.  This keeps that behaviour

@@ -37,6 +37,7 @@ FP32_FP64MATH = 3264
 
 BATCH_FUSED = 0
 BATCH_BRANCHES = 1
+BATCH_PERSISTENT = 2
 
 _P = c_void_p  # opaque solver handle
 _DP = POINTER(c_double)
@@ -117,6 +118,8 @@ SIGNATURES = {
     "bfvm_batch_get_config": (c_int, [_P, _IP, _IP, _LP]),
     "bfvm_batch_set_mode": (c_int, [_P, c_int]),
     "bfvm_batch_get_mode": (c_int, [_P, _IP]),
+    "bfvm_batch_set_persistent_chunk": (c_int, [_P, c_int]),
+    "bfvm_batch_get_persistent_chunk": (c_int, [_P, _IP]),
     "bfvm_batch_get_plan": (c_int, [_P, _IP, _LP]),
     "bfvm_batch_synchronize": (c_int, [_P]),
 }

@@ -3,9 +3,10 @@
 
 ``Batch.step(dt, n, flags)`` has the effect of ``Solver.step(dt, n, flags)``
 on every member; the members are packed into L2-sized groups and the whole
-run is one CUDA-graph replay, either one launch per phase over a group
-(``BATCH_FUSED``) or every member's own kernels on concurrent graph branches
-(``BATCH_BRANCHES``).  The reference has no such object: its drivers
+run is one CUDA-graph replay: one launch per phase over a group
+(``BATCH_FUSED``), every member's own kernels on concurrent graph branches
+(``BATCH_BRANCHES``), or all steps of a group's members in one persistent
+cooperative launch (``BATCH_PERSISTENT``).  The reference has no such object: its drivers
 loop over Microenvironment instances one by one.
 """
 from __future__ import annotations
@@ -74,10 +75,20 @@ class Batch:
         return tuple(ch), tuple(th), gb.value
 
     def set_mode(self, mode: int) -> None:
-        """BATCH_FUSED (one launch per phase over a group's members) or
+        """BATCH_FUSED (one launch per phase over a group's members),
         BATCH_BRANCHES (every member's own kernels on concurrent graph
-        branches)."""
+        branches) or BATCH_PERSISTENT (all steps of a group's members in one
+        persistent cooperative launch)."""
         call("bfvm_batch_set_mode", self._h, mode)
+
+    def set_persistent_chunk(self, chunk: int) -> None:
+        """Points per chunk of the persistent kernel: 8 or 16."""
+        call("bfvm_batch_set_persistent_chunk", self._h, chunk)
+
+    def get_persistent_chunk(self) -> int:
+        c = ctypes.c_int()
+        call("bfvm_batch_get_persistent_chunk", self._h, ctypes.byref(c))
+        return c.value
 
     def get_mode(self) -> int:
         m = ctypes.c_int()

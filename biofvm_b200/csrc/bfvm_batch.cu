@@ -40,6 +40,7 @@
 
 #include "bfvm.h"
 #include "bfvm_batch_kernels.cuh"
+#include "bfvm_kernels_batch_steps.cuh"
 #include "bfvm_state.h"
 
 namespace bfvm_rt {
@@ -50,6 +51,7 @@ struct BatchConfig {
   int threads[3] = {0, 0, 0};  // 0 = choose
   int64_t group_bytes = -1;    // -1 = default (half of L2), 0 = one group
   int mode = BFVM_BATCH_FUSED;
+  int pch = 8;                 // persistent mode: points per chunk (8 or 16)
 };
 
 // Device descriptors of one group, all in one buffer.
@@ -59,6 +61,22 @@ struct GroupPlan {
   int n_sweep[3] = {0, 0, 0}, n_bulk = 0, n_cells = 0, n_dir = 0;
   int64_t items[3] = {0, 0, 0};
   int64_t work_bulk = 0, work_cells = 0, work_dir = 0;
+  // persistent mode: the group runs as one cooperative launch over the member
+  // descriptors at off_members (0: the group's members run on branches)
+  int persistent = 0;
+  size_t off_members = 0;
+  int n_members = 0;
+  int64_t ptiles[3] = {0, 0, 0};
+  int64_t src_items = 0;
+};
+
+// Per-member scratch of the persistent mode: voxel maps, source and
+// Dirichlet line masks, Dirichlet values at their places.
+struct MemberScratch {
+  DevBuf buf;
+  size_t maps_bytes = 0;   // bulk_map + ag_map, set to -1 before each call
+  size_t masks_off = 0, masks_bytes = 0;  // src, x, y, z masks, set to 0
+  size_t dir_off = 0;      // dir_field (when the member has Dirichlet nodes)
 };
 
 }  // namespace
@@ -77,6 +95,13 @@ struct bfvm_batch {
   std::vector<std::vector<bfvm_solver*>> group_members;  // per group, in plan order
   int ch[3] = {16, 16, 16}, threads[3] = {256, 256, 256};
   bfvm_rt::DevBuf d_desc;
+  // persistent mode: per member scratch (parallel to inst), per group the
+  // host copies of the member descriptors, resident blocks per SM of the
+  // 8- and 16-point kernels (0: not queried), SMs
+  std::vector<bfvm_rt::MemberScratch> scratch;
+  std::vector<std::vector<bfvm::StepMember>> pmembers;
+  int p_per_sm[2] = {0, 0};
+  int num_sms = 0;
   // cached graph and what it was captured for
   cudaGraphExec_t exec = nullptr;
   std::string key;
@@ -168,13 +193,15 @@ BatchSweep<T> sweep_desc(const bfvm_solver* m, int a, int ch, int threads, int64
 // in decreasing size (a single instance larger than the budget is a group
 // of its own): small instances share groups, so that a group's members can
 // run side by side.  Members are independent, so the order is free.
-std::vector<std::vector<bfvm_solver*>> make_groups(const bfvm_batch* b, int64_t budget) {
+std::vector<std::vector<bfvm_solver*>> make_groups(const std::vector<bfvm_solver*>& inst,
+                                                   int64_t budget) {
   std::vector<std::vector<bfvm_solver*>> g;
+  if (inst.empty()) return g;
   if (budget <= 0) {
-    g.push_back(b->inst);
+    g.push_back(inst);
     return g;
   }
-  std::vector<bfvm_solver*> order(b->inst);
+  std::vector<bfvm_solver*> order(inst);
   auto bytes = [](const bfvm_solver* m) { return (int64_t)(m->NS() * m->elem()); };
   std::stable_sort(order.begin(), order.end(),
                    [&](const bfvm_solver* x, const bfvm_solver* y) { return bytes(x) > bytes(y); });
@@ -192,18 +219,126 @@ std::vector<std::vector<bfvm_solver*>> make_groups(const bfvm_batch* b, int64_t 
   return g;
 }
 
+// Whether a member can run in the persistent mode's kernel: FP64 field,
+// lines of at most 128 points.
+bool persistent_ok(const bfvm_solver* m) {
+  return m->precision == BFVM_FP64 && m->nx <= kBatchStepsMaxN && m->ny <= kBatchStepsMaxN &&
+         m->nz <= kBatchStepsMaxN;
+}
+
+size_t round256(size_t x) { return (x + 255) / 256 * 256; }
+
+// The persistent mode's descriptor of member m (device pointers into its
+// scratch, which is sized here), with its first work items in each phase.
+bfvm::StepMember step_member(bfvm_batch* b, bfvm_solver* m, int flags, int ch,
+                             const int64_t* tile0, int64_t src0) {
+  const size_t k = std::find(b->inst.begin(), b->inst.end(), m) - b->inst.begin();
+  if (b->scratch.size() < b->inst.size()) b->scratch.resize(b->inst.size());
+  MemberScratch& sc = b->scratch[k];
+  const int64_t N = m->N();
+  const int64_t lx = N / m->nx, ly = N / m->ny, lz = N / m->nz;
+  sc.maps_bytes = round256((size_t)2 * N * sizeof(int));
+  sc.masks_off = sc.maps_bytes;
+  sc.masks_bytes = round256((size_t)2 * (lz + lx + ly + lz) * sizeof(unsigned long long));
+  sc.dir_off = sc.masks_off + sc.masks_bytes;
+  const size_t dir_bytes = m->dir_unique > 0 ? (size_t)N * m->S * sizeof(double) : 0;
+  sc.buf.ensure(sc.dir_off + std::max<size_t>(dir_bytes, 256));
+  unsigned char* base = sc.buf.as<unsigned char>();
+  auto* masks = reinterpret_cast<unsigned long long*>(base + sc.masks_off);
+
+  bfvm::StepMember d;
+  std::memset(&d, 0, sizeof d);  // the bytes also key the graph cache
+  d.p = m->p.as<double>();
+  d.nx = m->nx;
+  d.ny = m->ny;
+  d.nz = m->nz;
+  d.S = m->S;
+  const int ns[3] = {m->nx, m->ny, m->nz};
+  for (int a = 0; a < 3; ++a) {
+    d.nc[a] = (ns[a] + ch - 1) / ch;
+    d.tw[a] = kBatchStepsThreads / d.nc[a];
+    d.ncols[a] = N / ns[a] * m->S;
+    d.tile0[a] = tile0[a];
+    d.coef[a] = coef_view<double>(m, a);
+  }
+  d.bulk = (flags & BFVM_STEP_BULK) && !m->bulk_vox.empty();
+  d.cells = (flags & BFVM_STEP_CELLS) && m->n_agents > 0;
+  d.dirichlet = m->dir_unique > 0;
+  d.src0 = src0;
+  d.nsrc = ((d.bulk ? (int64_t)m->bulk_vox.size() : 0) + (d.cells ? m->n_agents : 0)) * m->S;
+  d.bulk_map = reinterpret_cast<const int*>(base);
+  d.ag_map = d.bulk_map + N;
+  d.src_mask = masks;
+  d.dir_mask[0] = masks + 2 * lz;
+  d.dir_mask[1] = masks + 2 * (lz + lx);
+  d.dir_mask[2] = masks + 2 * (lz + lx + ly);
+  d.dir_field = reinterpret_cast<const double*>(base + sc.dir_off);
+  d.nbulk = (int64_t)m->bulk_vox.size();
+  d.bulk_vox = m->d_bulk_vox.as<int64_t>();
+  if (m->bulk_rows > 0) {  // shared rate rows: [rows][S][2]
+    d.st = m->d_bulk_tab.as<double>();
+    d.su = d.st + 1;
+    d.rs = 2;
+    d.bulk_row = m->d_bulk_row.as<int>();
+  } else {
+    d.st = m->d_bulk_st.as<double>();
+    d.su = m->d_bulk_su.as<double>();
+    d.rs = 1;
+    d.bulk_row = nullptr;
+  }
+  d.nagents = m->n_agents;
+  d.ag_key = m->d_ag_key.as<uint64_t>();
+  d.ag_idx = m->d_ag_idx.as<int>();
+  d.ag_t1 = m->d_ag_t1.as<double>();
+  d.ag_t2 = m->d_ag_t2.as<double>();
+  return d;
+}
+
 template <typename T>
-void build_plan(bfvm_batch* b) {
+void build_plan(bfvm_batch* b, int flags) {
   const int64_t budget = b->cfg.group_bytes < 0 ? (int64_t)b->l2_bytes / 2 : b->cfg.group_bytes;
-  auto groups = make_groups(b, budget);
+  // persistent mode (FP64, whole steps): the members its kernel can run form
+  // groups of their own, run first; the others run on branches
+  std::vector<bfvm_solver*> pers, rest;
+  const bool persistent = b->cfg.mode == BFVM_BATCH_PERSISTENT && sizeof(T) == sizeof(double) &&
+                          (flags & BFVM_STEP_DIFFUSION);
+  for (bfvm_solver* m : b->inst) (persistent && persistent_ok(m) ? pers : rest).push_back(m);
+  auto pgroups = make_groups(pers, budget);
+  const size_t n_pers = pgroups.size();
+  auto groups = pgroups;
+  for (auto& g : make_groups(rest, budget)) groups.push_back(g);
   std::vector<unsigned char>& buf = b->host_desc;
   buf.clear();
   b->groups.clear();
+  b->pmembers.clear();
   b->group_members = groups;
-  for (auto& members : groups) {
+  for (size_t gi = 0; gi < groups.size(); ++gi) {
+    auto& members = groups[gi];
     GroupPlan G;
     std::memset(&G, 0, sizeof G);
     for (bfvm_solver* m : members) G.field_bytes += (int64_t)(m->NS() * m->elem());
+    if (gi < n_pers) {
+      G.persistent = 1;
+      const int ch = b->cfg.pch;
+      std::vector<bfvm::StepMember> ds;
+      int64_t tile0[3] = {0, 0, 0}, src0 = 0;
+      for (bfvm_solver* m : members) {
+        bfvm::StepMember d = step_member(b, m, flags, ch, tile0, src0);
+        for (int a = 0; a < 3; ++a) tile0[a] += (d.ncols[a] + d.tw[a] - 1) / d.tw[a];
+        src0 += d.nsrc;
+        ds.push_back(d);
+      }
+      align_to(buf, 64);
+      G.off_members = buf.size();
+      for (const auto& d : ds) append(buf, d);
+      G.n_members = (int)ds.size();
+      for (int a = 0; a < 3; ++a) G.ptiles[a] = tile0[a];
+      G.src_items = src0;
+      b->pmembers.push_back(ds);
+      b->groups.push_back(G);
+      continue;
+    }
+    b->pmembers.emplace_back();
     for (int a = 0; a < 3; ++a) {
       align_to(buf, 64);
       G.off_sweep[a] = buf.size();
@@ -314,6 +449,95 @@ void enqueue_group_step(bfvm_batch* b, const GroupPlan& G, double dt, int flags,
   }
 }
 
+// Resident blocks per SM of the persistent kernel with ch-point chunks
+// (queried once per batch).
+int persistent_per_sm(bfvm_batch* b, int ch) {
+  const int i = ch == 8 ? 0 : 1;
+  if (b->p_per_sm[i] == 0) {
+    int coop = 0;
+    BFVM_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, b->device));
+    require(coop != 0, "batch: the device cannot launch cooperative kernels", BFVM_ERR_CUDA);
+    BFVM_CUDA(cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, b->device));
+    const void* k = ch == 8 ? (const void*)batch_steps_kernel<8> : (const void*)batch_steps_kernel<16>;
+    int per = 0;
+    BFVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per, k, kBatchStepsThreads, 4 * kBatchStepsThreads * sizeof(double)));
+    require(per > 0, "batch: the persistent kernel cannot be resident", BFVM_ERR_CUDA);
+    b->p_per_sm[i] = per;
+  }
+  return b->p_per_sm[i];
+}
+
+// Blocks of a persistent group's launch: enough for the widest phase, at
+// most one wave of resident blocks (every block must be resident).
+int persistent_blocks(bfvm_batch* b, const GroupPlan& G) {
+  const int64_t wave = (int64_t)persistent_per_sm(b, b->cfg.pch) * b->num_sms;
+  int64_t want = (G.src_items + kBatchStepsThreads - 1) / kBatchStepsThreads;
+  for (int a = 0; a < 3; ++a) want = std::max(want, G.ptiles[a]);
+  return (int)std::max<int64_t>(1, std::min(want, wave));
+}
+
+// A persistent group: every member's maps, then all nsteps steps of all
+// members in one cooperative launch.
+void enqueue_persistent_group(bfvm_batch* b, size_t gi, double dt, int nsteps,
+                              int64_t* kernels) {
+  const GroupPlan& G = b->groups[gi];
+  const std::vector<bfvm_solver*>& members = b->group_members[gi];
+  const std::vector<bfvm::StepMember>& ds = b->pmembers[gi];
+  bool sources = false;
+  for (size_t k = 0; k < members.size(); ++k) {
+    bfvm_solver* m = members[k];
+    const bfvm::StepMember& d = ds[k];
+    const size_t idx = std::find(b->inst.begin(), b->inst.end(), m) - b->inst.begin();
+    MemberScratch& sc = b->scratch[idx];
+    unsigned char* base = sc.buf.as<unsigned char>();
+    sources = sources || d.bulk || d.cells;
+    if (!d.bulk && !d.cells && !d.dirichlet) continue;
+    BFVM_CUDA(cudaMemsetAsync(base, 0xFF, sc.maps_bytes, b->stream));
+    BFVM_CUDA(cudaMemsetAsync(base + sc.masks_off, 0, sc.masks_bytes, b->stream));
+    const int64_t most = std::max({d.bulk ? d.nbulk : 0, d.cells ? d.nagents : 0, m->dir_unique});
+    if (most == 0) continue;
+    bfvm::StepMember dm = d;
+    if (!d.bulk) dm.nbulk = 0;
+    if (!d.cells) dm.nagents = 0;
+    batch_maps_kernel<<<(unsigned)blocks_for(most, 256), 256, 0, b->stream>>>(
+        dm, m->d_dir_vox.as<int64_t>(), m->d_dir_val.as<double>(), m->dir_unique,
+        reinterpret_cast<int*>(base), reinterpret_cast<int*>(base) + m->N(),
+        const_cast<unsigned long long*>(d.src_mask), const_cast<unsigned long long*>(d.dir_mask[0]),
+        const_cast<unsigned long long*>(d.dir_mask[1]),
+        const_cast<unsigned long long*>(d.dir_mask[2]), const_cast<double*>(d.dir_field));
+    BFVM_CUDA(cudaGetLastError());
+    ++*kernels;
+  }
+  bfvm::BatchStepsArgs a;
+  std::memset(&a, 0, sizeof a);
+  a.mem = reinterpret_cast<const bfvm::StepMember*>(b->d_desc.as<unsigned char>() + G.off_members);
+  a.nmem = G.n_members;
+  for (int ax = 0; ax < 3; ++ax) a.tiles[ax] = G.ptiles[ax];
+  a.src_items = G.src_items;
+  a.nsteps = nsteps;
+  a.dt = dt;
+  a.sources = sources ? 1 : 0;
+  const int blocks = persistent_blocks(b, G);
+  const size_t smem = 4 * kBatchStepsThreads * sizeof(double);
+  cudaLaunchConfig_t cfg;
+  std::memset(&cfg, 0, sizeof cfg);
+  cfg.gridDim = dim3((unsigned)blocks);
+  cfg.blockDim = dim3(kBatchStepsThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = b->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (b->cfg.pch == 8)
+    BFVM_CUDA(cudaLaunchKernelEx(&cfg, batch_steps_kernel<8>, a));
+  else
+    BFVM_CUDA(cudaLaunchKernelEx(&cfg, batch_steps_kernel<16>, a));
+  ++*kernels;
+}
+
 // Makes every instance ready for a step (Thomas setup from this dt when not
 // yet done, lists on the device) and orders the batch stream after the work
 // already queued on the instances' own streams.
@@ -337,12 +561,12 @@ void release_instances(bfvm_batch* b) {
 
 bool fp64(const bfvm_batch* b) { return b->inst.empty() || b->inst[0]->precision == BFVM_FP64; }
 
-void plan(bfvm_batch* b) {
+void plan(bfvm_batch* b, int flags) {
   choose_shapes(b);
   if (fp64(b))
-    build_plan<double>(b);
+    build_plan<double>(b, flags);
   else
-    build_plan<float>(b);
+    build_plan<float>(b, flags);
   b->d_desc.ensure(std::max<size_t>(b->host_desc.size(), 64));
   BFVM_CUDA(cudaMemcpyAsync(b->d_desc.ptr, b->host_desc.data(), b->host_desc.size(),
                             cudaMemcpyHostToDevice, b->stream));
@@ -376,7 +600,12 @@ void enqueue_instance_step(bfvm_solver* m, double dt, int flags, int axes) {
 // on first use (coefficient and chunk tables, kernel attributes) exists
 // before the capture, which must not upload or synchronise.
 void warm_instances(bfvm_batch* b, double dt, int flags) {
-  for (bfvm_solver* m : b->inst) {
+  std::vector<bfvm_solver*> on_branches;
+  for (size_t gi = 0; gi < b->groups.size(); ++gi)
+    if (!b->groups[gi].persistent)
+      on_branches.insert(on_branches.end(), b->group_members[gi].begin(),
+                         b->group_members[gi].end());
+  for (bfvm_solver* m : on_branches) {
     const size_t bytes = m->NS() * m->elem();
     if (bytes == 0) continue;
     DevBuf save;
@@ -394,12 +623,19 @@ cudaGraphExec_t capture(bfvm_batch* b, double dt, int nsteps, int flags, int axe
                         int64_t* kernels) {
   *kernels = 0;
   cudaGraph_t graph = nullptr;
-  const bool branches = b->cfg.mode == BFVM_BATCH_BRANCHES;
+  // branch mode, and the persistent mode's groups that its kernel cannot run
+  const bool branches =
+      b->cfg.mode == BFVM_BATCH_BRANCHES || b->cfg.mode == BFVM_BATCH_PERSISTENT;
   if (branches) warm_instances(b, dt, flags);
   BFVM_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
   try {
     for (size_t gi = 0; gi < b->groups.size(); ++gi) {
       const GroupPlan& G = b->groups[gi];
+      if (G.persistent) {
+        if (axes != 7) throw Error(BFVM_ERR_STATE, "persistent groups run whole steps");
+        enqueue_persistent_group(b, gi, dt, nsteps, kernels);
+        continue;
+      }
       if (branches) {
         // fork: every member's own stream joins the capture after the work
         // captured so far; join: the batch stream waits for every member
@@ -445,9 +681,10 @@ std::string plan_key(const bfvm_batch* b, double dt, int nsteps, int flags) {
   k.append(reinterpret_cast<const char*>(b->ch), sizeof b->ch);
   k.append(reinterpret_cast<const char*>(b->threads), sizeof b->threads);
   k.append(reinterpret_cast<const char*>(&b->cfg.mode), sizeof b->cfg.mode);
-  // branch mode bakes each member's own kernel choices and device buffers
-  // into the graph
-  if (b->cfg.mode == BFVM_BATCH_BRANCHES)
+  k.append(reinterpret_cast<const char*>(&b->cfg.pch), sizeof b->cfg.pch);
+  // branch mode (and the persistent mode's groups on branches) bakes each
+  // member's own kernel choices and device buffers into the graph
+  if (b->cfg.mode == BFVM_BATCH_BRANCHES || b->cfg.mode == BFVM_BATCH_PERSISTENT)
     for (const bfvm_solver* m : b->inst) {
       for (int a = 0; a < 3; ++a) {
         const Axis& A = m->axis[a];
@@ -493,7 +730,7 @@ void batch_step(bfvm_batch* b, double dt, int nsteps, int flags) {
   require((flags & ~BFVM_STEP_ALL) == 0, "unknown step flags");
   if (b->inst.empty() || nsteps == 0) return;
   prepare_instances(b, dt);
-  plan(b);
+  plan(b, flags);
   const std::string key = plan_key(b, dt, nsteps, flags);
   if (!b->exec || key != b->key) {
     drop_graph(b);
@@ -568,9 +805,10 @@ void batch_tune(bfvm_batch* b, double dt, int flags, int trial_steps) {
         for (int th : {128, 256, 512}) {
           if (!config_fits(b, a, ch, th)) continue;
           b->cfg = best;
+          b->cfg.mode = BFVM_BATCH_FUSED;  // the shapes are the fused kernels'
           b->cfg.ch[a] = ch;
           b->cfg.threads[a] = th;
-          plan(b);
+          plan(b, BFVM_STEP_DIFFUSION);
           const float ms = time_graph(b, dt, trial_steps, BFVM_STEP_DIFFUSION, 1 << a);
           if (ms < best_ms) {
             best_ms = ms;
@@ -585,26 +823,38 @@ void batch_tune(bfvm_batch* b, double dt, int flags, int trial_steps) {
       BFVM_CUDA(cudaStreamSynchronize(b->stream));
       tune_sweeps(m, dt, 3);
     }
-    // 3. the mode and the group budget, whole steps
+    // 3. the mode (and the persistent kernel's chunk length) and the group
+    // budget, whole steps
+    bool any_persistent = false;
+    for (const bfvm_solver* m : b->inst) any_persistent = any_persistent || persistent_ok(m);
     float best_ms = 1e30f;
     int64_t best_budget = 0;
-    int best_mode = BFVM_BATCH_FUSED;
-    for (int mode : {BFVM_BATCH_FUSED, BFVM_BATCH_BRANCHES})
-      for (int64_t budget : {(int64_t)0, (int64_t)b->l2_bytes, (int64_t)b->l2_bytes / 2,
-                             (int64_t)b->l2_bytes / 4, (int64_t)b->l2_bytes / 8}) {
-        b->cfg = best;
-        b->cfg.group_bytes = budget;
-        b->cfg.mode = mode;
-        plan(b);
-        const float ms = time_graph(b, dt, trial_steps, flags, 7);
-        if (ms < best_ms) {
-          best_ms = ms;
-          best_budget = budget;
-          best_mode = mode;
+    int best_mode = BFVM_BATCH_FUSED, best_pch = best.pch;
+    for (int mode : {BFVM_BATCH_FUSED, BFVM_BATCH_BRANCHES, BFVM_BATCH_PERSISTENT}) {
+      if (mode == BFVM_BATCH_PERSISTENT && (!any_persistent || !(flags & BFVM_STEP_DIFFUSION)))
+        continue;
+      for (int pch : {8, 16}) {
+        if (pch != 8 && mode != BFVM_BATCH_PERSISTENT) continue;
+        for (int64_t budget : {(int64_t)0, (int64_t)b->l2_bytes, (int64_t)b->l2_bytes / 2,
+                               (int64_t)b->l2_bytes / 4, (int64_t)b->l2_bytes / 8}) {
+          b->cfg = best;
+          b->cfg.group_bytes = budget;
+          b->cfg.mode = mode;
+          b->cfg.pch = pch;
+          plan(b, flags);
+          const float ms = time_graph(b, dt, trial_steps, flags, 7);
+          if (ms < best_ms) {
+            best_ms = ms;
+            best_budget = budget;
+            best_mode = mode;
+            best_pch = pch;
+          }
         }
       }
+    }
     best.group_bytes = best_budget;
     best.mode = best_mode;
+    best.pch = best_pch;
     b->cfg = best;
   } catch (...) {
     b->cfg = user;
@@ -657,6 +907,7 @@ int bfvm_batch_destroy(bfvm_batch* b) {
     cudaStreamSynchronize(b->stream);
     drop_graph(b);
     b->d_desc.release();
+    for (auto& sc : b->scratch) sc.buf.release();
     cudaEventDestroy(b->ev);
     cudaStreamDestroy(b->stream);
     delete b;
@@ -681,6 +932,8 @@ int bfvm_batch_clear(bfvm_batch* b) {
   return BATCH_CALL(b, {
     cudaStreamSynchronize(b->stream);
     b->inst.clear();
+    for (auto& sc : b->scratch) sc.buf.release();
+    b->scratch.clear();
     drop_graph(b);
   });
 }
@@ -735,8 +988,9 @@ int bfvm_batch_get_config(bfvm_batch* b, int* chunk, int* threads, int64_t* grou
 
 int bfvm_batch_set_mode(bfvm_batch* b, int mode) {
   return BATCH_CALL(b, {
-    require(mode == BFVM_BATCH_FUSED || mode == BFVM_BATCH_BRANCHES,
-            "mode must be BFVM_BATCH_FUSED or BFVM_BATCH_BRANCHES");
+    require(mode == BFVM_BATCH_FUSED || mode == BFVM_BATCH_BRANCHES ||
+                mode == BFVM_BATCH_PERSISTENT,
+            "mode must be BFVM_BATCH_FUSED, BFVM_BATCH_BRANCHES or BFVM_BATCH_PERSISTENT");
     b->cfg.mode = mode;
   });
 }
@@ -745,6 +999,20 @@ int bfvm_batch_get_mode(bfvm_batch* b, int* mode) {
   return BATCH_CALL(b, {
     require(mode != nullptr, "null output pointer");
     *mode = b->cfg.mode;
+  });
+}
+
+int bfvm_batch_set_persistent_chunk(bfvm_batch* b, int chunk) {
+  return BATCH_CALL(b, {
+    require(chunk == 8 || chunk == 16, "persistent chunk must be 8 or 16");
+    b->cfg.pch = chunk;
+  });
+}
+
+int bfvm_batch_get_persistent_chunk(bfvm_batch* b, int* chunk) {
+  return BATCH_CALL(b, {
+    require(chunk != nullptr, "null output pointer");
+    *chunk = b->cfg.pch;
   });
 }
 

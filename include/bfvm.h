@@ -370,8 +370,8 @@ BFVM_API int bfvm_batch_step(bfvm_batch* b, double dt, int nsteps, int flags);
 /* Autotuner: times short graph runs (trial_steps steps) of candidate chunk
  * lengths x threads per block for each axis, tunes every member's own sweeps
  * (bfvm_tune_sweeps, which branch mode runs), then candidate group budgets
- * in both modes (BFVM_BATCH_FUSED, BFVM_BATCH_BRANCHES), and keeps the
- * fastest.  The members' fields are saved before and restored
+ * in every mode (BFVM_BATCH_FUSED, BFVM_BATCH_BRANCHES, and
+ * BFVM_BATCH_PERSISTENT at 8- and 16-point chunks), and keeps the fastest.  The members' fields are saved before and restored
  * after, so tuning does not advance the simulation. */
 BFVM_API int bfvm_batch_tune(bfvm_batch* b, double dt, int flags, int trial_steps);
 /* chunk[3] in {8,16,32} with threads[3] in {128,256,512} per axis, or 0/0 to
@@ -380,17 +380,32 @@ BFVM_API int bfvm_batch_set_config(bfvm_batch* b, const int* chunk, const int* t
                                    int64_t group_bytes);
 BFVM_API int bfvm_batch_get_config(bfvm_batch* b, int* chunk, int* threads, int64_t* group_bytes);
 /* How a group of members runs (the whole call stays one CUDA-graph launch):
- *   BFVM_BATCH_FUSED     every phase of a step is one launch over all of the
- *                        group's members (default);
- *   BFVM_BATCH_BRANCHES  every member runs its own single-instance kernels
- *                        (its own sweep choices, bfvm_tune_sweeps) on its own
- *                        branch of the graph; the branches of a group run
- *                        concurrently.
+ *   BFVM_BATCH_FUSED       every phase of a step is one launch over all of
+ *                          the group's members (default);
+ *   BFVM_BATCH_BRANCHES    every member runs its own single-instance kernels
+ *                          (its own sweep choices, bfvm_tune_sweeps) on its
+ *                          own branch of the graph; the branches of a group
+ *                          run concurrently;
+ *   BFVM_BATCH_PERSISTENT  all n steps of every member of a group in ONE
+ *                          persistent cooperative launch over all SMs: the
+ *                          phases of a step (first-step sources, x, y, z
+ *                          with the next step's sources on the z stores)
+ *                          are shared by the members and separated by grid
+ *                          barriers, so a group that fits L2 keeps its fields
+ *                          on chip for the whole call.  Members with an FP64
+ *                          field and lines of at most 128 points; the others
+ *                          run as in BFVM_BATCH_BRANCHES, after the
+ *                          persistent groups.
  * bfvm_batch_tune chooses between them. */
 #define BFVM_BATCH_FUSED 0
 #define BFVM_BATCH_BRANCHES 1
+#define BFVM_BATCH_PERSISTENT 2
 BFVM_API int bfvm_batch_set_mode(bfvm_batch* b, int mode);
 BFVM_API int bfvm_batch_get_mode(bfvm_batch* b, int* mode);
+/* Points per chunk of the persistent mode's kernel: 8 (default) or 16
+ * (bfvm_batch_tune also picks it). */
+BFVM_API int bfvm_batch_set_persistent_chunk(bfvm_batch* b, int chunk);
+BFVM_API int bfvm_batch_get_persistent_chunk(bfvm_batch* b, int* chunk);
 /* Groups of the last plan and kernel launches in its graph. */
 BFVM_API int bfvm_batch_get_plan(bfvm_batch* b, int* groups, int64_t* kernels_per_call);
 BFVM_API int bfvm_batch_synchronize(bfvm_batch* b);

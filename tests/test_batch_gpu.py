@@ -7,7 +7,7 @@ import pytest
 
 from biofvm_b200 import STEP_ALL, STEP_CELLS, STEP_DIFFUSION, Batch, BfvmError, Solver, load_scenario
 from biofvm_b200 import workloads as W
-from biofvm_b200._abi import BATCH_BRANCHES, BATCH_FUSED
+from biofvm_b200._abi import BATCH_BRANCHES, BATCH_FUSED, BATCH_PERSISTENT
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
@@ -29,7 +29,8 @@ def members(seed=71, count=6):
     return out
 
 
-def run_batch(scns, steps, flags=STEP_ALL, config=None, tune=False, calls=1, mode=BATCH_FUSED):
+def run_batch(scns, steps, flags=STEP_ALL, config=None, tune=False, calls=1, mode=BATCH_FUSED,
+              pchunk=None):
     sols = [Solver(0) for _ in scns]
     for sv, scn in zip(sols, scns):
         load_scenario(sv, scn)
@@ -39,6 +40,8 @@ def run_batch(scns, steps, flags=STEP_ALL, config=None, tune=False, calls=1, mod
         if config:
             bt.set_config(*config)
         bt.set_mode(mode)
+        if pchunk:
+            bt.set_persistent_chunk(pchunk)
         if tune:
             bt.tune(scns[0].dt, flags, 2)
         for _ in range(calls):
@@ -261,7 +264,7 @@ def test_tuner_picks_a_mode_and_keeps_fields():
         for sv in sols:
             bt.add(sv)
         bt.tune(scns[0].dt, STEP_ALL, 2)
-        assert bt.get_mode() in (BATCH_FUSED, BATCH_BRANCHES)
+        assert bt.get_mode() in (BATCH_FUSED, BATCH_BRANCHES, BATCH_PERSISTENT)
         bt.step(scns[0].dt, 2)
         bt.synchronize()
         got = [sv.get_densities() for sv in sols]
@@ -276,3 +279,145 @@ def test_set_mode_rejects_unknown_modes():
     with Batch(0) as bt:
         with pytest.raises(BfvmError):
             bt.set_mode(7)
+
+
+# ---- persistent mode: all steps of a group's members in one cooperative
+# launch, phases shared by the members and separated by grid barriers ----
+
+@pytest.mark.parametrize("pchunk", [8, 16])
+@pytest.mark.parametrize("budget", [-1, 0, 200_000], ids=["default-groups", "one-group",
+                                                         "small-groups"])
+def test_persistent_matches_oracle_per_member(pchunk, budget):
+    scns = members(seed=91, count=6)
+    got, (groups, kernels) = run_batch(scns, 4, config=((0, 0, 0), (0, 0, 0), budget),
+                                       mode=BATCH_PERSISTENT, pchunk=pchunk)
+    assert kernels >= groups  # one cooperative launch per group (+ each member's maps)
+    if budget == 0:
+        assert groups == 1
+    for scn, p in zip(scns, got):
+        ref = O.oracle_run(scn, 4, 7)
+        assert np.all(O.max_rel_err(p, ref) <= TOL64), (pchunk, budget, scn.shape)
+
+
+def test_persistent_one_launch_per_group():
+    """Members without bulk, agents or Dirichlet nodes need no maps: the
+    graph holds exactly one kernel per group, whatever the step count."""
+    scns = [W.mixed_small(shape=(20 + 3 * b, 17, 11 + b), S=1 + b % 3, n_agents=0, seed=190 + b,
+                          dirichlet=False, bulk=False) for b in range(4)]
+    got, (groups, kernels) = run_batch(scns, 7, config=((0, 0, 0), (0, 0, 0), 0),
+                                       mode=BATCH_PERSISTENT)
+    assert groups == 1 and kernels == 1
+    for scn, p in zip(scns, got):
+        ref = O.oracle_run(scn, 7, 7)
+        assert np.all(O.max_rel_err(p, ref) <= TOL64), scn.shape
+
+
+def test_persistent_graph_replay_and_partial_flags():
+    scns = members(seed=92, count=4)
+    got, _ = run_batch(scns, 2, calls=3, mode=BATCH_PERSISTENT)
+    for scn, p in zip(scns, got):
+        ref = O.oracle_run(scn, 6, 7)
+        assert np.all(O.max_rel_err(p, ref) <= TOL64), scn.shape
+    # diffusion only (persistent groups); sources only (no sweep: branches)
+    for flags in (STEP_DIFFUSION, STEP_CELLS | 1, STEP_DIFFUSION | STEP_CELLS):
+        got, _ = run_batch(scns, 3, flags=flags, mode=BATCH_PERSISTENT)
+        for scn, p in zip(scns, got):
+            ref = O.oracle_run(scn, 3, flags)
+            assert np.all(O.max_rel_err(p, ref) <= TOL64), (flags, scn.shape)
+
+
+def test_persistent_lines_of_128_points_and_longer_members_on_branches():
+    """A member with 128-point lines runs in the persistent kernel (16 chunks
+    of 8); one with a 140-point axis cannot and runs on a branch."""
+    scns = [W.mixed_small(shape=(128, 6, 5), S=2, n_agents=80, seed=93),
+            W.mixed_small(shape=(5, 128, 7), S=1, n_agents=50, seed=94),
+            W.mixed_small(shape=(6, 5, 128), S=3, n_agents=50, seed=95),
+            W.mixed_small(shape=(140, 4, 3), S=2, n_agents=30, seed=96)]
+    for pchunk in (8, 16):
+        got, (groups, _) = run_batch(scns, 3, mode=BATCH_PERSISTENT, pchunk=pchunk)
+        assert groups >= 2  # the 140-point member is in a group of its own kind
+        for scn, p in zip(scns, got):
+            ref = O.oracle_run(scn, 3, 7)
+            assert np.all(O.max_rel_err(p, ref) <= TOL64), (pchunk, scn.shape)
+
+
+def test_persistent_sees_member_changes_between_calls():
+    """New agents (another count), then new Dirichlet values (same nodes)
+    between calls: the maps are rebuilt from the members' lists every call."""
+    a = W.mixed_small(shape=(12, 9, 8), S=2, n_agents=100, seed=97)
+    b = W.mixed_small(shape=(12, 9, 8), S=2, n_agents=400, seed=98)
+    c = W.mixed_small(shape=(7, 12, 5), S=3, n_agents=60, seed=99)
+    s1, s2 = Solver(0), Solver(0)
+    load_scenario(s1, a)
+    load_scenario(s2, c)
+    r1, r2 = Solver(0), Solver(0)
+    load_scenario(r1, a)
+    load_scenario(r2, c)
+    new_val = np.full(c.S, 0.25)
+    node = int(c.dirichlet_voxels[0])
+    with Batch(0) as bt:
+        bt.set_mode(BATCH_PERSISTENT)
+        bt.add(s1)
+        bt.add(s2)
+        bt.step(a.dt, 2)
+        r1.step(a.dt, 2)
+        r2.step(a.dt, 2)
+        for sv in (s1, r1):
+            sv.set_agents(*b.agent_arrays())
+        bt.step(a.dt, 2)
+        r1.step(a.dt, 2)
+        r2.step(a.dt, 2)
+        for sv in (s2, r2):
+            sv.update_dirichlet_node(node, new_val)
+        bt.step(a.dt, 2)
+        r1.step(a.dt, 2)
+        r2.step(a.dt, 2)
+        bt.synchronize()
+        for s, r in ((s1, r1), (s2, r2)):
+            assert np.all(O.max_rel_err(s.get_densities(), r.get_densities()) <= TOL64)
+    for sv in (s1, s2, r1, r2):
+        sv.close()
+
+
+def test_persistent_batched_workload_sample_matches_plain():
+    scns = W.batched_instances(count=5, seed=100, n_min=20, n_max=64, max_agents=4000)
+    got, _ = run_batch(scns, 6, mode=BATCH_PERSISTENT)
+    for scn, p in zip(scns, got):
+        with Solver(0) as sv:
+            load_scenario(sv, scn)
+            sv.step(scn.dt, 6)
+            plain = sv.get_densities()
+        assert np.all(O.max_rel_err(p, plain) <= TOL_BATCH_VS_PLAIN), scn.shape
+        ref = O.oracle_run(scn, 6, 7)
+        assert np.all(O.max_rel_err(p, ref) <= TOL64), scn.shape
+
+
+def test_persistent_fp32_members_run_on_branches():
+    """FP32 members cannot run in the FP64 persistent kernel: the batch runs
+    them on branches, within the FP32 bar against the FP64 oracle."""
+    scns = members(seed=101, count=3)
+    sols = [Solver(0) for _ in scns]
+    for sv, scn in zip(sols, scns):
+        load_scenario(sv, scn)
+        sv.set_precision(32)
+        sv.set_densities(scn.initial_field())
+    with Batch(0) as bt:
+        bt.set_mode(BATCH_PERSISTENT)
+        for sv in sols:
+            bt.add(sv)
+        bt.step(scns[0].dt, 3)
+        bt.synchronize()
+        got = [sv.get_densities() for sv in sols]
+    for sv in sols:
+        sv.close()
+    for scn, p in zip(scns, got):
+        ref = O.oracle_run(scn, 3, 7)
+        assert np.all(O.max_rel_err(p, ref) <= 1e-5), scn.shape
+
+
+def test_persistent_chunk_setter_rejects_other_lengths():
+    with Batch(0) as bt:
+        with pytest.raises(BfvmError):
+            bt.set_persistent_chunk(4)
+        bt.set_persistent_chunk(16)
+        assert bt.get_persistent_chunk() == 16

@@ -78,3 +78,130 @@ def test_substrate_shards_gather_to_the_unsharded_field(tmp_path, world):
     ref = O.oracle_run(scn, 3, 7)
     for r in range(world):
         assert np.array_equal(np.load(tmp_path / f"rank{r}.npy"), ref)
+
+
+# ---- the product path: every rank a Solver on the GPU ----
+
+def _shard_main(rank, world, port, backend, out_dir):
+    import torch
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    torch.cuda.set_device(0)
+    dist.init_process_group(backend, rank=rank, world_size=world)
+    try:
+        scn = W.mixed_small(shape=(19, 14, 11), S=5, n_agents=300, seed=35)
+        shard = SH.SubstrateShard(scn, device=0)
+        shard.step(scn.dt, 3)
+        dev = shard.gather_device()
+        np.save(os.path.join(out_dir, f"oncuda{rank}.npy"), np.array([int(dev.is_cuda)]))
+        full = dev.cpu().numpy()
+        blk = shard.device_block().cpu().numpy()
+        shard.close()
+        np.save(os.path.join(out_dir, f"rank{rank}.npy"), full)
+        np.save(os.path.join(out_dir, f"block{rank}.npy"), blk)
+    finally:
+        dist.destroy_process_group()
+
+
+def _run_ranks(target, world, args):
+    ctx = mp.get_context("spawn")
+    port = _free_port()
+    procs = [ctx.Process(target=target, args=(r, world, port, *args)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=300)
+        assert p.exitcode == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("world", [2, 3, 6], ids=["2", "3", "6-one-rank-empty"])
+def test_solver_shards_on_the_gpu_gather_to_the_oracle(tmp_path, world):
+    """Each rank (processes sharing the one GPU here; the collective runs over
+    gloo) steps its substrate block with a product Solver; the gathered field
+    matches the unsharded oracle run within the FP64 bar, and every rank's
+    block is its columns of it.  With 6 ranks and 5 substrates one rank holds
+    none and still takes part in the all-gather."""
+    from oracle import oracle as O
+
+    _run_ranks(_shard_main, world, ("gloo", str(tmp_path)))
+    scn = W.mixed_small(shape=(19, 14, 11), S=5, n_agents=300, seed=35)
+    ref = O.oracle_run(scn, 3, 7)
+    for r in range(world):
+        full = np.load(tmp_path / f"rank{r}.npy")
+        assert np.all(O.max_rel_err(full, ref) <= 1e-12)
+        a, b = SH.substrate_range(scn.S, world, r)
+        assert np.array_equal(np.load(tmp_path / f"block{r}.npy"), full[:, a:b])
+
+
+@pytest.mark.gpu
+def test_device_gather_over_nccl_stays_on_the_device(tmp_path):
+    """One rank over NCCL (the process group of one GPU): gather_device
+    returns a CUDA tensor equal to the oracle's field."""
+    from oracle import oracle as O
+
+    _run_ranks(_shard_main, 1, ("nccl", str(tmp_path)))
+    scn = W.mixed_small(shape=(19, 14, 11), S=5, n_agents=300, seed=35)
+    ref = O.oracle_run(scn, 3, 7)
+    assert np.load(tmp_path / "oncuda0.npy")[0] == 1
+    assert np.all(O.max_rel_err(np.load(tmp_path / "rank0.npy"), ref) <= 1e-12)
+
+
+def test_z_bounds_cover_every_plane_once():
+    for nz in range(1, 20):
+        for world in range(1, nz + 1):
+            b = SH.z_bounds(nz, world)
+            assert b[0] == 0 and b[-1] == nz and len(b) == world + 1
+            assert all(y > x for x, y in zip(b, b[1:]))
+    with pytest.raises(ValueError):
+        SH.z_bounds(3, 4)
+
+
+def _zslab_main(rank, world, port, backend, shape, out_dir):
+    import torch
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    torch.cuda.set_device(0)
+    dist.init_process_group(backend, rank=rank, world_size=world)
+    try:
+        scn = W.mixed_small(shape=shape, S=3, n_agents=400, seed=37)
+        shard = SH.ZSlabShard(scn, device=0)
+        shard.step(scn.dt, 4)
+        full = shard.gather()
+        shard.close()
+        np.save(os.path.join(out_dir, f"z{rank}.npy"), full)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("world,shape", [(2, (13, 11, 17)), (3, (13, 11, 17)),
+                                         (4, (9, 8, 5)), (2, (40, 36, 300))],
+                         ids=["2", "3", "4-thin-slabs", "2-long-z"])
+def test_z_slabs_join_to_the_unsplit_solve(tmp_path, world, shape):
+    """One field split by z planes over ranks (processes sharing the one GPU
+    here; the plane exchange runs over gloo): after 4 steps with bulk,
+    agents and Dirichlet nodes, every rank's gathered field matches the
+    unsplit oracle run within the FP64 bar."""
+    from oracle import oracle as O
+
+    _run_ranks(_zslab_main, world, ("gloo", shape, str(tmp_path)))
+    scn = W.mixed_small(shape=shape, S=3, n_agents=400, seed=37)
+    ref = O.oracle_run(scn, 4, 7)
+    for r in range(world):
+        got = np.load(tmp_path / f"z{r}.npy")
+        assert np.all(O.max_rel_err(got, ref) <= 1e-12), O.max_rel_err(got, ref)
+
+
+@pytest.mark.gpu
+def test_z_slab_of_one_rank_over_nccl(tmp_path):
+    """The NCCL path with one rank (the whole field is one slab)."""
+    from oracle import oracle as O
+
+    _run_ranks(_zslab_main, 1, ("nccl", (13, 11, 17), str(tmp_path)))
+    scn = W.mixed_small(shape=(13, 11, 17), S=3, n_agents=400, seed=37)
+    assert np.all(O.max_rel_err(np.load(tmp_path / "z0.npy"), O.oracle_run(scn, 4, 7)) <= 1e-12)

@@ -457,6 +457,92 @@ def run_ours(args, world, rank, local):
     sv.close()
 
 
+def run_sharded(args, world, rank, local):
+    """One microenvironment (the headline 256^3 x 10 workload by default)
+    split by substrate over the ranks, each rank a Solver stepping its block
+    (biofvm_b200.sharding.SubstrateShard): no collective inside a step, total
+    work fixed as N grows (strong scaling; 10 substrates over 8 ranks is
+    blocks of 2 and 1).  Time: the max over ranks of each rank's device time
+    (CUDA events on its solver's stream); then one all-gather of the whole
+    field into device memory (NCCL), timed on its own."""
+    import torch
+    import torch.distributed as dist
+
+    from biofvm_b200 import STEP_ALL
+    from biofvm_b200 import workloads as W
+    from biofvm_b200.sharding import SubstrateShard, substrate_range
+
+    if world == 1 and not dist.is_initialized():
+        import datetime
+
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        os.environ.setdefault("MASTER_PORT", "29533")
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", rank=0, world_size=1,
+                                timeout=datetime.timedelta(seconds=120))
+    if args.size == 256 and args.substrates == 10 and args.agents == 100_000:
+        scn = W.lod_256(steps=args.steps)
+    else:
+        scn = W.lod_cube(args.size, args.substrates, args.agents, steps=args.steps,
+                         name=f"lod_{args.size}")
+    N, S = scn.num_voxels, scn.S
+    shard = SubstrateShard(scn, device=local)
+    dt = scn.dt
+    sv = shard.solver
+    if sv is not None:
+        sv.step(dt, args.warmup, STEP_ALL)
+        if not args.no_tune:
+            sv.tune_sweeps(dt, 3)
+        sv.synchronize()
+    stream = (torch.cuda.ExternalStream(sv.stream, device=torch.device("cuda", local))
+              if sv is not None else torch.cuda.current_stream(local))
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    launches0 = sv.launch_count if sv is not None else 0
+    with ClockSampler(local) as clocks:
+        barrier(world)
+        torch.cuda.synchronize(local)
+        ev0.record(stream)
+        shard.step(dt, args.steps, STEP_ALL)
+        ev1.record(stream)
+        ev1.synchronize()
+        barrier(world)
+    launches = (sv.launch_count - launches0) if sv is not None else 0
+    ms = max_over_ranks(ev0.elapsed_time(ev1), world)
+    # one gather of the whole field into this GPU's memory
+    barrier(world)
+    torch.cuda.synchronize(local)
+    t0 = time.perf_counter()
+    full = shard.gather_device()
+    torch.cuda.synchronize(local)
+    t_gather = max_over_ranks(time.perf_counter() - t0, world)
+    ok = bool(tuple(full.shape) == (N, S))
+    del full
+    shard.close()
+    if rank == 0:
+        _, peak_kind = peaks()
+        vs = N * S * args.steps
+        line = {
+            "metric": METRIC + " (one microenvironment sharded by substrate)",
+            "value": vs / (ms / 1e3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)",
+            "config": {"workload": f"{scn.name}: {args.size}^3 voxels x {S} substrates FP64, "
+                                   f"{scn.num_agents} agents, bulk sphere r=500um",
+                       "parallelism": f"substrates x{world}",
+                       "substrates_per_rank": [b - a for a, b in (substrate_range(S, world, r)
+                                                                  for r in range(world))],
+                       "l2": "inputs larger than L2; no flush"},
+            "hbm_gbs_step_per_gpu": BYTES_PER_VS_STEP * N * S / world / (ms / args.steps / 1e3)
+            / 1e9,
+            "gather_device_seconds": t_gather, "gather_ok": ok,
+            "gpu_launches": int(launches), "peak_kind": peak_kind,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+
+
 def run_batched(args, world, rank, local):
     """The batched workload: 64 independent microenvironments (grids drawn
     from 32^3 to 128^3, 1-8 substrates, 0-20k agents each; seeded), 200 steps,
@@ -1037,6 +1123,10 @@ def main():
                          "gradients: compute_all_gradient_vectors at 256^3 x 10; lod2d: the "
                          "LOD_2D solver on a 1024^2 x 32 plane")
     ap.add_argument("--instances", type=int, default=64)
+    ap.add_argument("--shard", choices=["instances", "substrates"], default="instances",
+                    help="lod256 on N GPUs: independent microenvironments per rank (weak "
+                         "scaling, the default) or one microenvironment split by substrate "
+                         "(strong scaling)")
     ap.add_argument("--batch-trial-steps", type=int, default=10,
                     help="steps per trial run of the batch tuner")
     ap.add_argument("--batch-modes", action="store_true",
@@ -1067,6 +1157,8 @@ def main():
             run_gradients(args, world, rank, local)
         elif args.workload == "plain50":
             run_plain50(args, world, rank, local)
+        elif args.shard == "substrates":
+            run_sharded(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:

@@ -453,8 +453,124 @@ def run_ours(args, world, rank, local):
             "cpu_baseline": cpu,
             "clocks": clocks.summary(),
         }
+        if world == 1 and not args.no_configs:
+            try:
+                line["other_configs"] = other_configs(local)
+            except Exception as exc:  # reported, not fatal
+                line["other_configs"] = {"error": f"{type(exc).__name__}: {exc}"}
         print(json.dumps(line), flush=True)
     sv.close()
+
+
+def other_configs(local):
+    """The two other single-GPU configurations of the path, measured briefly
+    beside the headline line so that every run records them:
+      plain_50  50^3 x 1 FP64, all-boundary Dirichlet, 1000 agents, 100 steps:
+                microseconds per step of one bfvm_step call (all steps in one
+                cooperative launch) and of 100 one-step calls; the reference
+                on the host cores for the same 100 steps;
+      batched   the 64 instances (grids 32^3..128^3, 1-8 substrates, 0-20k
+                agents), 200 steps: the persistent batch mode (default group
+                budget, no tuning) against the same instances solved one by
+                one, wall clock around each, results compared within 1e-10."""
+    import torch
+
+    from biofvm_b200 import STEP_ALL, Batch, Solver, load_scenario
+    from biofvm_b200 import workloads as W
+    from biofvm_b200._abi import BATCH_PERSISTENT
+    from oracle import oracle as O
+
+    out = {}
+    # ---- plain_50
+    scn = W.plain_50(steps=100)
+    with Solver(local) as sv:
+        load_scenario(sv, scn)
+        stream = torch.cuda.ExternalStream(sv.stream, device=torch.device("cuda", local))
+        p0 = scn.initial_field()
+
+        def timed(fn):
+            sv.set_densities(p0)
+            sv.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            e1.synchronize()
+            return e0.elapsed_time(e1)
+
+        def one_step_calls():
+            for _ in range(100):
+                sv.step(scn.dt, 1, STEP_ALL)
+
+        sv.step(scn.dt, 3, STEP_ALL)
+        ms_one = timed(one_step_calls)
+        ms_all = timed(lambda: sv.step(scn.dt, 100, STEP_ALL))
+        got = sv.get_densities()
+    threads = os.cpu_count() or 1
+    variant = "v3" if (O.reference_available("v3") and _host_has_avx2()) else "core2"
+    r = O.Reference(scn, variant, threads=threads, cells_single_thread=False)
+    r.run(3)
+    secs = r.run(100)
+    r.close()
+    ref = O.oracle_run(scn, 100, 7)
+    out["plain_50"] = {
+        "workload": "50^3 x 1 FP64, all-boundary Dirichlet 1.0, 1000 uptake agents, 100 steps",
+        "us_per_step_one_call": 1e3 * ms_all / 100,
+        "us_per_step_one_step_calls": 1e3 * ms_one / 100,
+        "reference_us_per_step": 1e6 * secs / 100, "reference_threads": threads,
+        "max_rel_err_vs_oracle": float(O.max_rel_err(got, ref).max())}
+    # ---- batched
+    scns = W.batched_instances(count=64, steps=200)
+    sols = []
+    for sc in scns:
+        sv = Solver(local)
+        load_scenario(sv, sc)
+        sols.append(sv)
+    dt = scns[0].dt
+
+    def reset():
+        for sv, sc in zip(sols, scns):
+            sv.set_densities(sc.initial_field())
+        for sv in sols:
+            sv.synchronize()
+
+    for sv in sols:
+        sv.step(dt, 1, STEP_ALL)
+    reset()
+    t0 = time.perf_counter()
+    for sv in sols:
+        sv.step(dt, 200, STEP_ALL)
+        sv.synchronize()
+    t_plain = time.perf_counter() - t0
+    plain = [sv.get_densities() for sv in sols]
+    bt = Batch(local)
+    bt.set_mode(BATCH_PERSISTENT)
+    for sv in sols:
+        bt.add(sv)
+    reset()
+    bt.step(dt, 200, STEP_ALL)  # captures the graph
+    bt.synchronize()
+    reset()
+    t0 = time.perf_counter()
+    bt.step(dt, 200, STEP_ALL)
+    bt.synchronize()
+    t_batch = time.perf_counter() - t0
+    groups, kernels = bt.plan()
+    err = max(float(O.max_rel_err(sv.get_densities(), ref_p).max())
+              for sv, ref_p in zip(sols, plain))
+    bt.close()
+    for sv in sols:
+        sv.close()
+    vs = sum(sc.num_voxels * sc.S for sc in scns)
+    out["batched"] = {
+        "workload": "64 instances, grids 32^3..128^3, 1-8 substrates, 0-20k agents, 200 steps",
+        "mode": "persistent (default group budget, not tuned)",
+        "batched_seconds": t_batch, "looped_plain_seconds": t_plain,
+        "speedup_vs_looped_plain": t_plain / t_batch,
+        "value": vs * 200 / t_batch, "unit": UNIT, "groups": groups,
+        "kernels_per_call": kernels, "max_rel_err_vs_looped_plain": err}
+    return out
 
 
 def run_sharded(args, world, rank, local):
@@ -1107,6 +1223,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="lod256: skip the brief 50^3 and batched measurements")
     ap.add_argument("--no-tune", action="store_true",
                     help="keep the default kernel per axis (for profiler launch lists)")
     ap.add_argument("--size", type=int, default=256, help="cube edge in voxels (default 256)")

@@ -185,8 +185,11 @@ class SubstrateShard:
         cdev = dev if on_gpu else torch.device("cpu")
         send = torch.zeros((self.N, width), dtype=torch.float64, device=cdev)
         send[:, :block.shape[1]] = block
-        recv = torch.empty((self.world, self.N, width), dtype=torch.float64, device=cdev)
+        # the output is the ranks' blocks one after another along the first
+        # axis (the form every backend takes)
+        recv = torch.empty((self.world * self.N, width), dtype=torch.float64, device=cdev)
         dist.all_gather_into_tensor(recv, send, group=self.group)
+        recv = recv.view(self.world, self.N, width)
         out = torch.empty((self.N, self.S), dtype=torch.float64, device=dev)
         for r in range(self.world):
             a, b = substrate_range(self.S, self.world, r)
@@ -306,11 +309,12 @@ class ZSlabShard:
             with torch.cuda.stream(stream):
                 f = self._field()
                 send = torch.stack([f[0], f[-1]])
+                # [world * 2][C]: every slab's first and last plane in rank order
                 if on_gpu:
-                    recv = torch.empty((self.world, 2, C), dtype=torch.float64, device=dev)
+                    recv = torch.empty((self.world * 2, C), dtype=torch.float64, device=dev)
                     dist.all_gather_into_tensor(recv, send, group=self.group)
                 else:
-                    recv_h = torch.empty((self.world, 2, C), dtype=torch.float64)
+                    recv_h = torch.empty((self.world * 2, C), dtype=torch.float64)
                     dist.all_gather_into_tensor(recv_h, send.cpu(), group=self.group)
                     recv = recv_h.to(dev)
                 # recv was allocated on this stream: the allocator hands its
@@ -331,8 +335,9 @@ class ZSlabShard:
         cdev = dev if on_gpu else torch.device("cpu")
         send = torch.zeros((thick, C), dtype=torch.float64, device=cdev)
         send[:self.z1 - self.z0] = self._field()
-        recv = torch.empty((self.world, thick, C), dtype=torch.float64, device=cdev)
+        recv = torch.empty((self.world * thick, C), dtype=torch.float64, device=cdev)
         dist.all_gather_into_tensor(recv, send, group=self.group)
+        recv = recv.view(self.world, thick, C)
         out = torch.empty((self.nz, C), dtype=torch.float64, device=dev)
         for r in range(self.world):
             a, b = self.bounds[r], self.bounds[r + 1]

@@ -82,7 +82,8 @@ class Batch:
         call("bfvm_batch_set_mode", self._h, mode)
 
     def set_persistent_chunk(self, chunk: int) -> None:
-        """Points per chunk of the persistent kernel: 8 or 16."""
+        """Points per chunk of the persistent kernel: 8 or 16, or 0 for one
+        thread per (line, density) column solving the whole line."""
         call("bfvm_batch_set_persistent_chunk", self._h, chunk)
 
     def get_persistent_chunk(self) -> int:

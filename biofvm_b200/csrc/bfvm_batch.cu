@@ -51,7 +51,7 @@ struct BatchConfig {
   int threads[3] = {0, 0, 0};  // 0 = choose
   int64_t group_bytes = -1;    // -1 = default (half of L2), 0 = one group
   int mode = BFVM_BATCH_FUSED;
-  int pch = 8;                 // persistent mode: points per chunk (8 or 16)
+  int pch = 8;                 // persistent mode: points per chunk (8 or 16; 0: whole lines)
 };
 
 // Device descriptors of one group, all in one buffer.
@@ -100,7 +100,7 @@ struct bfvm_batch {
   // 8- and 16-point kernels (0: not queried), SMs
   std::vector<bfvm_rt::MemberScratch> scratch;
   std::vector<std::vector<bfvm::StepMember>> pmembers;
-  int p_per_sm[2] = {0, 0};
+  int p_per_sm[3] = {0, 0, 0};  // 8-, 16-point chunks, line form
   int num_sms = 0;
   // cached graph and what it was captured for
   cudaGraphExec_t exec = nullptr;
@@ -255,8 +255,9 @@ bfvm::StepMember step_member(bfvm_batch* b, bfvm_solver* m, int flags, int ch,
   d.S = m->S;
   const int ns[3] = {m->nx, m->ny, m->nz};
   for (int a = 0; a < 3; ++a) {
-    d.nc[a] = (ns[a] + ch - 1) / ch;
-    d.tw[a] = kBatchStepsThreads / d.nc[a];
+    // ch = 0: the line form, one column per work item
+    d.nc[a] = ch > 0 ? (ns[a] + ch - 1) / ch : 1;
+    d.tw[a] = ch > 0 ? kBatchStepsThreads / d.nc[a] : 1;
     d.ncols[a] = N / ns[a] * m->S;
     d.tile0[a] = tile0[a];
     d.coef[a] = coef_view<double>(m, a);
@@ -451,17 +452,26 @@ void enqueue_group_step(bfvm_batch* b, const GroupPlan& G, double dt, int flags,
 
 // Resident blocks per SM of the persistent kernel with ch-point chunks
 // (queried once per batch).
+// The persistent kernel for chunk length ch (0: the line form) and its
+// dynamic shared memory.
+const void* persistent_kernel(int ch, size_t* smem) {
+  *smem = ch > 0 ? 4 * kBatchStepsThreads * sizeof(double) : 0;
+  if (ch == 8) return (const void*)batch_steps_kernel<8>;
+  if (ch == 16) return (const void*)batch_steps_kernel<16>;
+  return (const void*)batch_lines_kernel<kBatchLineBatch>;
+}
+
 int persistent_per_sm(bfvm_batch* b, int ch) {
-  const int i = ch == 8 ? 0 : 1;
+  const int i = ch == 8 ? 0 : (ch == 16 ? 1 : 2);
   if (b->p_per_sm[i] == 0) {
     int coop = 0;
     BFVM_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, b->device));
     require(coop != 0, "batch: the device cannot launch cooperative kernels", BFVM_ERR_CUDA);
     BFVM_CUDA(cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, b->device));
-    const void* k = ch == 8 ? (const void*)batch_steps_kernel<8> : (const void*)batch_steps_kernel<16>;
+    size_t smem = 0;
+    const void* k = persistent_kernel(ch, &smem);
     int per = 0;
-    BFVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per, k, kBatchStepsThreads, 4 * kBatchStepsThreads * sizeof(double)));
+    BFVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, kBatchStepsThreads, smem));
     require(per > 0, "batch: the persistent kernel cannot be resident", BFVM_ERR_CUDA);
     b->p_per_sm[i] = per;
   }
@@ -473,7 +483,10 @@ int persistent_per_sm(bfvm_batch* b, int ch) {
 int persistent_blocks(bfvm_batch* b, const GroupPlan& G) {
   const int64_t wave = (int64_t)persistent_per_sm(b, b->cfg.pch) * b->num_sms;
   int64_t want = (G.src_items + kBatchStepsThreads - 1) / kBatchStepsThreads;
-  for (int a = 0; a < 3; ++a) want = std::max(want, G.ptiles[a]);
+  for (int a = 0; a < 3; ++a)
+    want = std::max(want, b->cfg.pch > 0 ? G.ptiles[a]
+                                         : (G.ptiles[a] + kBatchStepsThreads - 1) /
+                                               kBatchStepsThreads);
   return (int)std::max<int64_t>(1, std::min(want, wave));
 }
 
@@ -519,7 +532,8 @@ void enqueue_persistent_group(bfvm_batch* b, size_t gi, double dt, int nsteps,
   a.dt = dt;
   a.sources = sources ? 1 : 0;
   const int blocks = persistent_blocks(b, G);
-  const size_t smem = 4 * kBatchStepsThreads * sizeof(double);
+  size_t smem = 0;
+  const void* kern = persistent_kernel(b->cfg.pch, &smem);
   cudaLaunchConfig_t cfg;
   std::memset(&cfg, 0, sizeof cfg);
   cfg.gridDim = dim3((unsigned)blocks);
@@ -531,10 +545,8 @@ void enqueue_persistent_group(bfvm_batch* b, size_t gi, double dt, int nsteps,
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  if (b->cfg.pch == 8)
-    BFVM_CUDA(cudaLaunchKernelEx(&cfg, batch_steps_kernel<8>, a));
-  else
-    BFVM_CUDA(cudaLaunchKernelEx(&cfg, batch_steps_kernel<16>, a));
+  void* params[] = {&a};
+  BFVM_CUDA(cudaLaunchKernelExC(&cfg, kern, params));
   ++*kernels;
 }
 
@@ -833,7 +845,7 @@ void batch_tune(bfvm_batch* b, double dt, int flags, int trial_steps) {
     for (int mode : {BFVM_BATCH_FUSED, BFVM_BATCH_BRANCHES, BFVM_BATCH_PERSISTENT}) {
       if (mode == BFVM_BATCH_PERSISTENT && (!any_persistent || !(flags & BFVM_STEP_DIFFUSION)))
         continue;
-      for (int pch : {8, 16}) {
+      for (int pch : {8, 16, 0}) {
         if (pch != 8 && mode != BFVM_BATCH_PERSISTENT) continue;
         for (int64_t budget : {(int64_t)0, (int64_t)b->l2_bytes, (int64_t)b->l2_bytes / 2,
                                (int64_t)b->l2_bytes / 4, (int64_t)b->l2_bytes / 8}) {
@@ -1004,7 +1016,8 @@ int bfvm_batch_get_mode(bfvm_batch* b, int* mode) {
 
 int bfvm_batch_set_persistent_chunk(bfvm_batch* b, int chunk) {
   return BATCH_CALL(b, {
-    require(chunk == 8 || chunk == 16, "persistent chunk must be 8 or 16");
+    require(chunk == 0 || chunk == 8 || chunk == 16,
+            "persistent chunk must be 8, 16 or 0 (whole lines)");
     b->cfg.pch = chunk;
   });
 }

@@ -35,6 +35,7 @@ namespace bfvm {
 
 constexpr int kBatchStepsMaxN = 128;  // points per axis of a member (two mask words)
 constexpr int kBatchStepsThreads = 128;
+constexpr int kBatchLineBatch = 4;  // line form: points per load batch
 
 // One member of a group (device copy; read through the read-only cache).
 struct StepMember {
@@ -299,6 +300,150 @@ __global__ void __launch_bounds__(kBatchStepsThreads) batch_steps_kernel(const B
     batch_axis<1, CH>(a, batch_carries, false);
     grid.sync();
     batch_axis<2, CH>(a, batch_carries, a.sources && step + 1 < a.nsteps);
+    grid.sync();
+  }
+}
+
+// ---- line form: one thread per (line, density) column ---------------------
+//
+// The same phases with another work split: a work item is one column of one
+// member, solved whole by one thread (forward elimination, storing the
+// forward values, then back substitution reading them back), so there is no
+// fold between chunks and blocks need no barrier; the field crosses L2 twice
+// per phase (32 B/VS instead of 16).  Values move in batches of LB points:
+// the next batch is loaded before the current one is solved and stored, so
+// a thread keeps LB loads in flight.
+
+// Bulk and cell updates of the next step at one stored z-line point.
+__device__ __forceinline__ double member_point_sources(const StepMember& m, double x,
+                                                       int64_t vox, int s, double dt) {
+  if (m.bulk) {
+    const int row = __ldg(m.bulk_map + vox);
+    if (row >= 0) x = member_bulk(m, x, row, s, dt);
+  }
+  if (m.cells) {
+    const int r = __ldg(m.ag_map + vox);
+    if (r >= 0) x = member_cells(m, x, r, (uint64_t)vox, s);
+  }
+  return x;
+}
+
+template <int AX, int LB>
+__device__ __forceinline__ void member_line(const StepMember& m, int64_t vcol, bool sources_after,
+                                            double dt) {
+  const int S = m.S;
+  const int64_t plane = (int64_t)m.nx * m.ny;
+  const int n = AX == 0 ? m.nx : (AX == 1 ? m.ny : m.nz);
+  const int64_t C = AX == 0 ? S : (AX == 1 ? (int64_t)m.nx * S : plane * S);
+  const int64_t outer_stride = AX == 0 ? (int64_t)m.nx * S : (AX == 1 ? plane * S : 0);
+  const int64_t ls = C;
+  const int64_t outer = vcol / C;
+  const int64_t col = vcol - outer * C;
+  const int64_t off = outer * outer_stride + col;
+  const int s = (int)(col % S);
+  double* ptr = m.p + off;
+  const double* dptr = m.dir_field + off;
+  unsigned long long nd0 = 0ull, nd1 = 0ull;  // Dirichlet nodes of the line
+  if (m.dirichlet) {
+    nd0 = __ldg(m.dir_mask[AX] + 2 * (vcol / S));
+    nd1 = __ldg(m.dir_mask[AX] + 2 * (vcol / S) + 1);
+  }
+  const bool src = AX == 2 && sources_after && (m.bulk || m.cells);
+  unsigned long long sf0 = 0ull, sf1 = 0ull;  // points with bulk or agents (z lines)
+  if (src) {
+    sf0 = __ldg(m.src_mask + 2 * (vcol / S));
+    sf1 = __ldg(m.src_mask + 2 * (vcol / S) + 1);
+  }
+  const AxisCoef<double> cf = m.coef[AX];
+  const double c1 = __ldg(cf.c1 + s);
+  const double* inv = cf.inv_den + s;
+  const double* bwd = cf.bwd + s;
+  auto node = [&](int k) {
+    return ((k < 64 ? (nd0 >> k) : (nd1 >> (k - 64))) & 1ull) != 0;
+  };
+  auto load = [&](int k) { return node(k) ? __ldg(dptr + k * ls) : ptr[k * ls]; };
+  // forward: q_k = (p_k + c1 q_{k-1}) / d_k, stored over p
+  double cur[LB], nxt[LB];
+#pragma unroll
+  for (int i = 0; i < LB; ++i) cur[i] = (i < n) ? load(i) : 0.0;
+  double q = 0.0;
+  for (int k0 = 0; k0 < n; k0 += LB) {
+#pragma unroll
+    for (int i = 0; i < LB; ++i) nxt[i] = (k0 + LB + i < n) ? load(k0 + LB + i) : 0.0;
+#pragma unroll
+    for (int i = 0; i < LB; ++i) {
+      if (k0 + i < n) {
+        q = (cur[i] + c1 * q) * __ldg(inv + (int64_t)(k0 + i) * S);
+        cur[i] = q;
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < LB; ++i)
+      if (k0 + i < n) ptr[(k0 + i) * ls] = cur[i];
+#pragma unroll
+    for (int i = 0; i < LB; ++i) cur[i] = nxt[i];
+  }
+  // backward: x_k = q_k + b_k x_{k+1}, from the last point (x = q there)
+  double x = q;
+  const int64_t plane_s = plane;  // voxel step along z
+  const int64_t vox_line = vcol / S;  // z lines: j*nx + i
+  if (src && ((n - 1 < 64 ? (sf0 >> (n - 1)) : (sf1 >> (n - 65))) & 1ull))
+    ptr[(n - 1) * ls] = member_point_sources(m, x, vox_line + (int64_t)(n - 1) * plane_s, s, dt);
+  int top = n - 2;  // next point to solve, going down
+#pragma unroll
+  for (int i = 0; i < LB; ++i) cur[i] = (top - i >= 0) ? ptr[(top - i) * ls] : 0.0;
+  while (top >= 0) {
+#pragma unroll
+    for (int i = 0; i < LB; ++i) nxt[i] = (top - LB - i >= 0) ? ptr[(top - LB - i) * ls] : 0.0;
+#pragma unroll
+    for (int i = 0; i < LB; ++i) {
+      const int k = top - i;
+      if (k >= 0) {
+        x = cur[i] + __ldg(bwd + (int64_t)k * S) * x;
+        double out = x;
+        if (src && ((k < 64 ? (sf0 >> k) : (sf1 >> (k - 64))) & 1ull))
+          out = member_point_sources(m, x, vox_line + (int64_t)k * plane_s, s, dt);
+        cur[i] = out;
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < LB; ++i)
+      if (top - i >= 0) ptr[(top - i) * ls] = cur[i];
+#pragma unroll
+    for (int i = 0; i < LB; ++i) cur[i] = nxt[i];
+    top -= LB;
+  }
+}
+
+template <int AX, int LB>
+__device__ __forceinline__ void batch_axis_lines(const BatchStepsArgs& a, bool sources_after) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  int mi = 0;
+  for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < a.tiles[AX];
+       w += stride) {
+    while (mi + 1 < a.nmem && __ldg(&a.mem[mi + 1].tile0[AX]) <= w) ++mi;
+    const StepMember& m = a.mem[mi];
+    member_line<AX, LB>(m, w - m.tile0[AX], sources_after, a.dt);
+  }
+}
+
+// nsteps whole steps of every member in the line form (work items: columns,
+// tile0 = first column of a member in each phase); launched cooperatively
+// with kBatchStepsThreads threads and no shared memory.
+template <int LB>
+__global__ void __launch_bounds__(kBatchStepsThreads) batch_lines_kernel(const BatchStepsArgs a) {
+  namespace cg = cooperative_groups;
+  cg::grid_group grid = cg::this_grid();
+  for (int step = 0; step < a.nsteps; ++step) {
+    if (a.sources && step == 0) {
+      batch_sources(a);
+      grid.sync();
+    }
+    batch_axis_lines<0, LB>(a, false);
+    grid.sync();
+    batch_axis_lines<1, LB>(a, false);
+    grid.sync();
+    batch_axis_lines<2, LB>(a, a.sources && step + 1 < a.nsteps);
     grid.sync();
   }
 }

@@ -402,8 +402,10 @@ BFVM_API int bfvm_batch_get_config(bfvm_batch* b, int* chunk, int* threads, int6
 #define BFVM_BATCH_PERSISTENT 2
 BFVM_API int bfvm_batch_set_mode(bfvm_batch* b, int mode);
 BFVM_API int bfvm_batch_get_mode(bfvm_batch* b, int* mode);
-/* Points per chunk of the persistent mode's kernel: 8 (default) or 16
- * (bfvm_batch_tune also picks it). */
+/* Work split of the persistent mode's kernel: chunks of 8 (default) or 16
+ * points per thread, folded across the threads of a block; or 0, one thread
+ * per (line, density) column solving the whole line (no fold, the field read
+ * and written twice per sweep).  bfvm_batch_tune also picks it. */
 BFVM_API int bfvm_batch_set_persistent_chunk(bfvm_batch* b, int chunk);
 BFVM_API int bfvm_batch_get_persistent_chunk(bfvm_batch* b, int* chunk);
 /* Groups of the last plan and kernel launches in its graph. */

@@ -335,7 +335,7 @@ def run_ours(args, world, rank, local):
     # warm-up (also builds the Thomas coefficients and the device lists), then
     # the per-axis kernel choice timed on this field (which is restored)
     sv.step(dt, args.warmup, STEP_ALL)
-    tuned = sv.tune_sweeps(dt, 3) if not args.no_tune else [(0, 0, 0, 0)] * 3
+    tuned = sv.tune_sweeps(dt, 3) if not args.no_tune else [(0, 0, 0, 0, 0)] * 3
     sv.synchronize()
 
     launches0 = sv.launch_count
@@ -445,8 +445,8 @@ def run_ours(args, world, rank, local):
                          "algorithmic_bytes_per_launch": sweeps_in[dom] * BYTES_PER_VS_SWEEP * N * S},
             "kernel_ms": per,
             "tuned_sweeps": [{"axis": "xyz"[i], "kernel": ["default", "register", "tma", "direct"][k],
-                              "chunk": ch, "columns": tw, "min_blocks": mb}
-                             for i, (k, ch, tw, mb) in enumerate(tuned)],
+                              "chunk": ch, "columns": tw, "min_blocks": mb, "row_stages": st}
+                             for i, (k, ch, tw, mb, st) in enumerate(tuned)],
             "slab_planes": sv.get_slab_planes(), "fuse_sources": sv.get_fuse_sources(),
             "gpu_launches": int(launches),
             "e2e": e2e,
@@ -1064,7 +1064,7 @@ def run_lod2d(args, world, rank, local):
                        "l2": "field larger than L2; no flush"},
             "tuned_sweeps": [{"axis": "xy"[i], "kernel": ["default", "register", "tma",
                                                           "direct"][k],
-                              "chunk": ch, "columns": tw} for i, (k, ch, tw, _) in
+                              "chunk": ch, "columns": tw} for i, (k, ch, tw, *_) in
                              enumerate(tuned[:2])],
             "roofline": {"bound": "hbm", "kernel": "x and y sweeps of the plane",
                          "achieved": achieved, "peak": hbm, "peak_kind": peak_kind,

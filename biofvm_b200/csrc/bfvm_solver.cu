@@ -2593,6 +2593,13 @@ int bfvm_get_sweep_config(bfvm_solver* m, int axis, int* config) {
   });
 }
 
+int bfvm_set_row_stages(bfvm_solver* m, int stages) {
+  return SOLVER_CALL(m, {
+    require(stages == 2 || stages == 3, "stages must be 2 or 3");
+    m->axis[0].stages = stages;
+  });
+}
+
 int bfvm_synchronize(bfvm_solver* m) {
   return SOLVER_CALL(m, {
     BFVM_CUDA(cudaStreamSynchronize(m->stream));

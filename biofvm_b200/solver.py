@@ -199,8 +199,8 @@ class Solver:
 
     def tune_sweeps(self, dt: float, reps: int = 5):
         """Picks each axis's fastest sweep kernel by timing them on this field
-        (which is restored); returns [(kernel, chunk, columns, min_blocks)]
-        per axis."""
+        (which is restored); returns [(kernel, chunk, columns, min_blocks,
+        row-kernel ring stages)] per axis."""
         call("bfvm_tune_sweeps", self._h, dt, reps)
         out = []
         for ax in range(3):
@@ -208,7 +208,7 @@ class Solver:
             call("bfvm_get_sweep_kernel", self._h, ax, ctypes.byref(k))
             cfg = (ctypes.c_int * 4)()
             call("bfvm_get_sweep_config", self._h, ax, cfg)
-            out.append((k.value, cfg[0], cfg[1], cfg[2]))
+            out.append((k.value, cfg[0], cfg[1], cfg[2], cfg[3]))
         return out
 
     def get_sweep_kernel(self, axis: int) -> int:
@@ -226,6 +226,10 @@ class Solver:
         cfg = (ctypes.c_int * 4)()
         call("bfvm_get_sweep_config", self._h, axis, cfg)
         return tuple(cfg)
+
+    def set_row_stages(self, stages: int) -> None:
+        """Tiles in the x row kernel's shared-memory ring: 2 or 3."""
+        call("bfvm_set_row_stages", self._h, stages)
 
     def set_kernel_path(self, path: int) -> None:
         call("bfvm_set_kernel_path", self._h, path)

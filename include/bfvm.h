@@ -218,6 +218,10 @@ BFVM_API int bfvm_set_sweep_config(bfvm_solver* m, int axis, int chunk, int colu
                                    int min_blocks);
 /* config[4] = chunk, columns, min_blocks, and the tiles in the x row
  * kernel's shared-memory ring (2, or 3 where the tuner found it faster) */
+/* Tiles in the x row kernel's shared-memory ring: 2 (default) or 3 (one more
+ * tile in flight while a tile is solved; fewer rows per tile where shared
+ * memory runs short).  Kept until the next resize or tuning. */
+BFVM_API int bfvm_set_row_stages(bfvm_solver* m, int stages);
 /* Which sweep kernels run (all compute the same sweep):
  *   BFVM_PATH_AUTO    (default) the register kernel for x, the TMA-fed
  *                     persistent kernel for y and z where the layout allows

@@ -763,6 +763,29 @@ def run_batched(args, world, rank, local):
     bt.close()
     for sv in sols:
         sv.close()
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # the reference on the host cores, the instances one after another
+        # (one Microenvironment each), a bounded number of steps
+        try:
+            from oracle import oracle as O
+
+            threads = os.cpu_count() or 1
+            variant = "v3" if (O.reference_available("v3") and _host_has_avx2()) else "core2"
+            ref_steps = 5
+            secs = 0.0
+            for sc in scns:
+                r = O.Reference(sc, variant, threads=threads, cells_single_thread=False)
+                r.run(1)
+                secs += r.run(ref_steps)
+                r.close()
+            cpu = {"value": vs_per_step * ref_steps / secs, "unit": UNIT, "cores": threads,
+                   "kind": "reference",
+                   "sample": f"the {count} instances one after another, {ref_steps} timed steps "
+                             f"each after 1 warm-up; reference build {variant}"}
+        except Exception as exc:  # reported, not fatal
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                   "sample": f"unavailable: {exc}"}
     if rank == 0:
         line = {
             "metric": METRIC + " (batched instances)", "value": vs_per_step * args.steps * world /
@@ -786,6 +809,7 @@ def run_batched(args, world, rank, local):
                       "first_call_seconds": t_first},
             "modes_with_tuned_budget": per_mode,
             "gpu_launches": kernels,
+            "cpu_baseline": cpu,
             "clocks": clocks.summary(),
         }
         print(json.dumps(line), flush=True)

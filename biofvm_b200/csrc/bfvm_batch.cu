@@ -982,6 +982,7 @@ int bfvm_batch_set_config(bfvm_batch* b, const int* chunk, const int* threads,
     }
     c.group_bytes = group_bytes;
     c.mode = b->cfg.mode;
+    c.pch = b->cfg.pch;
     b->cfg = c;
   });
 }

@@ -315,7 +315,7 @@ __global__ void __launch_bounds__(kBatchStepsThreads) batch_steps_kernel(const B
 // a thread keeps LB loads in flight.
 
 // Bulk and cell updates of the next step at one stored z-line point.
-__device__ __forceinline__ double member_point_sources(const StepMember& m, double x,
+__device__ __noinline__ double member_point_sources(const StepMember& m, double x,
                                                        int64_t vox, int s, double dt) {
   if (m.bulk) {
     const int row = __ldg(m.bulk_map + vox);
@@ -328,90 +328,119 @@ __device__ __forceinline__ double member_point_sources(const StepMember& m, doub
   return x;
 }
 
-template <int AX, int LB>
-__device__ __forceinline__ void member_line(const StepMember& m, int64_t vcol, bool sources_after,
-                                            double dt) {
+// Loads of one line: points k0 .. k0+LB-1 (those below n), the Dirichlet
+// nodes' values where a mask bit is set (DIR).
+template <int LB, bool DIR>
+__device__ __forceinline__ void line_load(double (&v)[LB], const double* p, const double* d,
+                                          int ls, int k0, int n, unsigned long long nd0,
+                                          unsigned long long nd1) {
+#pragma unroll
+  for (int i = 0; i < LB; ++i) {
+    const int k = k0 + i;
+    if (k < n) {
+      bool node = false;
+      if (DIR) node = ((k < 64 ? (nd0 >> k) : (nd1 >> (k - 64))) & 1ull) != 0;
+      v[i] = node ? __ldg(d + k * ls) : p[k * ls];
+    }
+  }
+}
+
+// One (line, density) column of member m along axis AX, solved whole: the
+// forward values are stored over the field, then read back by the back
+// substitution.  Offsets inside a member fit in 32 bits (at most 128^3
+// voxels x the densities of an FP64 field that fits L2).  DIR: the line has
+// Dirichlet nodes; SRC: the z line has voxels with bulk or agent updates.
+template <int AX, int LB, bool DIR, bool SRC>
+__device__ __noinline__ void line_solve(const StepMember& m, double* ptr, const double* dptr,
+                                           int ls, int n, int s, int line,
+                                           unsigned long long nd0, unsigned long long nd1,
+                                           unsigned long long sf0, unsigned long long sf1,
+                                           double dt) {
   const int S = m.S;
-  const int64_t plane = (int64_t)m.nx * m.ny;
-  const int n = AX == 0 ? m.nx : (AX == 1 ? m.ny : m.nz);
-  const int64_t C = AX == 0 ? S : (AX == 1 ? (int64_t)m.nx * S : plane * S);
-  const int64_t outer_stride = AX == 0 ? (int64_t)m.nx * S : (AX == 1 ? plane * S : 0);
-  const int64_t ls = C;
-  const int64_t outer = vcol / C;
-  const int64_t col = vcol - outer * C;
-  const int64_t off = outer * outer_stride + col;
-  const int s = (int)(col % S);
-  double* ptr = m.p + off;
-  const double* dptr = m.dir_field + off;
-  unsigned long long nd0 = 0ull, nd1 = 0ull;  // Dirichlet nodes of the line
-  if (m.dirichlet) {
-    nd0 = __ldg(m.dir_mask[AX] + 2 * (vcol / S));
-    nd1 = __ldg(m.dir_mask[AX] + 2 * (vcol / S) + 1);
-  }
-  const bool src = AX == 2 && sources_after && (m.bulk || m.cells);
-  unsigned long long sf0 = 0ull, sf1 = 0ull;  // points with bulk or agents (z lines)
-  if (src) {
-    sf0 = __ldg(m.src_mask + 2 * (vcol / S));
-    sf1 = __ldg(m.src_mask + 2 * (vcol / S) + 1);
-  }
   const AxisCoef<double> cf = m.coef[AX];
   const double c1 = __ldg(cf.c1 + s);
   const double* inv = cf.inv_den + s;
   const double* bwd = cf.bwd + s;
-  auto node = [&](int k) {
-    return ((k < 64 ? (nd0 >> k) : (nd1 >> (k - 64))) & 1ull) != 0;
-  };
-  auto load = [&](int k) { return node(k) ? __ldg(dptr + k * ls) : ptr[k * ls]; };
-  // forward: q_k = (p_k + c1 q_{k-1}) / d_k, stored over p
   double cur[LB], nxt[LB];
-#pragma unroll
-  for (int i = 0; i < LB; ++i) cur[i] = (i < n) ? load(i) : 0.0;
+  line_load<LB, DIR>(cur, ptr, dptr, ls, 0, n, nd0, nd1);
   double q = 0.0;
   for (int k0 = 0; k0 < n; k0 += LB) {
-#pragma unroll
-    for (int i = 0; i < LB; ++i) nxt[i] = (k0 + LB + i < n) ? load(k0 + LB + i) : 0.0;
+    line_load<LB, DIR>(nxt, ptr, dptr, ls, k0 + LB, n, nd0, nd1);
 #pragma unroll
     for (int i = 0; i < LB; ++i) {
-      if (k0 + i < n) {
-        q = (cur[i] + c1 * q) * __ldg(inv + (int64_t)(k0 + i) * S);
-        cur[i] = q;
+      const int k = k0 + i;
+      if (k < n) {
+        q = (cur[i] + c1 * q) * __ldg(inv + k * S);
+        ptr[k * ls] = q;
       }
     }
 #pragma unroll
-    for (int i = 0; i < LB; ++i)
-      if (k0 + i < n) ptr[(k0 + i) * ls] = cur[i];
-#pragma unroll
     for (int i = 0; i < LB; ++i) cur[i] = nxt[i];
   }
-  // backward: x_k = q_k + b_k x_{k+1}, from the last point (x = q there)
+  // back substitution from the last point (x = q there)
+  const int plane = m.nx * m.ny;
   double x = q;
-  const int64_t plane_s = plane;  // voxel step along z
-  const int64_t vox_line = vcol / S;  // z lines: j*nx + i
-  if (src && ((n - 1 < 64 ? (sf0 >> (n - 1)) : (sf1 >> (n - 65))) & 1ull))
-    ptr[(n - 1) * ls] = member_point_sources(m, x, vox_line + (int64_t)(n - 1) * plane_s, s, dt);
-  int top = n - 2;  // next point to solve, going down
+  if (SRC && (((n - 1) < 64 ? (sf0 >> (n - 1)) : (sf1 >> (n - 65))) & 1ull))
+    ptr[(n - 1) * ls] = member_point_sources(m, x, (int64_t)line + (int64_t)(n - 1) * plane, s, dt);
 #pragma unroll
-  for (int i = 0; i < LB; ++i) cur[i] = (top - i >= 0) ? ptr[(top - i) * ls] : 0.0;
-  while (top >= 0) {
+  for (int i = 0; i < LB; ++i)
+    if (n - 2 - i >= 0) cur[i] = ptr[(n - 2 - i) * ls];
+  for (int top = n - 2; top >= 0; top -= LB) {
 #pragma unroll
-    for (int i = 0; i < LB; ++i) nxt[i] = (top - LB - i >= 0) ? ptr[(top - LB - i) * ls] : 0.0;
+    for (int i = 0; i < LB; ++i)
+      if (top - LB - i >= 0) nxt[i] = ptr[(top - LB - i) * ls];
 #pragma unroll
     for (int i = 0; i < LB; ++i) {
       const int k = top - i;
       if (k >= 0) {
-        x = cur[i] + __ldg(bwd + (int64_t)k * S) * x;
+        x = cur[i] + __ldg(bwd + k * S) * x;
         double out = x;
-        if (src && ((k < 64 ? (sf0 >> k) : (sf1 >> (k - 64))) & 1ull))
-          out = member_point_sources(m, x, vox_line + (int64_t)k * plane_s, s, dt);
-        cur[i] = out;
+        if (SRC && ((k < 64 ? (sf0 >> k) : (sf1 >> (k - 64))) & 1ull))
+          out = member_point_sources(m, x, (int64_t)line + (int64_t)k * plane, s, dt);
+        ptr[k * ls] = out;
       }
     }
 #pragma unroll
-    for (int i = 0; i < LB; ++i)
-      if (top - i >= 0) ptr[(top - i) * ls] = cur[i];
-#pragma unroll
     for (int i = 0; i < LB; ++i) cur[i] = nxt[i];
-    top -= LB;
+  }
+}
+
+template <int AX, int LB>
+__device__ __forceinline__ void member_line(const StepMember& m, int vcol, bool sources_after,
+                                            double dt) {
+  const int S = m.S;
+  const int plane = m.nx * m.ny;
+  const int n = AX == 0 ? m.nx : (AX == 1 ? m.ny : m.nz);
+  const int C = AX == 0 ? S : (AX == 1 ? m.nx * S : plane * S);
+  const int outer_stride = AX == 0 ? m.nx * S : (AX == 1 ? plane * S : 0);
+  const int outer = vcol / C;
+  const int col = vcol - outer * C;
+  const int s = col % S;
+  const int off = outer * outer_stride + col;
+  const int line = vcol / S;  // x: k*ny + j; y: k*nx + i; z: j*nx + i
+  double* ptr = m.p + off;
+  const double* dptr = m.dir_field + off;
+  unsigned long long nd0 = 0ull, nd1 = 0ull;
+  if (m.dirichlet) {
+    nd0 = __ldg(m.dir_mask[AX] + 2 * line);
+    nd1 = __ldg(m.dir_mask[AX] + 2 * line + 1);
+  }
+  unsigned long long sf0 = 0ull, sf1 = 0ull;
+  if (AX == 2 && sources_after && (m.bulk || m.cells)) {
+    sf0 = __ldg(m.src_mask + 2 * line);
+    sf1 = __ldg(m.src_mask + 2 * line + 1);
+  }
+  const bool dir = (nd0 | nd1) != 0ull, src = (sf0 | sf1) != 0ull;
+  if (dir) {
+    if (src)
+      line_solve<AX, LB, true, true>(m, ptr, dptr, C, n, s, line, nd0, nd1, sf0, sf1, dt);
+    else
+      line_solve<AX, LB, true, false>(m, ptr, dptr, C, n, s, line, nd0, nd1, sf0, sf1, dt);
+  } else {
+    if (src)
+      line_solve<AX, LB, false, true>(m, ptr, dptr, C, n, s, line, nd0, nd1, sf0, sf1, dt);
+    else
+      line_solve<AX, LB, false, false>(m, ptr, dptr, C, n, s, line, nd0, nd1, sf0, sf1, dt);
   }
 }
 
@@ -423,7 +452,7 @@ __device__ __forceinline__ void batch_axis_lines(const BatchStepsArgs& a, bool s
        w += stride) {
     while (mi + 1 < a.nmem && __ldg(&a.mem[mi + 1].tile0[AX]) <= w) ++mi;
     const StepMember& m = a.mem[mi];
-    member_line<AX, LB>(m, w - m.tile0[AX], sources_after, a.dt);
+    member_line<AX, LB>(m, (int)(w - m.tile0[AX]), sources_after, a.dt);
   }
 }
 
@@ -431,7 +460,7 @@ __device__ __forceinline__ void batch_axis_lines(const BatchStepsArgs& a, bool s
 // tile0 = first column of a member in each phase); launched cooperatively
 // with kBatchStepsThreads threads and no shared memory.
 template <int LB>
-__global__ void __launch_bounds__(kBatchStepsThreads) batch_lines_kernel(const BatchStepsArgs a) {
+__global__ void __launch_bounds__(kBatchStepsThreads, 8) batch_lines_kernel(const BatchStepsArgs a) {
   namespace cg = cooperative_groups;
   cg::grid_group grid = cg::this_grid();
   for (int step = 0; step < a.nsteps; ++step) {

@@ -82,8 +82,10 @@ class Batch:
         call("bfvm_batch_set_mode", self._h, mode)
 
     def set_persistent_chunk(self, chunk: int) -> None:
-        """Points per chunk of the persistent kernel: 8 or 16, or 0 for one
-        thread per (line, density) column solving the whole line."""
+        """Work split of the persistent kernel: 8 or 16 points per chunk
+        (chunks folded across a block), 32 (tiles of 32 columns with the
+        sweep kernels' chunk tables), or 0 (one thread per (line, density)
+        column solving the whole line)."""
         call("bfvm_batch_set_persistent_chunk", self._h, chunk)
 
     def get_persistent_chunk(self) -> int:

@@ -40,6 +40,7 @@
 
 #include "bfvm.h"
 #include "bfvm_batch_kernels.cuh"
+#include "bfvm_host_math.h"
 #include "bfvm_kernels_batch_steps.cuh"
 #include "bfvm_state.h"
 
@@ -51,7 +52,7 @@ struct BatchConfig {
   int threads[3] = {0, 0, 0};  // 0 = choose
   int64_t group_bytes = -1;    // -1 = default (half of L2), 0 = one group
   int mode = BFVM_BATCH_FUSED;
-  int pch = 8;                 // persistent mode: points per chunk (8 or 16; 0: whole lines)
+  int pch = 8;  // persistent mode: points per chunk (8, 16, 32: tile form; 0: whole lines)
 };
 
 // Device descriptors of one group, all in one buffer.
@@ -77,6 +78,7 @@ struct MemberScratch {
   size_t maps_bytes = 0;   // bulk_map + ag_map, set to -1 before each call
   size_t masks_off = 0, masks_bytes = 0;  // src, x, y, z masks, set to 0
   size_t dir_off = 0;      // dir_field (when the member has Dirichlet nodes)
+  DevBuf tabs;             // tile form: 32-point chunk tables of the three axes
 };
 
 }  // namespace
@@ -100,7 +102,7 @@ struct bfvm_batch {
   // 8- and 16-point kernels (0: not queried), SMs
   std::vector<bfvm_rt::MemberScratch> scratch;
   std::vector<std::vector<bfvm::StepMember>> pmembers;
-  int p_per_sm[3] = {0, 0, 0};  // 8-, 16-point chunks, line form
+  int p_per_sm[4] = {0, 0, 0, 0};  // 8-, 16-point chunks, line form, tile form
   int num_sms = 0;
   // cached graph and what it was captured for
   cudaGraphExec_t exec = nullptr;
@@ -255,9 +257,10 @@ bfvm::StepMember step_member(bfvm_batch* b, bfvm_solver* m, int flags, int ch,
   d.S = m->S;
   const int ns[3] = {m->nx, m->ny, m->nz};
   for (int a = 0; a < 3; ++a) {
-    // ch = 0: the line form, one column per work item
+    // ch = 0: the line form, one column per work item; ch = 32: the tile
+    // form, 32 columns per work item
     d.nc[a] = ch > 0 ? (ns[a] + ch - 1) / ch : 1;
-    d.tw[a] = ch > 0 ? kBatchStepsThreads / d.nc[a] : 1;
+    d.tw[a] = ch == 32 ? kBatchTileCols : (ch > 0 ? kBatchStepsThreads / d.nc[a] : 1);
     d.ncols[a] = N / ns[a] * m->S;
     d.tile0[a] = tile0[a];
     d.coef[a] = coef_view<double>(m, a);
@@ -286,6 +289,32 @@ bfvm::StepMember step_member(bfvm_batch* b, bfvm_solver* m, int flags, int ch,
     d.su = m->d_bulk_su.as<double>();
     d.rs = 1;
     d.bulk_row = nullptr;
+  }
+  if (ch == 32) {
+    // the sweep kernels' chunk tables for 32-point chunks, every chunk its
+    // own slot, from the FP64 Thomas coefficients
+    std::vector<double> all;
+    size_t off[3][3];
+    for (int a = 0; a < 3; ++a) {
+      const int n = ns[a], S = m->S, nc = (n + 31) / 32;
+      std::vector<double> k1((size_t)nc * 32 * S * 2), kg(k1.size()), kc((size_t)nc * S * 4);
+      bfvm::chunk_tables(n, S, 32, m->h_c1[a].data(), m->h_den[a].data(), m->h_cx[a].data(),
+                         k1.data(), kg.data(), kc.data());
+      off[a][0] = all.size();
+      all.insert(all.end(), k1.begin(), k1.end());
+      off[a][1] = all.size();
+      all.insert(all.end(), kg.begin(), kg.end());
+      off[a][2] = all.size();
+      all.insert(all.end(), kc.begin(), kc.end());
+      all.resize((all.size() + 1) & ~(size_t)1, 0.0);  // 16-byte aligned sections
+    }
+    upload(sc.tabs, all, b->stream);
+    const double* t = sc.tabs.as<double>();
+    for (int a = 0; a < 3; ++a) {
+      d.ck1[a] = t + off[a][0];
+      d.ckg[a] = t + off[a][1];
+      d.ckc[a] = t + off[a][2];
+    }
   }
   d.nagents = m->n_agents;
   d.ag_key = m->d_ag_key.as<uint64_t>();
@@ -455,14 +484,16 @@ void enqueue_group_step(bfvm_batch* b, const GroupPlan& G, double dt, int flags,
 // The persistent kernel for chunk length ch (0: the line form) and its
 // dynamic shared memory.
 const void* persistent_kernel(int ch, size_t* smem) {
-  *smem = ch > 0 ? 4 * kBatchStepsThreads * sizeof(double) : 0;
+  *smem = ch == 32 ? 4 * kBatchTileCols * sizeof(bfvm::Pair<double>)
+                   : (ch > 0 ? 4 * kBatchStepsThreads * sizeof(double) : 0);
   if (ch == 8) return (const void*)batch_steps_kernel<8>;
   if (ch == 16) return (const void*)batch_steps_kernel<16>;
+  if (ch == 32) return (const void*)batch_tiles_kernel;
   return (const void*)batch_lines_kernel<kBatchLineBatch>;
 }
 
 int persistent_per_sm(bfvm_batch* b, int ch) {
-  const int i = ch == 8 ? 0 : (ch == 16 ? 1 : 2);
+  const int i = ch == 8 ? 0 : (ch == 16 ? 1 : (ch == 0 ? 2 : 3));
   if (b->p_per_sm[i] == 0) {
     int coop = 0;
     BFVM_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, b->device));
@@ -845,7 +876,7 @@ void batch_tune(bfvm_batch* b, double dt, int flags, int trial_steps) {
     for (int mode : {BFVM_BATCH_FUSED, BFVM_BATCH_BRANCHES, BFVM_BATCH_PERSISTENT}) {
       if (mode == BFVM_BATCH_PERSISTENT && (!any_persistent || !(flags & BFVM_STEP_DIFFUSION)))
         continue;
-      for (int pch : {8, 16, 0}) {
+      for (int pch : {8, 16, 32, 0}) {
         if (pch != 8 && mode != BFVM_BATCH_PERSISTENT) continue;
         for (int64_t budget : {(int64_t)0, (int64_t)b->l2_bytes, (int64_t)b->l2_bytes / 2,
                                (int64_t)b->l2_bytes / 4, (int64_t)b->l2_bytes / 8}) {
@@ -1017,8 +1048,8 @@ int bfvm_batch_get_mode(bfvm_batch* b, int* mode) {
 
 int bfvm_batch_set_persistent_chunk(bfvm_batch* b, int chunk) {
   return BATCH_CALL(b, {
-    require(chunk == 0 || chunk == 8 || chunk == 16,
-            "persistent chunk must be 8, 16 or 0 (whole lines)");
+    require(chunk == 0 || chunk == 8 || chunk == 16 || chunk == 32,
+            "persistent chunk must be 8, 16, 32 or 0 (whole lines)");
     b->cfg.pch = chunk;
   });
 }

@@ -30,6 +30,7 @@
 #include <cooperative_groups.h>
 
 #include "bfvm_kernels.cuh"
+#include "bfvm_kernels_tma.cuh"
 
 namespace bfvm {
 
@@ -69,6 +70,12 @@ struct StepMember {
   // at their places in a field-shaped array [N][S]
   const unsigned long long* dir_mask[3];
   const double* dir_field;
+  // tile form: per axis the chunk tables of 32-point chunks, chunk c at
+  // k1 + c*32*S*2 and kg alike ({1/d, a} and {G, R} per point and density),
+  // kc [nc][S][4] the per-chunk transfer constants
+  const double* ck1[3];
+  const double* ckg[3];
+  const double* ckc[3];
 };
 
 struct BatchStepsArgs {
@@ -473,6 +480,118 @@ __global__ void __launch_bounds__(kBatchStepsThreads, 8) batch_lines_kernel(cons
     batch_axis_lines<1, LB>(a, false);
     grid.sync();
     batch_axis_lines<2, LB>(a, a.sources && step + 1 < a.nsteps);
+    grid.sync();
+  }
+}
+
+// ---- tile form: 32-point chunks with the sweep kernels' chunk tables -------
+//
+// A work item is a tile of 32 columns x NC <= 4 chunks of 32 points of one
+// member (128 threads), loaded straight from global memory (32 loads in
+// flight per thread) and solved with the chunk tables of the TMA sweep
+// kernels (chunk_local / chunk_carries / chunk_fix: three table loads per
+// point, the fold over at most four chunks).
+
+constexpr int kBatchTileCols = 32;
+constexpr int kBatchTileCh = 32;
+
+template <int AX>
+__device__ __forceinline__ void member_tile32(const StepMember& m, int tile, Pair<double>* fold,
+                                              bool sources_after, double dt) {
+  constexpr int CH = kBatchTileCh, W = kBatchTileCols;
+  const int S = m.S;
+  const int plane = m.nx * m.ny;
+  const int n = AX == 0 ? m.nx : (AX == 1 ? m.ny : m.nz);
+  const int C = AX == 0 ? S : (AX == 1 ? m.nx * S : plane * S);
+  const int outer_stride = AX == 0 ? m.nx * S : (AX == 1 ? plane * S : 0);
+  const int ls = C;
+  const int NC = m.nc[AX];
+  const int tx = threadIdx.x % W;
+  const int c = threadIdx.x / W;  // chunk; threads past NC chunks idle
+  const int k0 = c * CH;
+  const int vcol = tile * W + tx;
+  const bool active = c < NC && vcol < (int)m.ncols[AX];
+  const int len = active ? max(0, min(CH, n - k0)) : 0;
+  int s = 0, line = 0;
+  double* ptr = m.p;
+  const double* dptr = m.dir_field;
+  unsigned long long nodes = 0ull;
+  if (active) {
+    const int outer = vcol / C;
+    const int col = vcol - outer * C;
+    s = col % S;
+    line = vcol / S;
+    const int off = outer * outer_stride + col + k0 * ls;
+    ptr += off;
+    dptr += off;
+    if (m.dirichlet) nodes = chunk_bits(m.dir_mask[AX], line, k0);
+  }
+  double v[CH];
+  if (nodes == 0ull) {
+#pragma unroll
+    for (int i = 0; i < CH; ++i) v[i] = (i < len) ? ptr[i * ls] : 0.0;
+  } else {
+#pragma unroll
+    for (int i = 0; i < CH; ++i)
+      v[i] = (i < len) ? (((nodes >> i) & 1ull) ? __ldg(dptr + i * ls) : ptr[i * ls]) : 0.0;
+  }
+  const int row = (k0 * S + s) * 2;
+  double qe = 0.0, x0 = 0.0;
+  chunk_local<false, double, CH>(v, len, m.ck1[AX] + row, S, qe, x0);
+  if (c < NC) st_fold(fold + c * W + tx, qe, x0);
+  __syncthreads();
+  if (len > 0) {
+    ChunkCoef<double> tab;
+    tab.kc = m.ckc[AX];
+    double cf, cb;
+    chunk_carries<false, double>(fold, W, tx, c, NC, tab, s, S, cf, cb);
+    chunk_fix<false, double, CH>(v, len, m.ckg[AX] + row, S, cf, cb);
+    if (AX == 2 && sources_after && (m.bulk || m.cells)) {
+      const unsigned long long flagged = chunk_bits(m.src_mask, line, k0);
+      if (flagged != 0ull) {
+        const int64_t vox0 = (int64_t)line + (int64_t)k0 * plane;
+#pragma unroll
+        for (int i = 0; i < CH; ++i)
+          if (i < len && ((flagged >> i) & 1ull))
+            v[i] = member_point_sources(m, v[i], vox0 + (int64_t)i * plane, s, dt);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < CH; ++i)
+      if (i < len) ptr[i * ls] = v[i];
+  }
+  __syncthreads();  // the fold of this tile is read before the next overwrites it
+}
+
+template <int AX>
+__device__ __forceinline__ void batch_axis_tiles(const BatchStepsArgs& a, Pair<double>* fold,
+                                                 bool sources_after) {
+  int mi = 0;
+  for (int64_t t = blockIdx.x; t < a.tiles[AX]; t += gridDim.x) {
+    while (mi + 1 < a.nmem && __ldg(&a.mem[mi + 1].tile0[AX]) <= t) ++mi;
+    const StepMember& m = a.mem[mi];
+    member_tile32<AX>(m, (int)(t - m.tile0[AX]), fold, sources_after, a.dt);
+  }
+}
+
+// nsteps whole steps of every member in the tile form; launched
+// cooperatively with 128 threads and 4 x 32 (qe, x0) pairs of dynamic shared
+// memory per block.
+__global__ void __launch_bounds__(kBatchStepsThreads, 2) batch_tiles_kernel(const BatchStepsArgs a) {
+  namespace cg = cooperative_groups;
+  cg::grid_group grid = cg::this_grid();
+  extern __shared__ __align__(16) unsigned char tiles_smem[];
+  Pair<double>* fold = reinterpret_cast<Pair<double>*>(tiles_smem);
+  for (int step = 0; step < a.nsteps; ++step) {
+    if (a.sources && step == 0) {
+      batch_sources(a);
+      grid.sync();
+    }
+    batch_axis_tiles<0>(a, fold, false);
+    grid.sync();
+    batch_axis_tiles<1>(a, fold, false);
+    grid.sync();
+    batch_axis_tiles<2>(a, fold, a.sources && step + 1 < a.nsteps);
     grid.sync();
   }
 }

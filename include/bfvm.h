@@ -407,9 +407,11 @@ BFVM_API int bfvm_batch_get_config(bfvm_batch* b, int* chunk, int* threads, int6
 BFVM_API int bfvm_batch_set_mode(bfvm_batch* b, int mode);
 BFVM_API int bfvm_batch_get_mode(bfvm_batch* b, int* mode);
 /* Work split of the persistent mode's kernel: chunks of 8 (default) or 16
- * points per thread, folded across the threads of a block; or 0, one thread
- * per (line, density) column solving the whole line (no fold, the field read
- * and written twice per sweep).  bfvm_batch_tune also picks it. */
+ * points per thread, folded across the threads of a block; 32, tiles of 32
+ * columns x at most 4 chunks of 32 points solved with the sweep kernels'
+ * chunk tables; or 0, one thread per (line, density) column solving the
+ * whole line (no fold, the field read and written twice per sweep).
+ * bfvm_batch_tune also picks it. */
 BFVM_API int bfvm_batch_set_persistent_chunk(bfvm_batch* b, int chunk);
 BFVM_API int bfvm_batch_get_persistent_chunk(bfvm_batch* b, int* chunk);
 /* Groups of the last plan and kernel launches in its graph. */

@@ -284,7 +284,7 @@ def test_set_mode_rejects_unknown_modes():
 # ---- persistent mode: all steps of a group's members in one cooperative
 # launch, phases shared by the members and separated by grid barriers ----
 
-@pytest.mark.parametrize("pchunk", [8, 16, 0], ids=["ch8", "ch16", "lines"])
+@pytest.mark.parametrize("pchunk", [8, 16, 32, 0], ids=["ch8", "ch16", "tiles32", "lines"])
 @pytest.mark.parametrize("budget", [-1, 0, 200_000], ids=["default-groups", "one-group",
                                                          "small-groups"])
 def test_persistent_matches_oracle_per_member(pchunk, budget):
@@ -312,7 +312,7 @@ def test_persistent_one_launch_per_group():
         assert np.all(O.max_rel_err(p, ref) <= TOL64), scn.shape
 
 
-@pytest.mark.parametrize("pchunk", [8, 0], ids=["ch8", "lines"])
+@pytest.mark.parametrize("pchunk", [8, 32, 0], ids=["ch8", "tiles32", "lines"])
 def test_persistent_graph_replay_and_partial_flags(pchunk):
     scns = members(seed=92, count=4)
     got, _ = run_batch(scns, 2, calls=3, mode=BATCH_PERSISTENT, pchunk=pchunk)
@@ -334,7 +334,7 @@ def test_persistent_lines_of_128_points_and_longer_members_on_branches():
             W.mixed_small(shape=(5, 128, 7), S=1, n_agents=50, seed=94),
             W.mixed_small(shape=(6, 5, 128), S=3, n_agents=50, seed=95),
             W.mixed_small(shape=(140, 4, 3), S=2, n_agents=30, seed=96)]
-    for pchunk in (8, 16, 0):
+    for pchunk in (8, 16, 32, 0):
         got, (groups, _) = run_batch(scns, 3, mode=BATCH_PERSISTENT, pchunk=pchunk)
         assert groups >= 2  # the 140-point member is in a group of its own kind
         for scn, p in zip(scns, got):
@@ -380,7 +380,7 @@ def test_persistent_sees_member_changes_between_calls():
         sv.close()
 
 
-@pytest.mark.parametrize("pchunk", [8, 0], ids=["ch8", "lines"])
+@pytest.mark.parametrize("pchunk", [8, 32, 0], ids=["ch8", "tiles32", "lines"])
 def test_persistent_batched_workload_sample_matches_plain(pchunk):
     scns = W.batched_instances(count=5, seed=100, n_min=20, n_max=64, max_agents=4000)
     got, _ = run_batch(scns, 6, mode=BATCH_PERSISTENT, pchunk=pchunk)

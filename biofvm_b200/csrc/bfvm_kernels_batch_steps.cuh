@@ -177,10 +177,12 @@ __device__ __forceinline__ void member_tile(const StepMember& m, int64_t tile, d
     s = (int)(col % S);
     if (m.dirichlet) nodes = chunk_bits(m.dir_mask[AX], vcol / S, k0);
   }
+  // the field moves through L2 only, so that L1 keeps the coefficient tables
   double v[CH];
 #pragma unroll
   for (int q = 0; q < CH; ++q)
-    v[q] = (q < len) ? (((nodes >> q) & 1ull) ? __ldg(dptr + q * ls) : ptr[q * ls]) : 0.0;
+    v[q] = (q < len) ? (((nodes >> q) & 1ull) ? __ldcg(dptr + q * ls) : __ldcg(ptr + q * ls))
+                     : 0.0;
   const double* c_inv = cf.inv_den + (int64_t)k0 * S + s;
   const double* c_fwd = cf.fwd + (int64_t)k0 * S + s;
   const double* c_bwd = cf.bwd + (int64_t)k0 * S + s;
@@ -263,7 +265,7 @@ __device__ __forceinline__ void member_tile(const StepMember& m, int64_t tile, d
   }
 #pragma unroll
   for (int i = 0; i < CH; ++i)
-    if (i < len) ptr[i * ls] = v[i];
+    if (i < len) __stcg(ptr + i * ls, v[i]);
   __syncthreads();  // the carries of this tile are read before the next overwrites them
 }
 
@@ -347,7 +349,7 @@ __device__ __forceinline__ void line_load(double (&v)[LB], const double* p, cons
     if (k < n) {
       bool node = false;
       if (DIR) node = ((k < 64 ? (nd0 >> k) : (nd1 >> (k - 64))) & 1ull) != 0;
-      v[i] = node ? __ldg(d + k * ls) : p[k * ls];
+      v[i] = node ? __ldcg(d + k * ls) : __ldcg(p + k * ls);
     }
   }
 }
@@ -378,7 +380,7 @@ __device__ __noinline__ void line_solve(const StepMember& m, double* ptr, const 
       const int k = k0 + i;
       if (k < n) {
         q = (cur[i] + c1 * q) * __ldg(inv + k * S);
-        ptr[k * ls] = q;
+        __stcg(ptr + k * ls, q);
       }
     }
 #pragma unroll
@@ -391,11 +393,11 @@ __device__ __noinline__ void line_solve(const StepMember& m, double* ptr, const 
     ptr[(n - 1) * ls] = member_point_sources(m, x, (int64_t)line + (int64_t)(n - 1) * plane, s, dt);
 #pragma unroll
   for (int i = 0; i < LB; ++i)
-    if (n - 2 - i >= 0) cur[i] = ptr[(n - 2 - i) * ls];
+    if (n - 2 - i >= 0) cur[i] = __ldcg(ptr + (n - 2 - i) * ls);
   for (int top = n - 2; top >= 0; top -= LB) {
 #pragma unroll
     for (int i = 0; i < LB; ++i)
-      if (top - LB - i >= 0) nxt[i] = ptr[(top - LB - i) * ls];
+      if (top - LB - i >= 0) nxt[i] = __ldcg(ptr + (top - LB - i) * ls);
 #pragma unroll
     for (int i = 0; i < LB; ++i) {
       const int k = top - i;
@@ -404,7 +406,7 @@ __device__ __noinline__ void line_solve(const StepMember& m, double* ptr, const 
         double out = x;
         if (SRC && ((k < 64 ? (sf0 >> k) : (sf1 >> (k - 64))) & 1ull))
           out = member_point_sources(m, x, (int64_t)line + (int64_t)k * plane, s, dt);
-        ptr[k * ls] = out;
+        __stcg(ptr + k * ls, out);
       }
     }
 #pragma unroll
@@ -526,14 +528,17 @@ __device__ __forceinline__ void member_tile32(const StepMember& m, int tile, Pai
     dptr += off;
     if (m.dirichlet) nodes = chunk_bits(m.dir_mask[AX], line, k0);
   }
+  // the field moves through L2 only (__ldcg / __stcg), so that L1 keeps the
+  // chunk tables, which the recurrences wait on
   double v[CH];
   if (nodes == 0ull) {
 #pragma unroll
-    for (int i = 0; i < CH; ++i) v[i] = (i < len) ? ptr[i * ls] : 0.0;
+    for (int i = 0; i < CH; ++i) v[i] = (i < len) ? __ldcg(ptr + i * ls) : 0.0;
   } else {
 #pragma unroll
     for (int i = 0; i < CH; ++i)
-      v[i] = (i < len) ? (((nodes >> i) & 1ull) ? __ldg(dptr + i * ls) : ptr[i * ls]) : 0.0;
+      v[i] = (i < len) ? (((nodes >> i) & 1ull) ? __ldcg(dptr + i * ls) : __ldcg(ptr + i * ls))
+                       : 0.0;
   }
   const int row = (k0 * S + s) * 2;
   double qe = 0.0, x0 = 0.0;
@@ -558,7 +563,7 @@ __device__ __forceinline__ void member_tile32(const StepMember& m, int tile, Pai
     }
 #pragma unroll
     for (int i = 0; i < CH; ++i)
-      if (i < len) ptr[i * ls] = v[i];
+      if (i < len) __stcg(ptr + i * ls, v[i]);
   }
   __syncthreads();  // the fold of this tile is read before the next overwrites it
 }

@@ -103,6 +103,7 @@ struct bfvm_batch {
   std::vector<bfvm_rt::MemberScratch> scratch;
   std::vector<std::vector<bfvm::StepMember>> pmembers;
   int p_per_sm[4] = {0, 0, 0, 0};  // 8-, 16-point chunks, line form, tile form
+  size_t tile_tab_doubles = 0;  // tile form: the largest member's tables of one axis
   int num_sms = 0;
   // cached graph and what it was captured for
   cudaGraphExec_t exec = nullptr;
@@ -223,9 +224,11 @@ std::vector<std::vector<bfvm_solver*>> make_groups(const std::vector<bfvm_solver
 
 // Whether a member can run in the persistent mode's kernel: FP64 field,
 // lines of at most 128 points.
-bool persistent_ok(const bfvm_solver* m) {
+// (The tile form stages a member's chunk tables of one axis in shared
+// memory, about 4.2 KB per density: at most 32 densities there.)
+bool persistent_ok(const bfvm_solver* m, int pch) {
   return m->precision == BFVM_FP64 && m->nx <= kBatchStepsMaxN && m->ny <= kBatchStepsMaxN &&
-         m->nz <= kBatchStepsMaxN;
+         m->nz <= kBatchStepsMaxN && (pch != 32 || m->S <= 32);
 }
 
 size_t round256(size_t x) { return (x + 255) / 256 * 256; }
@@ -307,6 +310,7 @@ bfvm::StepMember step_member(bfvm_batch* b, bfvm_solver* m, int flags, int ch,
       off[a][2] = all.size();
       all.insert(all.end(), kc.begin(), kc.end());
       all.resize((all.size() + 1) & ~(size_t)1, 0.0);  // 16-byte aligned sections
+      b->tile_tab_doubles = std::max(b->tile_tab_doubles, all.size() - off[a][0]);
     }
     upload(sc.tabs, all, b->stream);
     const double* t = sc.tabs.as<double>();
@@ -332,7 +336,8 @@ void build_plan(bfvm_batch* b, int flags) {
   std::vector<bfvm_solver*> pers, rest;
   const bool persistent = b->cfg.mode == BFVM_BATCH_PERSISTENT && sizeof(T) == sizeof(double) &&
                           (flags & BFVM_STEP_DIFFUSION);
-  for (bfvm_solver* m : b->inst) (persistent && persistent_ok(m) ? pers : rest).push_back(m);
+  for (bfvm_solver* m : b->inst)
+    (persistent && persistent_ok(m, b->cfg.pch) ? pers : rest).push_back(m);
   auto pgroups = make_groups(pers, budget);
   const size_t n_pers = pgroups.size();
   auto groups = pgroups;
@@ -341,6 +346,7 @@ void build_plan(bfvm_batch* b, int flags) {
   buf.clear();
   b->groups.clear();
   b->pmembers.clear();
+  b->tile_tab_doubles = 0;
   b->group_members = groups;
   for (size_t gi = 0; gi < groups.size(); ++gi) {
     auto& members = groups[gi];
@@ -479,12 +485,19 @@ void enqueue_group_step(bfvm_batch* b, const GroupPlan& G, double dt, int flags,
   }
 }
 
+// Dynamic shared memory above the default 48 KB for a persistent kernel.
+void allow_persistent_smem(const void* k, size_t smem) {
+  if (smem > 48 * 1024)
+    BFVM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+}
+
 // Resident blocks per SM of the persistent kernel with ch-point chunks
 // (queried once per batch).
 // The persistent kernel for chunk length ch (0: the line form) and its
 // dynamic shared memory.
-const void* persistent_kernel(int ch, size_t* smem) {
-  *smem = ch == 32 ? 4 * kBatchTileCols * sizeof(bfvm::Pair<double>)
+const void* persistent_kernel(const bfvm_batch* b, int ch, size_t* smem) {
+  *smem = ch == 32 ? 4 * kBatchTileCols * sizeof(bfvm::Pair<double>) +
+                         b->tile_tab_doubles * sizeof(double)
                    : (ch > 0 ? 4 * kBatchStepsThreads * sizeof(double) : 0);
   if (ch == 8) return (const void*)batch_steps_kernel<8>;
   if (ch == 16) return (const void*)batch_steps_kernel<16>;
@@ -494,13 +507,14 @@ const void* persistent_kernel(int ch, size_t* smem) {
 
 int persistent_per_sm(bfvm_batch* b, int ch) {
   const int i = ch == 8 ? 0 : (ch == 16 ? 1 : (ch == 0 ? 2 : 3));
-  if (b->p_per_sm[i] == 0) {
+  if (b->p_per_sm[i] == 0 || i == 3) {  // the tile form's shared memory varies
     int coop = 0;
     BFVM_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, b->device));
     require(coop != 0, "batch: the device cannot launch cooperative kernels", BFVM_ERR_CUDA);
     BFVM_CUDA(cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, b->device));
     size_t smem = 0;
-    const void* k = persistent_kernel(ch, &smem);
+    const void* k = persistent_kernel(b, ch, &smem);
+    allow_persistent_smem(k, smem);
     int per = 0;
     BFVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, kBatchStepsThreads, smem));
     require(per > 0, "batch: the persistent kernel cannot be resident", BFVM_ERR_CUDA);
@@ -564,7 +578,7 @@ void enqueue_persistent_group(bfvm_batch* b, size_t gi, double dt, int nsteps,
   a.sources = sources ? 1 : 0;
   const int blocks = persistent_blocks(b, G);
   size_t smem = 0;
-  const void* kern = persistent_kernel(b->cfg.pch, &smem);
+  const void* kern = persistent_kernel(b, b->cfg.pch, &smem);
   cudaLaunchConfig_t cfg;
   std::memset(&cfg, 0, sizeof cfg);
   cfg.gridDim = dim3((unsigned)blocks);
@@ -869,7 +883,7 @@ void batch_tune(bfvm_batch* b, double dt, int flags, int trial_steps) {
     // 3. the mode (and the persistent kernel's chunk length) and the group
     // budget, whole steps
     bool any_persistent = false;
-    for (const bfvm_solver* m : b->inst) any_persistent = any_persistent || persistent_ok(m);
+    for (const bfvm_solver* m : b->inst) any_persistent = any_persistent || persistent_ok(m, 8);
     float best_ms = 1e30f;
     int64_t best_budget = 0;
     int best_mode = BFVM_BATCH_FUSED, best_pch = best.pch;

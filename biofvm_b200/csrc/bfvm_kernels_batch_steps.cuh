@@ -497,9 +497,30 @@ __global__ void __launch_bounds__(kBatchStepsThreads, 8) batch_lines_kernel(cons
 constexpr int kBatchTileCols = 32;
 constexpr int kBatchTileCh = 32;
 
+// Chunk tables of member m for axis AX in shared memory: k1 | kg | kc, each
+// section 16-byte aligned (the layout of the member's own table buffer).
+// Returns the number of doubles.
+template <int AX>
+__device__ __forceinline__ int tile_tables_doubles(const StepMember& m) {
+  const int n = AX == 0 ? m.nx : (AX == 1 ? m.ny : m.nz);
+  const int nc = (n + kBatchTileCh - 1) / kBatchTileCh;
+  const int kx = nc * kBatchTileCh * m.S * 2;
+  return 2 * kx + nc * m.S * 4;
+}
+
+template <int AX>
+__device__ __forceinline__ void stage_tile_tables(const StepMember& m, double* tab) {
+  // k1 and kg are adjacent in the member's buffer (kx doubles each, kx even)
+  // and kc follows kg directly: one contiguous copy
+  const int nd = tile_tables_doubles<AX>(m);
+  const double2* src = reinterpret_cast<const double2*>(m.ck1[AX]);
+  double2* dst = reinterpret_cast<double2*>(tab);
+  for (int i = threadIdx.x; i < nd / 2; i += blockDim.x) dst[i] = __ldcg(src + i);
+}
+
 template <int AX>
 __device__ __forceinline__ void member_tile32(const StepMember& m, int tile, Pair<double>* fold,
-                                              bool sources_after, double dt) {
+                                              const double* tab, bool sources_after, double dt) {
   constexpr int CH = kBatchTileCh, W = kBatchTileCols;
   const int S = m.S;
   const int plane = m.nx * m.ny;
@@ -508,6 +529,9 @@ __device__ __forceinline__ void member_tile32(const StepMember& m, int tile, Pai
   const int outer_stride = AX == 0 ? m.nx * S : (AX == 1 ? plane * S : 0);
   const int ls = C;
   const int NC = m.nc[AX];
+  const int kx = NC * CH * S * 2;
+  const double* k1 = tab;
+  const double* kg = tab + kx;
   const int tx = threadIdx.x % W;
   const int c = threadIdx.x / W;  // chunk; threads past NC chunks idle
   const int k0 = c * CH;
@@ -528,8 +552,8 @@ __device__ __forceinline__ void member_tile32(const StepMember& m, int tile, Pai
     dptr += off;
     if (m.dirichlet) nodes = chunk_bits(m.dir_mask[AX], line, k0);
   }
-  // the field moves through L2 only (__ldcg / __stcg), so that L1 keeps the
-  // chunk tables, which the recurrences wait on
+  // the field moves through L2 only (__ldcg / __stcg); the tables are in
+  // shared memory
   double v[CH];
   if (nodes == 0ull) {
 #pragma unroll
@@ -542,15 +566,15 @@ __device__ __forceinline__ void member_tile32(const StepMember& m, int tile, Pai
   }
   const int row = (k0 * S + s) * 2;
   double qe = 0.0, x0 = 0.0;
-  chunk_local<false, double, CH>(v, len, m.ck1[AX] + row, S, qe, x0);
+  chunk_local<true, double, CH>(v, len, k1 + row, S, qe, x0);
   if (c < NC) st_fold(fold + c * W + tx, qe, x0);
   __syncthreads();
   if (len > 0) {
-    ChunkCoef<double> tab;
-    tab.kc = m.ckc[AX];
+    ChunkCoef<double> ct;
+    ct.kc = tab + 2 * kx;
     double cf, cb;
-    chunk_carries<false, double>(fold, W, tx, c, NC, tab, s, S, cf, cb);
-    chunk_fix<false, double, CH>(v, len, m.ckg[AX] + row, S, cf, cb);
+    chunk_carries<true, double>(fold, W, tx, c, NC, ct, s, S, cf, cb);
+    chunk_fix<true, double, CH>(v, len, kg + row, S, cf, cb);
     if (AX == 2 && sources_after && (m.bulk || m.cells)) {
       const unsigned long long flagged = chunk_bits(m.src_mask, line, k0);
       if (flagged != 0ull) {
@@ -570,33 +594,40 @@ __device__ __forceinline__ void member_tile32(const StepMember& m, int tile, Pai
 
 template <int AX>
 __device__ __forceinline__ void batch_axis_tiles(const BatchStepsArgs& a, Pair<double>* fold,
-                                                 bool sources_after) {
-  int mi = 0;
+                                                 double* tab, bool sources_after) {
+  int mi = 0, staged = -1;
   for (int64_t t = blockIdx.x; t < a.tiles[AX]; t += gridDim.x) {
     while (mi + 1 < a.nmem && __ldg(&a.mem[mi + 1].tile0[AX]) <= t) ++mi;
     const StepMember& m = a.mem[mi];
-    member_tile32<AX>(m, (int)(t - m.tile0[AX]), fold, sources_after, a.dt);
+    if (mi != staged) {  // this member's tables for this axis into shared memory
+      stage_tile_tables<AX>(m, tab);
+      __syncthreads();
+      staged = mi;
+    }
+    member_tile32<AX>(m, (int)(t - m.tile0[AX]), fold, tab, sources_after, a.dt);
   }
+  __syncthreads();  // the tables are restaged by the next phase
 }
 
 // nsteps whole steps of every member in the tile form; launched
-// cooperatively with 128 threads and 4 x 32 (qe, x0) pairs of dynamic shared
-// memory per block.
+// cooperatively with 128 threads and, in dynamic shared memory, 4 x 32
+// (qe, x0) pairs plus the largest member's chunk tables of one axis.
 __global__ void __launch_bounds__(kBatchStepsThreads, 2) batch_tiles_kernel(const BatchStepsArgs a) {
   namespace cg = cooperative_groups;
   cg::grid_group grid = cg::this_grid();
   extern __shared__ __align__(16) unsigned char tiles_smem[];
   Pair<double>* fold = reinterpret_cast<Pair<double>*>(tiles_smem);
+  double* tab = reinterpret_cast<double*>(fold + 4 * kBatchTileCols);
   for (int step = 0; step < a.nsteps; ++step) {
     if (a.sources && step == 0) {
       batch_sources(a);
       grid.sync();
     }
-    batch_axis_tiles<0>(a, fold, false);
+    batch_axis_tiles<0>(a, fold, tab, false);
     grid.sync();
-    batch_axis_tiles<1>(a, fold, false);
+    batch_axis_tiles<1>(a, fold, tab, false);
     grid.sync();
-    batch_axis_tiles<2>(a, fold, a.sources && step + 1 < a.nsteps);
+    batch_axis_tiles<2>(a, fold, tab, a.sources && step + 1 < a.nsteps);
     grid.sync();
   }
 }

@@ -102,7 +102,7 @@ struct bfvm_batch {
   // 8- and 16-point kernels (0: not queried), SMs
   std::vector<bfvm_rt::MemberScratch> scratch;
   std::vector<std::vector<bfvm::StepMember>> pmembers;
-  int p_per_sm[4] = {0, 0, 0, 0};  // 8-, 16-point chunks, line form, tile form
+  int p_per_sm[5] = {0, 0, 0, 0, 0};  // 8-, 16-point chunks, line form, tile form, 4-point
   size_t tile_tab_doubles = 0;  // tile form: the largest member's tables of one axis
   int num_sms = 0;
   // cached graph and what it was captured for
@@ -499,6 +499,7 @@ const void* persistent_kernel(const bfvm_batch* b, int ch, size_t* smem) {
   *smem = ch == 32 ? 4 * kBatchTileCols * sizeof(bfvm::Pair<double>) +
                          b->tile_tab_doubles * sizeof(double)
                    : (ch > 0 ? 4 * kBatchStepsThreads * sizeof(double) : 0);
+  if (ch == 4) return (const void*)batch_steps_kernel<4>;
   if (ch == 8) return (const void*)batch_steps_kernel<8>;
   if (ch == 16) return (const void*)batch_steps_kernel<16>;
   if (ch == 32) return (const void*)batch_tiles_kernel;
@@ -506,7 +507,7 @@ const void* persistent_kernel(const bfvm_batch* b, int ch, size_t* smem) {
 }
 
 int persistent_per_sm(bfvm_batch* b, int ch) {
-  const int i = ch == 8 ? 0 : (ch == 16 ? 1 : (ch == 0 ? 2 : 3));
+  const int i = ch == 8 ? 0 : (ch == 16 ? 1 : (ch == 0 ? 2 : (ch == 32 ? 3 : 4)));
   if (b->p_per_sm[i] == 0 || i == 3) {  // the tile form's shared memory varies
     int coop = 0;
     BFVM_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, b->device));
@@ -890,7 +891,7 @@ void batch_tune(bfvm_batch* b, double dt, int flags, int trial_steps) {
     for (int mode : {BFVM_BATCH_FUSED, BFVM_BATCH_BRANCHES, BFVM_BATCH_PERSISTENT}) {
       if (mode == BFVM_BATCH_PERSISTENT && (!any_persistent || !(flags & BFVM_STEP_DIFFUSION)))
         continue;
-      for (int pch : {8, 16, 32, 0}) {
+      for (int pch : {8, 4, 16, 32, 0}) {
         if (pch != 8 && mode != BFVM_BATCH_PERSISTENT) continue;
         for (int64_t budget : {(int64_t)0, (int64_t)b->l2_bytes, (int64_t)b->l2_bytes / 2,
                                (int64_t)b->l2_bytes / 4, (int64_t)b->l2_bytes / 8}) {
@@ -1062,8 +1063,8 @@ int bfvm_batch_get_mode(bfvm_batch* b, int* mode) {
 
 int bfvm_batch_set_persistent_chunk(bfvm_batch* b, int chunk) {
   return BATCH_CALL(b, {
-    require(chunk == 0 || chunk == 8 || chunk == 16 || chunk == 32,
-            "persistent chunk must be 8, 16, 32 or 0 (whole lines)");
+    require(chunk == 0 || chunk == 4 || chunk == 8 || chunk == 16 || chunk == 32,
+            "persistent chunk must be 4, 8, 16, 32 or 0 (whole lines)");
     b->cfg.pch = chunk;
   });
 }

@@ -295,7 +295,7 @@ __device__ __forceinline__ void batch_sources(const BatchStepsArgs& a) {
 // to 128 points in at most 16 or 8 chunks); launched cooperatively with 128
 // threads and 4 * 128 doubles of dynamic shared memory per block.
 template <int CH>
-__global__ void __launch_bounds__(kBatchStepsThreads) batch_steps_kernel(const BatchStepsArgs a) {
+__global__ void __launch_bounds__(kBatchStepsThreads, 6) batch_steps_kernel(const BatchStepsArgs a) {
   namespace cg = cooperative_groups;
   cg::grid_group grid = cg::this_grid();
   extern __shared__ double batch_carries[];

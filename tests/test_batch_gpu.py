@@ -284,7 +284,7 @@ def test_set_mode_rejects_unknown_modes():
 # ---- persistent mode: all steps of a group's members in one cooperative
 # launch, phases shared by the members and separated by grid barriers ----
 
-@pytest.mark.parametrize("pchunk", [8, 16, 32, 0], ids=["ch8", "ch16", "tiles32", "lines"])
+@pytest.mark.parametrize("pchunk", [4, 8, 16, 32, 0], ids=["ch4", "ch8", "ch16", "tiles32", "lines"])
 @pytest.mark.parametrize("budget", [-1, 0, 200_000], ids=["default-groups", "one-group",
                                                          "small-groups"])
 def test_persistent_matches_oracle_per_member(pchunk, budget):

@@ -420,7 +420,7 @@ def test_persistent_fp32_members_run_on_branches():
 def test_persistent_chunk_setter_rejects_other_lengths():
     with Batch(0) as bt:
         with pytest.raises(BfvmError):
-            bt.set_persistent_chunk(4)
+            bt.set_persistent_chunk(12)
         bt.set_persistent_chunk(16)
         assert bt.get_persistent_chunk() == 16
         bt.set_persistent_chunk(0)

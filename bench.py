@@ -713,7 +713,13 @@ def run_batched(args, world, rank, local):
         bt.add(sv)
     reset()
     t0 = time.perf_counter()
-    bt.tune(dt, STEP_ALL, args.batch_trial_steps)
+    if args.batch_mode == "tuned":
+        bt.tune(dt, STEP_ALL, args.batch_trial_steps)
+    else:
+        from biofvm_b200._abi import BATCH_BRANCHES, BATCH_FUSED, BATCH_PERSISTENT
+        bt.set_mode({"fused": BATCH_FUSED, "branches": BATCH_BRANCHES,
+                     "persistent": BATCH_PERSISTENT}[args.batch_mode])
+        bt.set_persistent_chunk(args.batch_chunk)
     t_tune = time.perf_counter() - t0
     cfg = bt.get_config()
     pch = bt.get_persistent_chunk()
@@ -1281,6 +1287,10 @@ def main():
                     help="steps per trial run of the batch tuner")
     ap.add_argument("--batch-modes", action="store_true",
                     help="batched: also time every batch mode with the tuned group budget")
+    ap.add_argument("--batch-mode", choices=["tuned", "fused", "branches", "persistent"],
+                    default="tuned", help="batched: the tuner's choice, or one mode untuned")
+    ap.add_argument("--batch-chunk", type=int, default=8,
+                    help="batched, persistent mode untuned: 4, 8, 16, 32 or 0 (whole lines)")
     args = ap.parse_args()
     if args.workload == "batched" and "--steps" not in sys.argv:
         args.steps = 200

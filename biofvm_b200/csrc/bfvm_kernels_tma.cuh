@@ -82,12 +82,10 @@ struct ChunkCoef {
   const T* k1;    // [slot][ch][S][2] {1/d, a}
   const T* kg;    // [slot][ch][S][2] {G, R}
   const T* kc;    // [chunk][S][4] {P_end, G_start, R_start, 0}
-  const T* ku;    // [slot][S] 1 where {1/d, a} are the same at every point of
-                  // the slot's chunk for that density (converged interior), else 0
   const int* slot;  // [nc] slot of each chunk of the line
   int ch;
   int nc;
-  int tab_elems;  // elements of k1 | kg | kc | ku, contiguous from k1
+  int tab_elems;  // elements of k1 | kg | kc, contiguous from k1
 };
 
 // Copies the chunk tables (k1 | kg | kc, contiguous) and the slot map into
@@ -105,7 +103,6 @@ __device__ __forceinline__ ChunkCoef<T> stage_tables(const ChunkCoef<T>& g, T* s
   s.k1 = sm_tab;
   s.kg = sm_tab + (g.kg - g.k1);
   s.kc = sm_tab + (g.kc - g.k1);
-  s.ku = sm_tab + (g.ku - g.k1);
   s.slot = sm_slot;
   return s;
 }
@@ -114,12 +111,6 @@ __device__ __forceinline__ ChunkCoef<T> stage_tables(const ChunkCoef<T>& g, T* s
 template <bool SMEM, typename T>
 __device__ __forceinline__ size_t chunk_row(const ChunkCoef<T>& cc, int c, int s, int S) {
   return ((size_t)ld_one<SMEM>(cc.slot + c) * cc.ch * S + s) * 2;
-}
-
-// Whether chunk c's {1/d, a} are one pair for density s at every point.
-template <bool SMEM, typename T>
-__device__ __forceinline__ bool chunk_uniform(const ChunkCoef<T>& cc, int c, int s, int S) {
-  return ld_one<SMEM>(cc.ku + (size_t)ld_one<SMEM>(cc.slot + c) * S + s) != T(0);
 }
 
 template <typename T, typename CT = T>
@@ -194,37 +185,6 @@ __device__ __forceinline__ void chunk_local(T (&v)[CH], int len, const T* k1, in
   for (int m = CH - 1; m >= 0; --m) {
     if (m < len) {
       x = fma(ld_one<SMEM>(k1 + (size_t)2 * S * m + 1), x, v[m]);
-      v[m] = x;
-    }
-  }
-  x0 = x;
-}
-
-// chunk_local for a chunk whose {1/d, a} may be one pair at every point
-// (uni): then the pair is read once and the passes run on two registers, the
-// same operations on the same values as the table path.
-template <bool SMEM, typename T, int CH>
-__device__ __forceinline__ void chunk_local_u(T (&v)[CH], int len, const T* k1, int S, bool uni,
-                                              T& qe, T& x0) {
-  if (!uni) {
-    chunk_local<SMEM, T, CH>(v, len, k1, S, qe, x0);
-    return;
-  }
-  const Pair<T> c = ld_pair<SMEM>(k1);
-  T q = T(0);
-#pragma unroll
-  for (int m = 0; m < CH; ++m) {
-    if (m < len) {
-      q = fma(c.y, q, v[m] * c.x);
-      v[m] = q;
-    }
-  }
-  qe = q;
-  T x = T(0);
-#pragma unroll
-  for (int m = CH - 1; m >= 0; --m) {
-    if (m < len) {
-      x = fma(c.y, x, v[m]);
       v[m] = x;
     }
   }
@@ -367,9 +327,8 @@ __global__ void __launch_bounds__(W * MAXNC)
     for (int m = 0; m < CH; ++m) v[m] = (m < lenA) ? (CT)buf[m * W] : CT(0);
 
     const size_t row = chunk_row<SMEM_TAB>(tab, c, s, S);
-    const bool uni = chunk_uniform<SMEM_TAB>(tab, c, s, S);
     CT qe, x0;
-    chunk_local_u<SMEM_TAB, CT, CH>(v, lenA, tab.k1 + row, S, uni, qe, x0);
+    chunk_local<SMEM_TAB, CT, CH>(v, lenA, tab.k1 + row, S, qe, x0);
     Pair<CT>* sF = fold + (i & 1) * NC * W;
     st_fold(sF + c * W + tx, qe, x0);
     // every thread has read its chunk of this stage: it can be refilled
@@ -454,7 +413,6 @@ __global__ void __launch_bounds__(MAXT, rows_min_blocks(CH, MAXT))
   }
   __syncthreads();
   const size_t crow = (c < NC) ? chunk_row<SMEM_TAB>(tab, c, s, S) : 0;
-  const bool uni = (c < NC) && chunk_uniform<SMEM_TAB>(tab, c, s, S);
   const CT* k1 = tab.k1 + crow;
   const CT* kg = tab.kg + crow;
 
@@ -527,7 +485,7 @@ __global__ void __launch_bounds__(MAXT, rows_min_blocks(CH, MAXT))
 
     // ---- sweep
     CT qe, x0;
-    chunk_local_u<SMEM_TAB, CT, CH>(v, lenA, k1, S, uni, qe, x0);
+    chunk_local<SMEM_TAB, CT, CH>(v, lenA, k1, S, qe, x0);
     Pair<CT>* sF = fold + (i & 1) * NC * FW;
     if (c < NC && fc < FW) st_fold(sF + c * FW + fc, qe, x0);
     // every thread has its chunk in registers: the stage can be refilled
@@ -664,9 +622,8 @@ __global__ void __launch_bounds__(512) lod_sweep_direct_kernel(const DirectArgs<
   tab.kc = kc_sm;
   tab.slot = slot_sm;
   const size_t row = active ? ((size_t)slot_sm[c] * tab.ch * S + s) * 2 : 0;
-  const bool uni = active && __ldg(a.cc.ku + (size_t)slot_sm[c] * S + s) != CT(0);
   CT qe, x0;
-  chunk_local_u<false, CT, CH>(v, lenA, a.cc.k1 + row, S, uni, qe, x0);
+  chunk_local<false, CT, CH>(v, lenA, a.cc.k1 + row, S, qe, x0);
   st_fold(fold + c * W + tx, qe, x0);
   __syncthreads();
   CT cf, cb;

@@ -256,21 +256,11 @@ bfvm::ChunkCoef<T> chunk_view(bfvm_solver* m, int a) {
     }
     const size_t ns_ = slot_chunk.size();
     const size_t k1n = up4(ns_ * cw), kgn = up4(ns_ * cw), kcn = up4((size_t)nc * S * 4);
-    const size_t kun = up4(ns_ * S);
-    std::vector<double> tab(k1n + kgn + kcn + kun, 0.0);
+    std::vector<double> tab(k1n + kgn + kcn, 0.0);
     for (size_t sl = 0; sl < ns_; ++sl) {
       const int r = slot_chunk[sl];
       std::copy_n(&k1[r * cw], cw, &tab[sl * cw]);
       std::copy_n(&kg[r * cw], cw, &tab[k1n + sl * cw]);
-      // one {1/d, a} pair at every point of the chunk (per density)?
-      const int len = std::min(ch, n - r * ch);
-      for (int s = 0; s < S; ++s) {
-        bool same = true;
-        for (int mm = 1; mm < len && same; ++mm)
-          same = std::memcmp(&k1[r * cw + ((size_t)mm * S + s) * 2],
-                             &k1[r * cw + (size_t)s * 2], 2 * sizeof(double)) == 0;
-        tab[k1n + kgn + kcn + sl * S + s] = same ? 1.0 : 0.0;
-      }
     }
     // transfer constants per chunk (not per slot): the fold reads every chunk
     std::copy_n(kc.data(), (size_t)nc * S * 4, &tab[k1n + kgn]);
@@ -286,17 +276,16 @@ bfvm::ChunkCoef<T> chunk_view(bfvm_solver* m, int a) {
   }
   const size_t cw = (size_t)ch * S * 2;
   const size_t ns_ = (size_t)m->chunk_nslots[a];
-  const size_t k1n = up4(ns_ * cw), kgn = up4(ns_ * cw), kcn = up4((size_t)nc * S * 4);
+  const size_t k1n = up4(ns_ * cw), kgn = up4(ns_ * cw);
   const T* base = m->chunk[a].as<T>();
   bfvm::ChunkCoef<T> c;
   c.k1 = base;
   c.kg = base + k1n;
   c.kc = base + k1n + kgn;
-  c.ku = base + k1n + kgn + kcn;
   c.slot = m->chunk_slots[a].as<int>();
   c.ch = ch;
   c.nc = nc;
-  c.tab_elems = (int)(k1n + kgn + kcn + up4(ns_ * S));
+  c.tab_elems = (int)(k1n + kgn + up4((size_t)nc * S * 4));
   const T* vec_sections[3] = {c.k1, c.kg, c.kc};
   for (const T* q : vec_sections)
     require(reinterpret_cast<uintptr_t>(q) % (2 * sizeof(T)) == 0,
@@ -689,7 +678,7 @@ size_t table_bytes(const bfvm_solver* m, int a) {
   const int ns[3] = {m->nx, m->ny, m->nz};
   const size_t ch = m->axis[a].ch, S = m->S, nsl = m->chunk_nslots[a];
   const size_t nc = (ns[a] + ch - 1) / ch;
-  const size_t elems = up4(nsl * ch * S * 2) * 2 + up4(nc * S * 4) + up4(nsl * S);
+  const size_t elems = up4(nsl * ch * S * 2) * 2 + up4(nc * S * 4);
   return elems * m->math_elem() + nc * sizeof(int) + 16;
 }
 

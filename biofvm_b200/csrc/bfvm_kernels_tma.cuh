@@ -367,8 +367,11 @@ __global__ void __launch_bounds__(W * MAXNC)
 // two resident blocks per SM (the plan sizes their shared memory for two).
 constexpr int rows_min_blocks(int ch, int maxt) { return (ch <= 16 && maxt <= 256) ? 2 : 1; }
 
-template <typename T, int CH, int STAGES, bool SMEM_TAB, int MAXT, typename CT = T>
-__global__ void __launch_bounds__(MAXT, rows_min_blocks(CH, MAXT))
+// MINB: resident blocks per SM the kernel is compiled for (two at 32-point
+// chunks caps the registers at 128: more warps, some spilled state).
+template <typename T, int CH, int STAGES, bool SMEM_TAB, int MAXT, typename CT = T,
+          int MINB = rows_min_blocks(CH, MAXT)>
+__global__ void __launch_bounds__(MAXT, MINB)
     lod_rows_tma_kernel(const RowsArgs<T, CT> a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   // Threads: column (r, s) fastest, then chunk c.  A stage holds R rows at a

@@ -756,6 +756,7 @@ struct RowsPlan {
   bool smem_tab = false;
   int ch = 0, nc = 0, R = 0, stages = 0, maxt = 256;
   int tpc = 0;  // threads per chunk
+  int minb = 1;  // resident blocks per SM the kernel is compiled for
   int64_t pitch = 0;
   size_t smem = 0;
 };
@@ -801,8 +802,11 @@ RowsPlan plan_rows(const bfvm_solver* m) {
   // register file (32-point chunks).
   for (int maxt : {256, 512}) {
     if (cols > maxt) continue;
-    const size_t budget =
-        bfvm::rows_min_blocks(P.ch, maxt) == 2 ? 113 * 1024 : kSmemBudget;
+    // two blocks per SM also at 32-point chunks where the axis asks for it
+    const int minb = (maxt == 256 && P.ch == 32 && m->axis[0].minb == 2)
+                         ? 2
+                         : bfvm::rows_min_blocks(P.ch, maxt);
+    const size_t budget = minb == 2 ? 113 * 1024 : kSmemBudget;
     for (int staged = 1; staged >= 0; --staged) {
       if (staged && tab == 0) continue;
       for (int R = (int)std::min<int64_t>(maxt / cols, rows); R >= 1; --R) {
@@ -817,6 +821,7 @@ RowsPlan plan_rows(const bfvm_solver* m) {
         const int fw = R * m->S, fw32 = (fw + 31) / 32 * 32;
         P.tpc = fw32 * P.nc <= maxt ? fw32 : fw;
         P.stages = nst;
+        P.minb = minb;
         P.maxt = maxt;
         P.smem_tab = staged != 0;
         P.smem = smem;
@@ -1019,9 +1024,10 @@ bool launch_direct(bfvm_solver* m, int ax, int fuse, double dt, int64_t z0 = 0,
   return true;
 }
 
-template <typename T, typename CT, int CH, bool TAB, int MAXT, int ST>
+template <typename T, typename CT, int CH, bool TAB, int MAXT, int ST,
+          int MINB = bfvm::rows_min_blocks(CH, MAXT)>
 void launch_rows_inst(const bfvm::RowsArgs<T, CT>& a, dim3 block, size_t smem, bfvm_solver* m) {
-  auto k = bfvm::lod_rows_tma_kernel<T, CH, ST, TAB, MAXT, CT>;
+  auto k = bfvm::lod_rows_tma_kernel<T, CH, ST, TAB, MAXT, CT, MINB>;
   allow_smem((const void*)k, m->device, smem);
   int per_sm = 0;
   BFVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, block.x * block.y, smem));
@@ -1032,7 +1038,12 @@ void launch_rows_inst(const bfvm::RowsArgs<T, CT>& a, dim3 block, size_t smem, b
 
 template <typename T, typename CT, int CH, int ST>
 void launch_rows_st(const bfvm::RowsArgs<T, CT>& a, const RowsPlan& P, dim3 block, bfvm_solver* m) {
-  if (P.maxt == 256) {
+  if (P.maxt == 256 && CH == 32 && P.minb == 2) {
+    if (P.smem_tab)
+      launch_rows_inst<T, CT, CH, true, 256, ST, 2>(a, block, P.smem, m);
+    else
+      launch_rows_inst<T, CT, CH, false, 256, ST, 2>(a, block, P.smem, m);
+  } else if (P.maxt == 256) {
     if (P.smem_tab)
       launch_rows_inst<T, CT, CH, true, 256, ST>(a, block, P.smem, m);
     else
@@ -2454,7 +2465,7 @@ void tune_sweeps(bfvm_solver* m, double dt, int reps) {
   BFVM_CUDA(cudaEventCreate(&e0));
   BFVM_CUDA(cudaEventCreate(&e1));
   struct Choice {
-    int kind, ch, tw, stages;
+    int kind, ch, tw, stages, minb;
   };
   const int ns[3] = {m->nx, m->ny, m->nz};
   const int fuses[3] = {bfvm::kFuseDirPro | bfvm::kFuseDirEpi, bfvm::kFuseDirEpi, 0};
@@ -2467,13 +2478,15 @@ void tune_sweeps(bfvm_solver* m, double dt, int reps) {
         if (nc > 64) continue;
         for (int tw : {32, 16, 8})
           if (nc * tw <= bfvm::sweep_max_threads(ch))
-            cand.push_back({BFVM_PATH_GENERIC, ch, tw, 0});
+            cand.push_back({BFVM_PATH_GENERIC, ch, tw, 0, 1});
         // the line kernel (y, z) also takes 17-32 chunks of 32 points
         if (nc <= 16 || (ax > 0 && ch == 32 && nc <= 32))
-          cand.push_back({BFVM_PATH_TMA, ch, 16, 0});
-        // the row kernel (x) with a ring of three tiles
-        if (ax == 0 && nc <= 16) cand.push_back({BFVM_PATH_TMA, ch, 16, 3});
-        if (nc <= 16) cand.push_back({BFVM_PATH_DIRECT, ch, 16, 0});
+          cand.push_back({BFVM_PATH_TMA, ch, 16, 0, 1});
+        // the row kernel (x) with a ring of three tiles, and at 32-point
+        // chunks compiled for two blocks per SM
+        if (ax == 0 && nc <= 16) cand.push_back({BFVM_PATH_TMA, ch, 16, 3, 1});
+        if (ax == 0 && nc <= 16 && ch == 32) cand.push_back({BFVM_PATH_TMA, ch, 16, 0, 2});
+        if (nc <= 16) cand.push_back({BFVM_PATH_DIRECT, ch, 16, 0, 1});
       }
       Axis best = m->axis[ax];
       float best_ms = 1e30f;
@@ -2482,7 +2495,7 @@ void tune_sweeps(bfvm_solver* m, double dt, int reps) {
         if (A.ch != c.ch) m->bulk_dirty = m->dir_dirty = m->ag_seg_dirty = true;
         A.ch = c.ch;
         A.tw = c.tw;
-        A.minb = 1;
+        A.minb = c.minb;
         A.kind = c.kind;
         A.stages = c.stages;
         A.user = true;

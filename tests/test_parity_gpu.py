@@ -516,17 +516,20 @@ def test_sweep_tuner_keeps_the_field_and_the_results(shape):
 @pytest.mark.parametrize("shape,S", [((256, 12, 9), 10), ((160, 20, 7), 4), ((96, 9, 5), 7)])
 def test_row_kernel_with_three_stage_ring(shape, S):
     """The x row kernel with a ring of three tiles (and whole warps per
-    chunk) against the oracle, next to the two-tile ring."""
+    chunk) against the oracle, next to the two-tile ring, and compiled for
+    two blocks per SM at 32-point chunks."""
     scn = W.mixed_small(shape=shape, S=S, n_agents=500, seed=sum(shape) + S)
     ref = O.oracle_run(scn, 3, 7)
-    for stages in (2, 3):
+    for stages, minb in ((2, 1), (3, 1), (2, 2)):
         with Solver(0) as sv:
             load_scenario(sv, scn)
             sv.set_kernel_path(PATH_TMA)
+            if minb == 2:
+                sv.set_sweep_config(0, 32, 16, 2)
             sv.set_row_stages(stages)
             sv.step(scn.dt, 3)
             assert sv.get_sweep_config(0)[3] == stages
-            assert np.all(rel_err(sv.get_densities(), ref) <= TOL64), stages
+            assert np.all(rel_err(sv.get_densities(), ref) <= TOL64), (stages, minb)
 
 
 # ---- x and y sweeps by slabs of z planes (bfvm_set_slab_planes) ----

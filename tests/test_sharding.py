@@ -205,3 +205,60 @@ def test_z_slab_of_one_rank_over_nccl(tmp_path):
     _run_ranks(_zslab_main, 1, ("nccl", (13, 11, 17), str(tmp_path)))
     scn = W.mixed_small(shape=(13, 11, 17), S=3, n_agents=400, seed=37)
     assert np.all(O.max_rel_err(np.load(tmp_path / "z0.npy"), O.oracle_run(scn, 4, 7)) <= 1e-12)
+
+
+@pytest.mark.parametrize("bounds", [[0, 5, 6, 11, 17], [0, 17], [0, 1, 2, 3, 17], [0, 9, 17]])
+def test_z_slab_join_algebra(bounds):
+    """The join of bfvm_zslab_fixup restated in numpy on one z line: every
+    slab solves its segment with the whole line's Thomas rows and zero
+    carries at its ends (x'); the carries folded from the slabs' first and
+    last values give x = x' + C G + X Rk, equal to the whole-line solve."""
+    from oracle import oracle as O
+
+    n, S = bounds[-1], 2
+    rng = np.random.default_rng(len(bounds))
+    D, decay = np.array([3.7e4, 900.0]), np.array([0.3, 0.02])
+    c1, den, cx = O.oracle_thomas(n, S, 10.0, 0.01, D, decay)
+    p = rng.random((n, S))
+    # the reference's sequence on the whole line
+    ref = p.copy()
+    ref[0] /= den[0]
+    for k in range(1, n):
+        ref[k] = (ref[k] + c1 * ref[k - 1]) / den[k]
+    for k in range(n - 2, -1, -1):
+        ref[k] -= cx[k] * ref[k + 1]
+    a = -cx  # forward and backward slopes (c = a except at the line end)
+    c = np.where(np.arange(n)[:, None] + 1 < n, -cx, 0.0)
+    R = len(bounds) - 1
+    local, cst, pts = [], [], []
+    for r in range(R):
+        g0, g1 = bounds[r], bounds[r + 1]
+        q, x = np.zeros((g1 - g0, S)), np.zeros((g1 - g0, S))
+        prev = np.zeros(S)
+        for k in range(g0, g1):
+            prev = (p[k] + c1 * prev) / den[k]
+            q[k - g0] = prev
+        nxt = np.zeros(S)
+        for k in range(g1 - 1, g0 - 1, -1):
+            nxt = q[k - g0] + c[k] * nxt
+            x[k - g0] = nxt
+        A = np.cumprod(a[g0:g1], axis=0)
+        G, Rk = np.zeros((g1 - g0 + 1, S)), np.ones((g1 - g0 + 1, S))
+        for k in range(g1 - 1, g0 - 1, -1):
+            G[k - g0] = A[k - g0] + c[k] * G[k - g0 + 1]
+            Rk[k - g0] = c[k] * Rk[k - g0 + 1]
+        local.append(x)
+        cst.append((A[-1], G[0], Rk[0]))
+        pts.append((G[:-1], Rk[:-1]))
+    out = np.zeros((n, S))
+    for rank in range(R):
+        Q, C = np.zeros(S), []
+        for r in range(R):
+            C.append(Q)
+            Q = cst[r][0] * Q + local[r][-1]
+        X = np.zeros(S)
+        for r in range(R - 1, rank, -1):
+            X = local[r][0] + C[r] * cst[r][1] + cst[r][2] * X
+        g0, g1 = bounds[rank], bounds[rank + 1]
+        out[g0:g1] = local[rank] + C[rank] * pts[rank][0] + X * pts[rank][1]
+    assert np.all(np.abs(out - ref).max(axis=0) / np.abs(ref).max(axis=0) <= 1e-13)

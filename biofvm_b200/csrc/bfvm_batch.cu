@@ -625,6 +625,11 @@ void plan(bfvm_batch* b, int flags) {
     build_plan<double>(b, flags);
   else
     build_plan<float>(b, flags);
+  // the persistent kernel's shared-memory limit and occupancy, settled here,
+  // outside any graph capture
+  bool any_persistent = false;
+  for (const GroupPlan& G : b->groups) any_persistent = any_persistent || G.persistent;
+  if (any_persistent) persistent_per_sm(b, b->cfg.pch);
   b->d_desc.ensure(std::max<size_t>(b->host_desc.size(), 64));
   BFVM_CUDA(cudaMemcpyAsync(b->d_desc.ptr, b->host_desc.data(), b->host_desc.size(),
                             cudaMemcpyHostToDevice, b->stream));

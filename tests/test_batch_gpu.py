@@ -417,6 +417,20 @@ def test_persistent_fp32_members_run_on_branches():
         assert np.all(O.max_rel_err(p, ref) <= 1e-5), scn.shape
 
 
+@pytest.mark.parametrize("pchunk", [32, 8])
+def test_persistent_many_densities(pchunk):
+    """Members with 12 and 20 densities: the tile form stages chunk tables of
+    more than 48 KB in shared memory (the kernel's limit is raised while the
+    batch is planned); every form matches the oracle."""
+    scns = [W.mixed_small(shape=(70, 40, 33), S=12, n_agents=200, seed=301),
+            W.mixed_small(shape=(128, 21, 17), S=20, n_agents=100, seed=302),
+            W.mixed_small(shape=(20, 31, 90), S=3, n_agents=50, seed=303)]
+    got, _ = run_batch(scns, 3, mode=BATCH_PERSISTENT, pchunk=pchunk)
+    for scn, p in zip(scns, got):
+        ref = O.oracle_run(scn, 3, 7)
+        assert np.all(O.max_rel_err(p, ref) <= TOL64), (pchunk, scn.shape, scn.S)
+
+
 def test_persistent_chunk_setter_rejects_other_lengths():
     with Batch(0) as bt:
         with pytest.raises(BfvmError):

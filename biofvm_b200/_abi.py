@@ -73,6 +73,9 @@ SIGNATURES = {
     "bfvm_get_num_dirichlet_nodes": (c_int, [_P, _LP]),
     "bfvm_set_agents": (c_int, [_P, c_int64, _LP, _DP, _DP]),
     "bfvm_get_agent_densities": (c_int, [_P, _DP]),
+    "bfvm_set_agents_async": (c_int, [_P, c_int64, _LP, _DP, _DP]),
+    "bfvm_get_agent_densities_async": (c_int, [_P, _DP]),
+    "bfvm_wait_transfers": (c_int, [_P]),
     "bfvm_simulate_bulk_sources_and_sinks": (c_int, [_P, c_double]),
     "bfvm_simulate_cell_sources_and_sinks": (c_int, [_P, c_double]),
     "bfvm_simulate_diffusion_decay": (c_int, [_P, c_double]),

@@ -437,32 +437,36 @@ void build_dirichlet(bfvm_solver* m) {
 
 // Agents stably sorted by voxel on the device (radix sort of (voxel, list
 // position) pairs; a radix sort is stable, so agents of one voxel keep their
-// list order, BioFVM_microenvironment.cpp:626-633).
+// list order, BioFVM_microenvironment.cpp:626-633): keys[A] (voxels, checked
+// to lie in [0, N)) into key/idx, on stream st.
+void sort_agents(int64_t A, int64_t N, const uint64_t* keys_in, DevBuf& key, DevBuf& idx_in,
+                 DevBuf& idx, DevBuf& tmp_buf, cudaStream_t st, bfvm_solver* m) {
+  key.ensure(A * sizeof(uint64_t));
+  idx_in.ensure(A * sizeof(int));
+  idx.ensure(A * sizeof(int));
+  bfvm::iota_kernel<<<(unsigned)blocks_for(A, 256), 256, 0, st>>>(idx_in.as<int>(), A);
+  check_launch(m);
+  int end_bit = 1;
+  while (end_bit < 63 && ((int64_t)1 << end_bit) < N) ++end_bit;
+  // as unsigned keys the (non-negative) voxel indices sort like the signed values
+  size_t tmp = 0;
+  BFVM_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, keys_in, key.as<uint64_t>(),
+                                            idx_in.as<int>(), idx.as<int>(), (int)A, 0, end_bit,
+                                            st));
+  tmp_buf.ensure(std::max<size_t>(tmp, 16));
+  BFVM_CUDA(cub::DeviceRadixSort::SortPairs(tmp_buf.ptr, tmp, keys_in, key.as<uint64_t>(),
+                                            idx_in.as<int>(), idx.as<int>(), (int)A, 0, end_bit,
+                                            st));
+}
+
 void build_agents(bfvm_solver* m) {
   if (!m->ag_dirty) return;
   ++m->lists_version;
   const int64_t A = m->n_agents;
   m->ag_dirty = false;
   if (A == 0) return;
-  cudaStream_t st = m->stream;
-  m->d_ag_key.ensure(A * sizeof(uint64_t));
-  m->d_ag_idx_in.ensure(A * sizeof(int));
-  m->d_ag_idx.ensure(A * sizeof(int));
-  bfvm::iota_kernel<<<(unsigned)blocks_for(A, 256), 256, 0, st>>>(m->d_ag_idx_in.as<int>(), A);
-  check_launch(m);
-  int end_bit = 1;
-  while (end_bit < 63 && ((int64_t)1 << end_bit) < m->N()) ++end_bit;
-  // voxel indices were checked to lie in [0, N): as unsigned keys they sort
-  // like the signed values
-  const uint64_t* keys_in = m->d_ag_vox_orig.as<uint64_t>();
-  size_t tmp = 0;
-  BFVM_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, keys_in, m->d_ag_key.as<uint64_t>(),
-                                            m->d_ag_idx_in.as<int>(), m->d_ag_idx.as<int>(),
-                                            (int)A, 0, end_bit, st));
-  m->d_sort_tmp.ensure(std::max<size_t>(tmp, 16));
-  BFVM_CUDA(cub::DeviceRadixSort::SortPairs(m->d_sort_tmp.ptr, tmp, keys_in,
-                                            m->d_ag_key.as<uint64_t>(), m->d_ag_idx_in.as<int>(),
-                                            m->d_ag_idx.as<int>(), (int)A, 0, end_bit, st));
+  sort_agents(A, m->N(), m->d_ag_vox_orig.as<uint64_t>(), m->d_ag_key, m->d_ag_idx_in,
+              m->d_ag_idx, m->d_sort_tmp, m->stream, m);
 }
 
 // Segment lists of the agents for the fused x-sweep prologue: entries grouped
@@ -1404,6 +1408,36 @@ template void dirichlet_standalone<double>(bfvm_solver* m);
 
 using namespace bfvm_rt;
 
+// Upload and download streams of the asynchronous agent exchange and their
+// events, created on first use.
+void ensure_transfer_streams(bfvm_solver* m) {
+  if (m->xf_down_done) return;  // created last
+  if (!m->xf_up) BFVM_CUDA(cudaStreamCreateWithFlags(&m->xf_up, cudaStreamNonBlocking));
+  if (!m->xf_down) BFVM_CUDA(cudaStreamCreateWithFlags(&m->xf_down, cudaStreamNonBlocking));
+  for (cudaEvent_t* e : {&m->xf_up_done, &m->xf_spare_free, &m->xf_gathered, &m->xf_down_done})
+    if (!*e) BFVM_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+}
+
+// Both transfer streams drained (the host arrays of the asynchronous calls
+// are free, their outputs written).
+void wait_transfers(bfvm_solver* m) {
+  if (m->xf_up_pending) BFVM_CUDA(cudaEventSynchronize(m->xf_up_done));
+  if (m->xf_down_pending) BFVM_CUDA(cudaEventSynchronize(m->xf_down_done));
+  m->xf_up_pending = m->xf_down_pending = false;
+}
+
+// The densities at the agents' voxels into d_gather [A][S] FP64, after any
+// copy out of d_gather still running on the download stream.
+void gather_agents(bfvm_solver* m) {
+  const int64_t A = m->n_agents;
+  if (m->xf_down_pending) BFVM_CUDA(cudaStreamWaitEvent(m->stream, m->xf_down_done, 0));
+  m->d_gather.ensure(A * m->S * sizeof(double));
+  if (m->precision == BFVM_FP64)
+    gather<double>(m, A, m->d_ag_vox_orig.as<int64_t>(), m->d_gather.as<double>());
+  else
+    gather<float>(m, A, m->d_ag_vox_orig.as<int64_t>(), m->d_gather.as<double>());
+}
+
 extern "C" {
 
 const char* bfvm_last_error(void) { return g_last_error.c_str(); }
@@ -1438,6 +1472,15 @@ int bfvm_destroy(bfvm_solver* m) {
     if (!m) return;
     DeviceGuard dg(m->device);
     cudaStreamSynchronize(m->stream);
+    for (cudaStream_t x : {m->xf_up, m->xf_down})
+      if (x) cudaStreamSynchronize(x);
+    for (DevBuf* d : {&m->xf_vox, &m->xf_t1, &m->xf_t2, &m->xf_key, &m->xf_idx_in, &m->xf_idx,
+                      &m->xf_sort_tmp})
+      d->release();
+    for (cudaEvent_t e : {m->xf_up_done, m->xf_spare_free, m->xf_gathered, m->xf_down_done})
+      if (e) cudaEventDestroy(e);
+    for (cudaStream_t x : {m->xf_up, m->xf_down})
+      if (x) cudaStreamDestroy(x);
     m->p.release();
     for (auto& c : m->coef) c.release();
     m->d_bulk_vox.release();
@@ -1899,15 +1942,74 @@ int bfvm_get_agent_densities(bfvm_solver* m, double* values) {
     const int64_t A = m->n_agents;
     if (A == 0) return;
     require(values != nullptr, "null output buffer");
-    m->d_gather.ensure(A * m->S * sizeof(double));
-    if (m->precision == BFVM_FP64)
-      gather<double>(m, A, m->d_ag_vox_orig.as<int64_t>(), m->d_gather.as<double>());
-    else
-      gather<float>(m, A, m->d_ag_vox_orig.as<int64_t>(), m->d_gather.as<double>());
+    gather_agents(m);
     BFVM_CUDA(cudaMemcpyAsync(values, m->d_gather.ptr, A * m->S * sizeof(double),
                               cudaMemcpyDeviceToHost, m->stream));
     BFVM_CUDA(cudaStreamSynchronize(m->stream));
   });
+}
+
+int bfvm_set_agents_async(bfvm_solver* m, int64_t count, const int64_t* voxel,
+                          const double* temp1, const double* temp2) {
+  return SOLVER_CALL(m, {
+    require(count >= 0 && (count == 0 || (voxel && temp1 && temp2)), "bad arguments");
+    require(count < ((int64_t)1 << 31), "too many agents");
+    validate_voxels(m, count, voxel);
+    ensure_transfer_streams(m);
+    cudaStream_t up = m->xf_up;
+    // the spare set is still read by the steps enqueued before it was swapped out
+    if (m->xf_spare_recorded) BFVM_CUDA(cudaStreamWaitEvent(up, m->xf_spare_free, 0));
+    if (count > 0) {
+      const size_t tbytes = (size_t)count * m->S * sizeof(double);
+      m->xf_vox.ensure(count * sizeof(int64_t));
+      m->xf_t1.ensure(tbytes);
+      m->xf_t2.ensure(tbytes);
+      BFVM_CUDA(cudaMemcpyAsync(m->xf_vox.ptr, voxel, count * sizeof(int64_t),
+                                cudaMemcpyHostToDevice, up));
+      BFVM_CUDA(cudaMemcpyAsync(m->xf_t1.ptr, temp1, tbytes, cudaMemcpyHostToDevice, up));
+      BFVM_CUDA(cudaMemcpyAsync(m->xf_t2.ptr, temp2, tbytes, cudaMemcpyHostToDevice, up));
+      sort_agents(count, m->N(), m->xf_vox.as<uint64_t>(), m->xf_key, m->xf_idx_in, m->xf_idx,
+                  m->xf_sort_tmp, up, m);
+    }
+    BFVM_CUDA(cudaEventRecord(m->xf_up_done, up));
+    m->xf_up_pending = true;
+    // the current set becomes the spare once the work enqueued so far is done;
+    // work enqueued from here on reads the new set after its upload
+    BFVM_CUDA(cudaEventRecord(m->xf_spare_free, m->stream));
+    m->xf_spare_recorded = true;
+    BFVM_CUDA(cudaStreamWaitEvent(m->stream, m->xf_up_done, 0));
+    std::swap(m->d_ag_vox_orig, m->xf_vox);
+    std::swap(m->d_ag_t1, m->xf_t1);
+    std::swap(m->d_ag_t2, m->xf_t2);
+    std::swap(m->d_ag_key, m->xf_key);
+    std::swap(m->d_ag_idx_in, m->xf_idx_in);
+    std::swap(m->d_ag_idx, m->xf_idx);
+    std::swap(m->d_sort_tmp, m->xf_sort_tmp);
+    m->n_agents = count;
+    m->ag_dirty = false;  // sorted on the upload stream
+    m->ag_seg_dirty = true;
+    ++m->lists_version;
+  });
+}
+
+int bfvm_get_agent_densities_async(bfvm_solver* m, double* values) {
+  return SOLVER_CALL(m, {
+    const int64_t A = m->n_agents;
+    if (A == 0) return;
+    require(values != nullptr, "null output buffer");
+    ensure_transfer_streams(m);
+    gather_agents(m);
+    BFVM_CUDA(cudaEventRecord(m->xf_gathered, m->stream));
+    BFVM_CUDA(cudaStreamWaitEvent(m->xf_down, m->xf_gathered, 0));
+    BFVM_CUDA(cudaMemcpyAsync(values, m->d_gather.ptr, A * m->S * sizeof(double),
+                              cudaMemcpyDeviceToHost, m->xf_down));
+    BFVM_CUDA(cudaEventRecord(m->xf_down_done, m->xf_down));
+    m->xf_down_pending = true;
+  });
+}
+
+int bfvm_wait_transfers(bfvm_solver* m) {
+  return SOLVER_CALL(m, { wait_transfers(m); });
 }
 
 int bfvm_simulate_bulk_sources_and_sinks(bfvm_solver* m, double dt) {
@@ -2616,6 +2718,7 @@ int bfvm_set_row_stages(bfvm_solver* m, int stages) {
 int bfvm_synchronize(bfvm_solver* m) {
   return SOLVER_CALL(m, {
     BFVM_CUDA(cudaStreamSynchronize(m->stream));
+    wait_transfers(m);
     check_status(m);
   });
 }

@@ -195,6 +195,18 @@ struct bfvm_solver {
   bfvm_rt::DevBuf d_ag_key, d_ag_idx_in, d_ag_idx, d_sort_tmp;
   bfvm_rt::DevBuf d_gather;
   bfvm_rt::DevSegList seg_cells;
+  // Asynchronous agent exchange (bfvm_set_agents_async,
+  // bfvm_get_agent_densities_async), set up on first use: uploads and their
+  // sort run on xf_up into the spare buffer set, which then swaps with the
+  // current one; reads of d_gather go out on xf_down.  Events: xf_up_done
+  // (spare set filled and sorted), xf_spare_free (compute work that read the
+  // spare set, recorded when it stopped being current), xf_gathered
+  // (d_gather written), xf_down_done (d_gather copied out).
+  cudaStream_t xf_up = nullptr, xf_down = nullptr;
+  cudaEvent_t xf_up_done = nullptr, xf_spare_free = nullptr, xf_gathered = nullptr,
+              xf_down_done = nullptr;
+  bool xf_spare_recorded = false, xf_up_pending = false, xf_down_pending = false;
+  bfvm_rt::DevBuf xf_vox, xf_t1, xf_t2, xf_key, xf_idx_in, xf_idx, xf_sort_tmp;
 
   // device status word: set to non-zero by a kernel whose bounded wait failed
   bfvm_rt::DevBuf d_status;

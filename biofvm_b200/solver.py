@@ -23,6 +23,7 @@ class Solver:
         call("bfvm_create", ctypes.byref(h), device)
         self._h = h
         self.device = device
+        self._in_flight = []  # host arrays of asynchronous transfers not yet waited for
 
     # -- lifetime -----------------------------------------------------------
     def close(self) -> None:
@@ -162,6 +163,29 @@ class Solver:
         call("bfvm_get_agent_densities", self._h, dptr(out))
         return out
 
+    def set_agents_async(self, voxels, temp1, temp2) -> None:
+        """bfvm_set_agents_async: returns at once; steps enqueued afterwards use
+        these agents.  The arrays (page-locked, for the copies to overlap the
+        steps) are held until wait_transfers() or synchronize()."""
+        v = np.ascontiguousarray(voxels, np.int64)
+        a = np.ascontiguousarray(temp1, np.float64)
+        b = np.ascontiguousarray(temp2, np.float64)
+        call("bfvm_set_agents_async", self._h, v.size, lptr(v), dptr(a), dptr(b))
+        self._in_flight.extend((v, a, b))
+
+    def get_agent_densities_async(self, out: np.ndarray) -> np.ndarray:
+        """bfvm_get_agent_densities_async into out ([A][S] float64, C order),
+        which holds the densities after wait_transfers() or synchronize()."""
+        if out.dtype != np.float64 or not out.flags.c_contiguous:
+            raise ValueError("out must be a C-ordered float64 array")
+        call("bfvm_get_agent_densities_async", self._h, dptr(out))
+        self._in_flight.append(out)
+        return out
+
+    def wait_transfers(self) -> None:
+        call("bfvm_wait_transfers", self._h)
+        self._in_flight.clear()
+
     # -- stepping -------------------------------------------------------------
     def simulate_bulk_sources_and_sinks(self, dt: float) -> None:
         call("bfvm_simulate_bulk_sources_and_sinks", self._h, dt)
@@ -244,6 +268,7 @@ class Solver:
 
     def synchronize(self) -> None:
         call("bfvm_synchronize", self._h)
+        self._in_flight.clear()
 
     @property
     def stream(self) -> int:

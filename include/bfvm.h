@@ -157,6 +157,29 @@ BFVM_API int bfvm_set_agents(bfvm_solver* m, int64_t count, const int64_t* voxel
  * makes through Basic_Agent::nearest_density_vector (BioFVM_basic_agent.cpp:223). */
 BFVM_API int bfvm_get_agent_densities(bfvm_solver* m, double* values);
 
+/* Asynchronous forms of the two calls above, for a host loop that exchanges
+ * agent data with the solver every step (the reference's per-step
+ * set_internal_uptake_constants and nearest_density_vector,
+ * BioFVM_basic_agent.cpp:114-148, 223).  Both return at once.
+ *
+ * bfvm_set_agents_async: the copies of voxel/temp1/temp2 and the sort of the
+ * agents by voxel run on the solver's upload stream, into a second device
+ * buffer set, while steps enqueued earlier still run on the first; steps
+ * enqueued after this call use the new agents.  The host arrays must stay
+ * unchanged until bfvm_wait_transfers (or bfvm_synchronize) returns.
+ *
+ * bfvm_get_agent_densities_async: the densities at the agents' voxels as
+ * they stand after the work enqueued so far, copied into values [A][S] on
+ * the solver's download stream while later steps run; values holds them once
+ * bfvm_wait_transfers (or bfvm_synchronize) returns.
+ *
+ * The copies overlap the steps when the host arrays are page-locked. */
+BFVM_API int bfvm_set_agents_async(bfvm_solver* m, int64_t count, const int64_t* voxel,
+                                   const double* temp1, const double* temp2);
+BFVM_API int bfvm_get_agent_densities_async(bfvm_solver* m, double* values);
+/* Waits for the transfers of the asynchronous calls enqueued so far. */
+BFVM_API int bfvm_wait_transfers(bfvm_solver* m);
+
 /* Microenvironment::simulate_bulk_sources_and_sinks
  * (BioFVM_microenvironment.cpp:584-613). */
 BFVM_API int bfvm_simulate_bulk_sources_and_sinks(bfvm_solver* m, double dt);

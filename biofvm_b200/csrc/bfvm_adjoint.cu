@@ -121,15 +121,17 @@ void step_keeping_solves(bfvm_solver* m, double dt, int flags, const void* in, u
 
 void dot_into_acc(bfvm_solver* m, AdjointTape& T, const double* y, int axis) {
   const int S = m->S;
-  const int W = std::max(1, 256 / S);
-  const int blocks = std::max(1, std::min<int>(4 * m->num_sms, (int)((m->N() + W - 1) / W)));
+  const int threads = S * std::max(1, 256 / S);  // a multiple of S (S <= 256)
+  const int64_t rows = (int64_t)m->ny * m->nz;
+  const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(8 * m->num_sms, rows));
   T.part.ensure((size_t)blocks * 2 * S * sizeof(double));
-  const size_t smem = 2 * sizeof(double) * (size_t)S * W;
-  adj_axis_dot_kernel<<<blocks, dim3(S, W), smem, m->stream>>>(
+  const size_t smem = 2 * sizeof(double) * (size_t)threads;
+  adj_axis_dot_kernel<<<blocks, threads, smem, m->stream>>>(
       T.abar.as<double>(), y, m->nx, m->ny, m->nz, S, axis, T.part.as<double>());
   check_launch(m);
-  adj_reduce_parts_kernel<<<1, 2 * S, 0, m->stream>>>(T.part.as<double>(), blocks, S,
-                                                      T.acc.as<double>());
+  adj_reduce_parts_kernel<<<2 * S, kAdjReduceThreads, 0, m->stream>>>(T.part.as<double>(),
+                                                                      blocks, S,
+                                                                      T.acc.as<double>());
   check_launch(m);
 }
 

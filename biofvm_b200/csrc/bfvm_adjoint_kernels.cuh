@@ -15,60 +15,80 @@
 
 namespace bfvm {
 
-// Per-substrate sums over the field of a*(L_axis y) and a*y: block (S, W)
-// threads, thread (s, w) walks voxels w, w + W*gridDim.x, ...; each block
-// writes its partial sums to part[block][2S] (deterministic order).
-static __global__ void adj_axis_dot_kernel(const double* __restrict__ a, const double* __restrict__ y,
-                                    int nx, int ny, int nz, int S, int axis,
-                                    double* __restrict__ part) {
+// Per-substrate sums over the field of a*(L_axis y) and a*y.  Blocks take
+// whole rows (fixed y, z: nx*S contiguous elements), block b the rows b,
+// b + gridDim.x, ...; blockDim.x is a multiple of S, so thread t keeps one
+// density s = t % S and steps through x = t / S, t / S + blockDim.x / S, ...
+// of each row (coalesced; the row's position along y and z is found once per
+// row, and along x by counting).  Each block writes its per-density partial
+// sums to part[block][2S]; the order of every sum is fixed.
+static __global__ void adj_axis_dot_kernel(const double* __restrict__ a,
+                                           const double* __restrict__ y, int nx, int ny, int nz,
+                                           int S, int axis, double* __restrict__ part) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  double* sL = reinterpret_cast<double*>(smem_raw);  // [W][S]
-  double* sI = sL + blockDim.x * blockDim.y;
-  const int s = threadIdx.x, w = threadIdx.y, W = blockDim.y;
-  const int64_t N = (int64_t)nx * ny * nz;
-  const int64_t jump = axis == 0 ? 1 : (axis == 1 ? nx : (int64_t)nx * ny);
-  const int n = axis == 0 ? nx : (axis == 1 ? ny : nz);
+  double* sL = reinterpret_cast<double*>(smem_raw);  // [blockDim.x]
+  double* sI = sL + blockDim.x;
+  const int t = threadIdx.x, B = blockDim.x;
+  const int s = t % S, xstep = B / S;
+  const int64_t rows = (int64_t)ny * nz;
+  const int64_t RS = (int64_t)nx * S;
+  const int64_t jump = axis == 1 ? RS : (int64_t)ny * RS;  // y and z neighbours
   double accL = 0.0, accI = 0.0;
-  for (int64_t v = (int64_t)blockIdx.x * W + w; v < N; v += (int64_t)gridDim.x * W) {
-    int k;
-    if (axis == 0)
-      k = (int)(v % nx);
-    else if (axis == 1)
-      k = (int)((v / nx) % ny);
-    else
-      k = (int)(v / ((int64_t)nx * ny));
-    const int64_t q = v * S + s;
-    const double yv = y[q];
-    double ly = 0.0;
-    if (k > 0) ly += yv - y[q - jump * S];
-    if (k < n - 1) ly += yv - y[q + jump * S];
-    const double av = a[q];
-    accL += av * ly;
-    accI += av * yv;
-  }
-  sL[w * S + s] = accL;
-  sI[w * S + s] = accI;
-  __syncthreads();
-  if (w == 0) {
-    double L = 0.0, I = 0.0;
-    for (int u = 0; u < W; ++u) {
-      L += sL[u * S + s];
-      I += sI[u * S + s];
+  for (int64_t r = blockIdx.x; r < rows; r += gridDim.x) {
+    const int64_t zz = r / ny;
+    const int yy = (int)(r - zz * ny);
+    const bool lo = axis == 1 ? yy > 0 : zz > 0;
+    const bool hi = axis == 1 ? yy < ny - 1 : zz < nz - 1;
+    const double* yr = y + r * RS;
+    const double* ar = a + r * RS;
+    for (int x = t / S; x < nx; x += xstep) {
+      const int64_t c = (int64_t)x * S + s;
+      const double yv = yr[c];
+      double ly = 0.0;
+      if (axis == 0) {
+        if (x > 0) ly += yv - yr[c - S];
+        if (x < nx - 1) ly += yv - yr[c + S];
+      } else {
+        if (lo) ly += yv - yr[c - jump];
+        if (hi) ly += yv - yr[c + jump];
+      }
+      const double av = ar[c];
+      accL += av * ly;
+      accI += av * yv;
     }
-    part[(int64_t)blockIdx.x * 2 * S + s] = L;
-    part[(int64_t)blockIdx.x * 2 * S + S + s] = I;
+  }
+  sL[t] = accL;
+  sI[t] = accI;
+  __syncthreads();
+  if (t < S) {
+    double L = 0.0, I = 0.0;
+    for (int u = t; u < B; u += S) {
+      L += sL[u];
+      I += sI[u];
+    }
+    part[(int64_t)blockIdx.x * 2 * S + t] = L;
+    part[(int64_t)blockIdx.x * 2 * S + S + t] = I;
   }
 }
 
-// acc[2S] -= sum over blocks of part (in block order): the solve's
-// contributions -a.(L y) and -a.y.
-static __global__ void adj_reduce_parts_kernel(const double* __restrict__ part, int blocks, int S,
-                                        double* __restrict__ acc) {
-  const int t = threadIdx.x;
-  if (t >= 2 * S) return;
+// acc[j] -= sum over blocks of part[.][j], one block of kAdjReduceThreads
+// per output j in [0, 2S) (thread i sums blocks i, i + kAdjReduceThreads, ...,
+// then a fixed tree): the solve's contributions -a.(L y) and -a.y.
+constexpr int kAdjReduceThreads = 256;
+static __global__ void __launch_bounds__(kAdjReduceThreads)
+    adj_reduce_parts_kernel(const double* __restrict__ part, int blocks, int S,
+                            double* __restrict__ acc) {
+  __shared__ double sm[kAdjReduceThreads];
+  const int j = blockIdx.x, i = threadIdx.x;
   double sum = 0.0;
-  for (int b = 0; b < blocks; ++b) sum += part[(int64_t)b * 2 * S + t];
-  acc[t] -= sum;
+  for (int b = i; b < blocks; b += kAdjReduceThreads) sum += part[(int64_t)b * 2 * S + j];
+  sm[i] = sum;
+  __syncthreads();
+  for (int w = kAdjReduceThreads / 2; w > 0; w >>= 1) {
+    if (i < w) sm[i] += sm[i + w];
+    __syncthreads();
+  }
+  if (i == 0) acc[j] -= sm[0];
 }
 
 // a = 0 at the Dirichlet nodes (the adjoint of the overwrite).

@@ -702,7 +702,12 @@ LinesPlan plan_lines(const bfvm_solver* m, int ax) {
   LinesPlan L;
   const int64_t es = (int64_t)m->elem();
   const int64_t nx = m->nx, ny = m->ny, nz = m->nz, S = m->S;
-  if (ax == 1) {
+  if (ax == 0) {
+    // x lines: the densities of a voxel are the columns, the rows the outer
+    // blocks (rows too long for the row kernel's tiles)
+    L.n = (int)nx; L.C = S; L.nouter = ny * ((m->lod_dims == 2) ? 1 : nz); L.ls = S;
+    L.os = nx * S;
+  } else if (ax == 1) {
     L.n = (int)ny; L.C = nx * S; L.nouter = (m->lod_dims == 2) ? 1 : nz; L.ls = nx * S;
     L.os = nx * ny * S;
   } else {
@@ -715,6 +720,7 @@ LinesPlan plan_lines(const bfvm_solver* m, int ax) {
   L.w = (m->math_elem() == 8) ? 16 : 32;
   if (L.nc > 32 || (L.nc > 16 && L.ch < 32)) return L;
   if (L.nc > 16) L.w /= 2;  // 513-1024 points: half-width tiles, 32 chunks
+  if (ax == 0 && L.C % L.w) return L;  // x: whole tiles of densities only
   L.box_n = std::min(L.n, 256);
   L.nboxes = (L.n + L.box_n - 1) / L.box_n;
   const int64_t ctiles = (L.C + L.w - 1) / L.w;
@@ -903,9 +909,11 @@ void launch_lines_st(const CUtensorMap& map, const bfvm::LinesArgs<T, CT>& a, in
 template <typename T, typename CT>
 void launch_lines(bfvm_solver* m, int ax, const LinesPlan& L, bool dir, int64_t z0 = 0,
                   int64_t z1 = -1) {
-  // (re)encode the tensor map when the field moved
-  if (m->map_key[ax] != m->p.ptr || m->map_w[ax] != L.w) {
-    const int64_t es = (int64_t)sizeof(T);
+  // (re)encode the tensor map when the field or its geometry changed
+  const int64_t es = (int64_t)sizeof(T);
+  const int64_t geom[9] = {(int64_t)(uintptr_t)m->p.ptr, es, L.C, L.n, L.nouter, L.ls, L.os,
+                           L.w, L.box_n};
+  if (!std::equal(geom, geom + 9, m->map_geom[ax])) {
     cuuint64_t dims[3] = {(cuuint64_t)L.C, (cuuint64_t)L.n, (cuuint64_t)L.nouter};
     cuuint64_t strides[2] = {(cuuint64_t)(L.ls * es), (cuuint64_t)(L.os * es)};
     cuuint32_t box[3] = {(cuuint32_t)L.w, (cuuint32_t)L.box_n, 1};
@@ -917,8 +925,7 @@ void launch_lines(bfvm_solver* m, int ax, const LinesPlan& L, bool dir, int64_t 
         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     require(r == CUDA_SUCCESS, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")",
             BFVM_ERR_CUDA);
-    m->map_key[ax] = m->p.ptr;
-    m->map_w[ax] = L.w;
+    std::copy(geom, geom + 9, m->map_geom[ax]);
   }
   bfvm::LinesArgs<T, CT> a{};
   a.p = m->p.as<T>();
@@ -933,6 +940,9 @@ void launch_lines(bfvm_solver* m, int ax, const LinesPlan& L, bool dir, int64_t 
   if (z1 >= 0 && ax == 1) {  // the outer blocks of the y lines are the z planes
     a.tile0 = (uint32_t)(a.ctiles * z0);
     a.ntiles = (uint32_t)(a.ctiles * z1);
+  } else if (z1 >= 0 && ax == 0) {  // those of the x lines the rows, ny per plane
+    a.tile0 = (uint32_t)(a.ctiles * z0 * m->ny);
+    a.ntiles = (uint32_t)(a.ctiles * z1 * m->ny);
   }
   const int run_tiles = (int)(a.ntiles - a.tile0);
   a.box_n = L.box_n;
@@ -1214,6 +1224,16 @@ void sweep(bfvm_solver* m, int ax, int fuse, double dt, int64_t z0, int64_t z1) 
         const RowsPlan P = plan_rows(m);
         if (P.ok) {
           launch_rows<T, CT>(m, P, fuse, dt, z0, z1);
+          return;
+        }
+        // rows too long for the row kernel: the line kernel, with the
+        // Dirichlet overwrites around it (sources fused into the x sweep
+        // stay with the kernels that fuse them)
+        const LinesPlan L = plan_lines(m, 0);
+        if (L.ok && !(fuse & (bfvm::kFuseBulk | bfvm::kFuseCells))) {
+          if ((fuse & bfvm::kFuseDirPro) && m->dir_unique > 0) dirichlet_standalone<T>(m);
+          launch_lines<T, CT>(m, 0, L, false, z0, z1);
+          if ((fuse & bfvm::kFuseDirEpi) && m->dir_unique > 0) dirichlet_standalone<T>(m);
           return;
         }
       } else if (want_tma) {
@@ -2581,9 +2601,9 @@ void tune_sweeps(bfvm_solver* m, double dt, int reps) {
         for (int tw : {32, 16, 8})
           if (nc * tw <= bfvm::sweep_max_threads(ch))
             cand.push_back({BFVM_PATH_GENERIC, ch, tw, 0, 1});
-        // the line kernel (y, z) also takes 17-32 chunks of 32 points
-        if (nc <= 16 || (ax > 0 && ch == 32 && nc <= 32))
-          cand.push_back({BFVM_PATH_TMA, ch, 16, 0, 1});
+        // the line kernel also takes 17-32 chunks of 32 points (x: where the
+        // rows are too long for the row kernel)
+        if (nc <= 16 || (ch == 32 && nc <= 32)) cand.push_back({BFVM_PATH_TMA, ch, 16, 0, 1});
         // the row kernel (x) with a ring of three tiles, and at 32-point
         // chunks compiled for two blocks per SM
         if (ax == 0 && nc <= 16) cand.push_back({BFVM_PATH_TMA, ch, 16, 3, 1});

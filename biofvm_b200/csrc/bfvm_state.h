@@ -234,10 +234,12 @@ struct bfvm_solver {
   int64_t grid_maps_version = -1;
   int grid_maps_S = 0;
   int grid_per_sm[2] = {0, 0};  // 4- and 8-point chunk kernels (-1: not usable)
-  // cached tensor maps of the y and z sweeps (keyed by field pointer)
+  // cached tensor maps of the line sweeps, per axis, with the geometry they
+  // were encoded for (field address, element size, C, n, outer blocks, the
+  // two strides, tile width, box rows): a resize that keeps the allocation,
+  // a precision change or a LOD_2D step re-encodes them
   CUtensorMap maps[3];
-  const void* map_key[3] = {nullptr, nullptr, nullptr};
-  int map_w[3] = {0, 0, 0};
+  int64_t map_geom[3][9] = {};
 
   // z slab of a field split by z planes over several solvers (one per GPU):
   // this solver holds global planes [zs_bounds[zs_rank], zs_bounds[zs_rank+1])

@@ -7,7 +7,7 @@ Dirichlet) are bit-exact; FP32 sweeps <= 1e-5.
 import numpy as np
 import pytest
 
-from biofvm_b200 import STEP_BULK, STEP_CELLS, STEP_DIFFUSION, Solver, load_scenario
+from biofvm_b200 import STEP_ALL, STEP_BULK, STEP_CELLS, STEP_DIFFUSION, Solver, load_scenario
 from biofvm_b200 import workloads as W
 from biofvm_b200._abi import FP32_FP64MATH, PATH_AUTO, PATH_DIRECT, PATH_GENERIC, PATH_TMA, BfvmError
 from cases import CASES, sha
@@ -424,6 +424,63 @@ def test_lod2d(shape, path):
             sv.simulate_diffusion_decay_2d(scn.dt)
         p = sv.get_densities()
     assert np.all(rel_err(p, ref) <= TOL64)
+
+
+X_LINE_CASES = [
+    # more densities x chunks per row than the row kernel's tiles hold
+    # (S * chunks > 512), so the x sweep runs on the line kernel; Dirichlet
+    # nodes before and after it
+    ((520, 6, 4), 32, False),  # 17 chunks of 32 points: 8-density tiles
+    ((400, 5, 3), 48, False),  # 13 chunks: 16-density tiles
+    ((600, 8, 1), 32, True),   # LOD_2D plane
+]
+
+
+@pytest.mark.parametrize("shape,S,two_d", X_LINE_CASES)
+def test_x_sweep_on_the_line_kernel(shape, S, two_d):
+    scn = W.mixed_small(shape=shape, S=S, n_agents=40, seed=sum(shape) + S, bulk=True)
+    steps = 2
+    ref = O.oracle_lod2d_run(scn, steps) if two_d else O.oracle_run(scn, steps, STEP_ALL)
+    with Solver(0) as sv:
+        load_scenario(sv, scn)
+        sv.set_kernel_path(PATH_TMA)
+        if two_d:
+            for _ in range(steps):
+                sv.simulate_diffusion_decay_2d(scn.dt)
+        else:
+            sv.step(scn.dt, steps, STEP_ALL)
+        p = sv.get_densities()
+    assert np.all(rel_err(p, ref) <= TOL64)
+
+
+def test_line_sweeps_after_a_resize_that_keeps_the_allocation():
+    """The y and z sweeps' tensor maps follow the mesh: a smaller mesh in the
+    same device allocation, then a LOD_2D step and 3-D steps on one solver,
+    match fresh solvers."""
+    big = W.mixed_small(shape=(40, 36, 30), S=2, n_agents=0, seed=81, bulk=False)
+    small = W.mixed_small(shape=(24, 20, 16), S=2, n_agents=30, seed=82)
+    with Solver(0) as sv:
+        sv.set_kernel_path(PATH_TMA)
+        load_scenario(sv, big)
+        sv.step(big.dt, 2, STEP_ALL)
+        load_scenario(sv, small)
+        sv.step(small.dt, 3, STEP_ALL)
+        p = sv.get_densities()
+    ref = O.oracle_run(small, 3, STEP_ALL)
+    assert np.all(rel_err(p, ref) <= TOL64)
+    with Solver(0) as sv:
+        sv.set_kernel_path(PATH_TMA)
+        load_scenario(sv, small)
+        sv.simulate_diffusion_decay_2d(small.dt)
+        sv.step(small.dt, 2, STEP_ALL)
+        p = sv.get_densities()
+    with Solver(0) as sv:
+        sv.set_kernel_path(PATH_GENERIC)
+        load_scenario(sv, small)
+        sv.simulate_diffusion_decay_2d(small.dt)
+        sv.step(small.dt, 2, STEP_ALL)
+        q = sv.get_densities()
+    assert np.all(rel_err(p, q) <= TOL64)
 
 
 def test_agents_sharing_voxels_keep_list_order():

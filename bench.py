@@ -731,9 +731,9 @@ def run_batched(args, world, rank, local):
     if args.batch_mode == "tuned":
         bt.tune(dt, STEP_ALL, args.batch_trial_steps)
     else:
-        from biofvm_b200._abi import BATCH_BRANCHES, BATCH_FUSED, BATCH_PERSISTENT
+        from biofvm_b200._abi import BATCH_BRANCHES, BATCH_FUSED, BATCH_PERSISTENT, BATCH_PLANES
         bt.set_mode({"fused": BATCH_FUSED, "branches": BATCH_BRANCHES,
-                     "persistent": BATCH_PERSISTENT}[args.batch_mode])
+                     "persistent": BATCH_PERSISTENT, "planes": BATCH_PLANES}[args.batch_mode])
         bt.set_persistent_chunk(args.batch_chunk)
     t_tune = time.perf_counter() - t0
     cfg = bt.get_config()
@@ -757,9 +757,9 @@ def run_batched(args, world, rank, local):
     # timed on a replay)
     per_mode = {}
     if args.batch_modes:
-        from biofvm_b200._abi import BATCH_BRANCHES, BATCH_FUSED, BATCH_PERSISTENT
+        from biofvm_b200._abi import BATCH_BRANCHES, BATCH_FUSED, BATCH_PERSISTENT, BATCH_PLANES
         for name, md in (("fused", BATCH_FUSED), ("branches", BATCH_BRANCHES),
-                         ("persistent", BATCH_PERSISTENT)):
+                         ("persistent", BATCH_PERSISTENT), ("planes", BATCH_PLANES)):
             bt.set_mode(md)
             reset()
             bt.step(dt, args.steps, STEP_ALL)
@@ -831,7 +831,7 @@ def run_batched(args, world, rank, local):
                                           t_plain_tuned, "seconds": t_plain_tuned},
             "batched_seconds": t_batch, "speedup_vs_looped_plain": t_plain / t_batch,
             "max_rel_err_vs_looped_plain": err,
-            "tuned": {"mode": ["fused", "branches", "persistent"][mode], "chunk": cfg[0],
+            "tuned": {"mode": ["fused", "branches", "persistent", "planes"][mode], "chunk": cfg[0],
                       "threads": cfg[1], "group_bytes": cfg[2], "persistent_chunk": pch,
                       "tune_seconds": t_tune, "trial_steps": args.batch_trial_steps},
             "graph": {"groups": groups, "kernels_per_call": kernels,
@@ -1302,7 +1302,7 @@ def main():
                     help="steps per trial run of the batch tuner")
     ap.add_argument("--batch-modes", action="store_true",
                     help="batched: also time every batch mode with the tuned group budget")
-    ap.add_argument("--batch-mode", choices=["tuned", "fused", "branches", "persistent"],
+    ap.add_argument("--batch-mode", choices=["tuned", "fused", "branches", "persistent", "planes"],
                     default="tuned", help="batched: the tuner's choice, or one mode untuned")
     ap.add_argument("--batch-chunk", type=int, default=8,
                     help="batched, persistent mode untuned: 4, 8, 16, 32 or 0 (whole lines)")

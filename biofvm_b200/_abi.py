@@ -38,6 +38,7 @@ FP32_FP64MATH = 3264
 BATCH_FUSED = 0
 BATCH_BRANCHES = 1
 BATCH_PERSISTENT = 2
+BATCH_PLANES = 3
 
 _P = c_void_p  # opaque solver handle
 _DP = POINTER(c_double)

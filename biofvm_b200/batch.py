@@ -6,8 +6,10 @@ on every member; the members are packed into L2-sized groups and the whole
 run is one CUDA-graph replay: one launch per phase over a group
 (``BATCH_FUSED``), every member's own kernels on concurrent graph branches
 (``BATCH_BRANCHES``), or all steps of a group's members in one persistent
-cooperative launch (``BATCH_PERSISTENT``).  The reference has no such object: its drivers
-loop over Microenvironment instances one by one.
+cooperative launch (``BATCH_PERSISTENT``: x, y, z phases of chunked line
+tiles; ``BATCH_PLANES``: xy planes and xz strips staged in shared memory, two
+phases per step).  The reference has no such object: its drivers loop over
+Microenvironment instances one by one.
 """
 from __future__ import annotations
 
@@ -77,8 +79,10 @@ class Batch:
     def set_mode(self, mode: int) -> None:
         """BATCH_FUSED (one launch per phase over a group's members),
         BATCH_BRANCHES (every member's own kernels on concurrent graph
-        branches) or BATCH_PERSISTENT (all steps of a group's members in one
-        persistent cooperative launch)."""
+        branches), BATCH_PERSISTENT (all steps of a group's members in one
+        persistent cooperative launch, x, y and z phases) or BATCH_PLANES
+        (the same launch with two phases per step: xy planes solved along x
+        and y in shared memory, then xz strips along z)."""
         call("bfvm_batch_set_mode", self._h, mode)
 
     def set_persistent_chunk(self, chunk: int) -> None:

@@ -22,6 +22,12 @@
 //                        graph paths that the GPU runs concurrently, so the
 //                        short kernels of small instances overlap instead of
 //                        running one after another.
+//   BFVM_BATCH_PERSISTENT / BFVM_BATCH_PLANES
+//                        all n steps of a group in one cooperative launch
+//                        (bfvm_kernels_batch_steps.cuh: chunked and line
+//                        forms; bfvm_kernels_batch_planes.cuh: xy planes and
+//                        xz strips in shared memory); members that kernel
+//                        cannot run form groups that run on branches.
 // The whole sequence -- groups x steps x phases -- is captured once into a
 // CUDA graph and replayed by one graph launch per call; the graph is rebuilt
 // only when the plan changes (instances, their lists or device buffers, dt,
@@ -41,6 +47,7 @@
 #include "bfvm.h"
 #include "bfvm_batch_kernels.cuh"
 #include "bfvm_host_math.h"
+#include "bfvm_kernels_batch_planes.cuh"
 #include "bfvm_kernels_batch_steps.cuh"
 #include "bfvm_state.h"
 
@@ -79,6 +86,12 @@ struct MemberScratch {
   size_t masks_off = 0, masks_bytes = 0;  // src, x, y, z masks, set to 0
   size_t dir_off = 0;      // dir_field (when the member has Dirichlet nodes)
   DevBuf tabs;             // tile form: 32-point chunk tables of the three axes
+  // plane form: x-line bulk runs and their per-line offsets (rebuilt when the
+  // member's lists change), per-line first sorted agents
+  DevBuf runs;
+  int64_t runs_version = -1;
+  size_t runs_off = 0;
+  DevBuf xag;
 };
 
 }  // namespace
@@ -102,9 +115,10 @@ struct bfvm_batch {
   // 8- and 16-point kernels (0: not queried), SMs
   std::vector<bfvm_rt::MemberScratch> scratch;
   std::vector<std::vector<bfvm::StepMember>> pmembers;
-  int p_per_sm[5] = {0, 0, 0, 0, 0};  // 8-, 16-point chunks, line form, tile form, 4-point
+  int p_per_sm[6] = {0, 0, 0, 0, 0, 0};  // 8-, 16-point chunks, line form, tile form, 4-point, planes
   size_t tile_tab_doubles = 0;  // tile form: the largest member's tables of one axis
   int num_sms = 0;
+  bfvm_rt::DevBuf d_ctr;  // plane form: work-item counters, 2 per step
   // cached graph and what it was captured for
   cudaGraphExec_t exec = nullptr;
   std::string key;
@@ -231,6 +245,58 @@ bool persistent_ok(const bfvm_solver* m, int pch) {
          m->nz <= kBatchStepsMaxN && (pch != 32 || m->S <= 32);
 }
 
+// The persistent kernel's form: the chunk length of BFVM_BATCH_PERSISTENT
+// (0: whole lines), or kPlaneForm for BFVM_BATCH_PLANES.
+constexpr int kPlaneForm = -1;
+bool persistent_mode(int mode) {
+  return mode == BFVM_BATCH_PERSISTENT || mode == BFVM_BATCH_PLANES;
+}
+int pform(const bfvm_batch* b) { return b->cfg.mode == BFVM_BATCH_PLANES ? kPlaneForm : b->cfg.pch; }
+
+// Plane form shapes of member m: densities per xy item (sg, balanced over
+// the plane's items) and columns per z item (cw); false when even one
+// density's xy plane, or one column of nz points, exceeds the block's shared
+// memory.
+bool plane_shape(const bfvm_solver* m, int* sg_out, int* groups_out, int* cw_out,
+                 int* strips_out) {
+  const int nx = m->nx, ny = m->ny, nz = m->nz, S = m->S;
+  auto fits = [&](int sg) {
+    return (int64_t)ny * plane_pitch(nx, sg) <= kPlaneSmemDoubles &&
+           (int64_t)(nx + ny) * sg <= kPlaneTabPairs;
+  };
+  int sg = S;
+  while (sg > 0 && !fits(sg)) --sg;
+  if (sg == 0) return false;
+  int groups = (S + sg - 1) / sg;
+  sg = (S + groups - 1) / groups;  // the same items, balanced
+  // the last item of a plane has S - (groups - 1)*sg densities; its pitch
+  // rounds up on its own
+  if (!fits(S - (groups - 1) * sg)) return false;
+  const int C = nx * S;
+  const int most = kPlaneSmemDoubles / nz;
+  if (most < 1) return false;
+  const int strips = (C + most - 1) / most;
+  *sg_out = sg;
+  *groups_out = groups;
+  *cw_out = (C + strips - 1) / strips;
+  *strips_out = strips;
+  return true;
+}
+
+// Whether a member can run in the plane form: FP64, lines of at most 128
+// points (two mask words per line), plane items that fit shared memory, and
+// offsets of 32 bits inside the member.
+bool planes_ok(const bfvm_solver* m) {
+  int a, b, c, d;
+  return m->precision == BFVM_FP64 && m->nx <= kBatchStepsMaxN && m->ny <= kBatchStepsMaxN &&
+         m->nz <= kBatchStepsMaxN && m->S <= 4096 && m->NS() < ((int64_t)1 << 31) &&
+         plane_shape(m, &a, &b, &c, &d);
+}
+
+bool form_ok(const bfvm_solver* m, int form) {
+  return form == kPlaneForm ? planes_ok(m) : persistent_ok(m, form);
+}
+
 size_t round256(size_t x) { return (x + 255) / 256 * 256; }
 
 // The persistent mode's descriptor of member m (device pointers into its
@@ -261,7 +327,7 @@ bfvm::StepMember step_member(bfvm_batch* b, bfvm_solver* m, int flags, int ch,
   const int ns[3] = {m->nx, m->ny, m->nz};
   for (int a = 0; a < 3; ++a) {
     // ch = 0: the line form, one column per work item; ch = 32: the tile
-    // form, 32 columns per work item
+    // form, 32 columns per work item; kPlaneForm: planes (below)
     d.nc[a] = ch > 0 ? (ns[a] + ch - 1) / ch : 1;
     d.tw[a] = ch == 32 ? kBatchTileCols : (ch > 0 ? kBatchStepsThreads / d.nc[a] : 1);
     d.ncols[a] = N / ns[a] * m->S;
@@ -293,9 +359,10 @@ bfvm::StepMember step_member(bfvm_batch* b, bfvm_solver* m, int flags, int ch,
     d.rs = 1;
     d.bulk_row = nullptr;
   }
-  if (ch == 32) {
+  if (ch == 32 || ch == kPlaneForm) {
     // the sweep kernels' chunk tables for 32-point chunks, every chunk its
-    // own slot, from the FP64 Thomas coefficients
+    // own slot, from the FP64 Thomas coefficients (the plane form reads
+    // their {1/d, a} pairs, [point][density], as whole-line tables)
     std::vector<double> all;
     size_t off[3][3];
     for (int a = 0; a < 3; ++a) {
@@ -325,6 +392,59 @@ bfvm::StepMember step_member(bfvm_batch* b, bfvm_solver* m, int flags, int ch,
   d.ag_idx = m->d_ag_idx.as<int>();
   d.ag_t1 = m->d_ag_t1.as<double>();
   d.ag_t2 = m->d_ag_t2.as<double>();
+  if (ch == kPlaneForm) {
+    require(plane_shape(m, &d.psg, &d.pgroups, &d.pcw, &d.pstrips),
+            "batch: member does not fit the plane form", BFVM_ERR_STATE);
+    const int64_t lines = (int64_t)m->ny * m->nz;
+    if (d.bulk && (sc.runs_version != m->lists_version || !sc.runs.ptr)) {
+      // runs of consecutive voxels of one x line whose rates are bitwise
+      // equal, the offsets of each line's runs after them
+      const int S = m->S;
+      const int64_t E = (int64_t)m->bulk_vox.size();
+      std::vector<int> runs, off((size_t)lines + 1, 0);
+      auto same = [&](int64_t a, int64_t c) {
+        return std::memcmp(&m->bulk_st[a * S], &m->bulk_st[c * S], S * sizeof(double)) == 0 &&
+               std::memcmp(&m->bulk_su[a * S], &m->bulk_su[c * S], S * sizeof(double)) == 0;
+      };
+      int64_t first = 0;
+      for (int64_t e = 0; e < E; ++e) {
+        const int64_t v = m->bulk_vox[e];
+        const bool open = e > 0 && v == m->bulk_vox[e - 1] + 1 && v / m->nx == (v - 1) / m->nx &&
+                          same(first, e);
+        if (open) {
+          runs[runs.size() - 3] += 1;  // end x
+          continue;
+        }
+        first = e;
+        const int64_t line = v / m->nx;
+        const int x = (int)(v - line * m->nx);
+        runs.push_back(x);
+        runs.push_back(x + 1);
+        runs.push_back((int)e);
+        runs.push_back(0);
+        off[(size_t)line + 1] += 1;
+      }
+      for (size_t i = 1; i < off.size(); ++i) off[i] += off[i - 1];
+      sc.runs_off = round256(runs.size() * sizeof(int));
+      sc.runs.ensure(sc.runs_off + off.size() * sizeof(int));
+      if (!runs.empty())
+        BFVM_CUDA(cudaMemcpyAsync(sc.runs.ptr, runs.data(), runs.size() * sizeof(int),
+                                  cudaMemcpyHostToDevice, b->stream));
+      BFVM_CUDA(cudaMemcpyAsync(sc.runs.as<unsigned char>() + sc.runs_off, off.data(),
+                                off.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream));
+      sc.runs_version = m->lists_version;
+    }
+    if (d.bulk) {
+      d.xruns = sc.runs.as<int4>();
+      d.xrun_off = reinterpret_cast<const int*>(sc.runs.as<unsigned char>() + sc.runs_off);
+      d.est = m->d_bulk_st.as<double>();
+      d.esu = m->d_bulk_su.as<double>();
+    }
+    if (d.cells) {
+      sc.xag.ensure((size_t)(lines + 1) * sizeof(int));
+      d.xag_off = sc.xag.as<int>();
+    }
+  }
   return d;
 }
 
@@ -334,10 +454,10 @@ void build_plan(bfvm_batch* b, int flags) {
   // persistent mode (FP64, whole steps): the members its kernel can run form
   // groups of their own, run first; the others run on branches
   std::vector<bfvm_solver*> pers, rest;
-  const bool persistent = b->cfg.mode == BFVM_BATCH_PERSISTENT && sizeof(T) == sizeof(double) &&
+  const bool persistent = persistent_mode(b->cfg.mode) && sizeof(T) == sizeof(double) &&
                           (flags & BFVM_STEP_DIFFUSION);
-  for (bfvm_solver* m : b->inst)
-    (persistent && persistent_ok(m, b->cfg.pch) ? pers : rest).push_back(m);
+  const int form = pform(b);
+  for (bfvm_solver* m : b->inst) (persistent && form_ok(m, form) ? pers : rest).push_back(m);
   auto pgroups = make_groups(pers, budget);
   const size_t n_pers = pgroups.size();
   auto groups = pgroups;
@@ -355,12 +475,18 @@ void build_plan(bfvm_batch* b, int flags) {
     for (bfvm_solver* m : members) G.field_bytes += (int64_t)(m->NS() * m->elem());
     if (gi < n_pers) {
       G.persistent = 1;
-      const int ch = b->cfg.pch;
       std::vector<bfvm::StepMember> ds;
       int64_t tile0[3] = {0, 0, 0}, src0 = 0;
       for (bfvm_solver* m : members) {
-        bfvm::StepMember d = step_member(b, m, flags, ch, tile0, src0);
-        for (int a = 0; a < 3; ++a) tile0[a] += (d.ncols[a] + d.tw[a] - 1) / d.tw[a];
+        bfvm::StepMember d = step_member(b, m, flags, form, tile0, src0);
+        if (form == kPlaneForm) {
+          // xy items: every plane's density groups; z items: every xz
+          // plane's strips
+          tile0[0] += (int64_t)m->nz * d.pgroups;
+          tile0[2] += (int64_t)m->ny * d.pstrips;
+        } else {
+          for (int a = 0; a < 3; ++a) tile0[a] += (d.ncols[a] + d.tw[a] - 1) / d.tw[a];
+        }
         src0 += d.nsrc;
         ds.push_back(d);
       }
@@ -496,6 +622,10 @@ void allow_persistent_smem(const void* k, size_t smem) {
 // The persistent kernel for chunk length ch (0: the line form) and its
 // dynamic shared memory.
 const void* persistent_kernel(const bfvm_batch* b, int ch, size_t* smem) {
+  if (ch == kPlaneForm) {
+    *smem = (size_t)kPlaneSmemDoubles * sizeof(double) + (size_t)kPlaneTabPairs * 16;
+    return (const void*)batch_planes_kernel;
+  }
   *smem = ch == 32 ? 4 * kBatchTileCols * sizeof(bfvm::Pair<double>) +
                          b->tile_tab_doubles * sizeof(double)
                    : (ch > 0 ? 4 * kBatchStepsThreads * sizeof(double) : 0);
@@ -506,8 +636,12 @@ const void* persistent_kernel(const bfvm_batch* b, int ch, size_t* smem) {
   return (const void*)batch_lines_kernel<kBatchLineBatch>;
 }
 
+int persistent_threads(int ch) { return ch == kPlaneForm ? kPlaneThreads : kBatchStepsThreads; }
+
 int persistent_per_sm(bfvm_batch* b, int ch) {
-  const int i = ch == 8 ? 0 : (ch == 16 ? 1 : (ch == 0 ? 2 : (ch == 32 ? 3 : 4)));
+  const int i = ch == kPlaneForm
+                    ? 5
+                    : (ch == 8 ? 0 : (ch == 16 ? 1 : (ch == 0 ? 2 : (ch == 32 ? 3 : 4))));
   if (b->p_per_sm[i] == 0 || i == 3) {  // the tile form's shared memory varies
     int coop = 0;
     BFVM_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, b->device));
@@ -517,7 +651,7 @@ int persistent_per_sm(bfvm_batch* b, int ch) {
     const void* k = persistent_kernel(b, ch, &smem);
     allow_persistent_smem(k, smem);
     int per = 0;
-    BFVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, kBatchStepsThreads, smem));
+    BFVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, persistent_threads(ch), smem));
     require(per > 0, "batch: the persistent kernel cannot be resident", BFVM_ERR_CUDA);
     b->p_per_sm[i] = per;
   }
@@ -527,12 +661,12 @@ int persistent_per_sm(bfvm_batch* b, int ch) {
 // Blocks of a persistent group's launch: enough for the widest phase, at
 // most one wave of resident blocks (every block must be resident).
 int persistent_blocks(bfvm_batch* b, const GroupPlan& G) {
-  const int64_t wave = (int64_t)persistent_per_sm(b, b->cfg.pch) * b->num_sms;
-  int64_t want = (G.src_items + kBatchStepsThreads - 1) / kBatchStepsThreads;
+  const int form = pform(b);
+  const int64_t wave = (int64_t)persistent_per_sm(b, form) * b->num_sms;
+  const int th = persistent_threads(form);
+  int64_t want = (G.src_items + th - 1) / th;
   for (int a = 0; a < 3; ++a)
-    want = std::max(want, b->cfg.pch > 0 ? G.ptiles[a]
-                                         : (G.ptiles[a] + kBatchStepsThreads - 1) /
-                                               kBatchStepsThreads);
+    want = std::max(want, form != 0 ? G.ptiles[a] : (G.ptiles[a] + th - 1) / th);
   return (int)std::max<int64_t>(1, std::min(want, wave));
 }
 
@@ -551,7 +685,19 @@ void enqueue_persistent_group(bfvm_batch* b, size_t gi, double dt, int nsteps,
     MemberScratch& sc = b->scratch[idx];
     unsigned char* base = sc.buf.as<unsigned char>();
     sources = sources || d.bulk || d.cells;
-    if (!d.bulk && !d.cells && !d.dirichlet) continue;
+    if (pform(b) == kPlaneForm) {
+      if (d.cells) {  // the x lines' first sorted agents
+        const int64_t lines = (int64_t)m->ny * m->nz;
+        plane_agent_lines_kernel<<<(unsigned)blocks_for(lines + 1, 256), 256, 0, b->stream>>>(
+            d, const_cast<int*>(d.xag_off));
+        BFVM_CUDA(cudaGetLastError());
+        ++*kernels;
+      }
+      // the plane form reads only the Dirichlet masks and values of the maps
+      if (!d.dirichlet) continue;
+    } else if (!d.bulk && !d.cells && !d.dirichlet) {
+      continue;
+    }
     BFVM_CUDA(cudaMemsetAsync(base, 0xFF, sc.maps_bytes, b->stream));
     BFVM_CUDA(cudaMemsetAsync(base + sc.masks_off, 0, sc.masks_bytes, b->stream));
     const int64_t most = std::max({d.bulk ? d.nbulk : 0, d.cells ? d.nagents : 0, m->dir_unique});
@@ -577,13 +723,21 @@ void enqueue_persistent_group(bfvm_batch* b, size_t gi, double dt, int nsteps,
   a.nsteps = nsteps;
   a.dt = dt;
   a.sources = sources ? 1 : 0;
+  const int form = pform(b);
+  if (form == kPlaneForm) {
+    // the phases' work-item counters start at zero for every launch
+    const size_t bytes = (size_t)2 * nsteps * sizeof(int);
+    require(b->d_ctr.bytes >= bytes, "batch: work-item counters not sized", BFVM_ERR_STATE);
+    a.ctr = b->d_ctr.as<int>();
+    BFVM_CUDA(cudaMemsetAsync(a.ctr, 0, bytes, b->stream));
+  }
   const int blocks = persistent_blocks(b, G);
   size_t smem = 0;
-  const void* kern = persistent_kernel(b, b->cfg.pch, &smem);
+  const void* kern = persistent_kernel(b, form, &smem);
   cudaLaunchConfig_t cfg;
   std::memset(&cfg, 0, sizeof cfg);
   cfg.gridDim = dim3((unsigned)blocks);
-  cfg.blockDim = dim3(kBatchStepsThreads);
+  cfg.blockDim = dim3(persistent_threads(form));
   cfg.dynamicSmemBytes = smem;
   cfg.stream = b->stream;
   cudaLaunchAttribute attr[1];
@@ -629,7 +783,7 @@ void plan(bfvm_batch* b, int flags) {
   // outside any graph capture
   bool any_persistent = false;
   for (const GroupPlan& G : b->groups) any_persistent = any_persistent || G.persistent;
-  if (any_persistent) persistent_per_sm(b, b->cfg.pch);
+  if (any_persistent) persistent_per_sm(b, pform(b));
   b->d_desc.ensure(std::max<size_t>(b->host_desc.size(), 64));
   BFVM_CUDA(cudaMemcpyAsync(b->d_desc.ptr, b->host_desc.data(), b->host_desc.size(),
                             cudaMemcpyHostToDevice, b->stream));
@@ -686,10 +840,10 @@ cudaGraphExec_t capture(bfvm_batch* b, double dt, int nsteps, int flags, int axe
                         int64_t* kernels) {
   *kernels = 0;
   cudaGraph_t graph = nullptr;
-  // branch mode, and the persistent mode's groups that its kernel cannot run
-  const bool branches =
-      b->cfg.mode == BFVM_BATCH_BRANCHES || b->cfg.mode == BFVM_BATCH_PERSISTENT;
+  // branch mode, and the persistent modes' groups that their kernel cannot run
+  const bool branches = b->cfg.mode == BFVM_BATCH_BRANCHES || persistent_mode(b->cfg.mode);
   if (branches) warm_instances(b, dt, flags);
+  if (b->cfg.mode == BFVM_BATCH_PLANES) b->d_ctr.ensure((size_t)2 * std::max(nsteps, 1) * sizeof(int));
   BFVM_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
   try {
     for (size_t gi = 0; gi < b->groups.size(); ++gi) {
@@ -747,7 +901,7 @@ std::string plan_key(const bfvm_batch* b, double dt, int nsteps, int flags) {
   k.append(reinterpret_cast<const char*>(&b->cfg.pch), sizeof b->cfg.pch);
   // branch mode (and the persistent mode's groups on branches) bakes each
   // member's own kernel choices and device buffers into the graph
-  if (b->cfg.mode == BFVM_BATCH_BRANCHES || b->cfg.mode == BFVM_BATCH_PERSISTENT)
+  if (b->cfg.mode == BFVM_BATCH_BRANCHES || persistent_mode(b->cfg.mode))
     for (const bfvm_solver* m : b->inst) {
       for (int a = 0; a < 3; ++a) {
         const Axis& A = m->axis[a];
@@ -888,13 +1042,19 @@ void batch_tune(bfvm_batch* b, double dt, int flags, int trial_steps) {
     }
     // 3. the mode (and the persistent kernel's chunk length) and the group
     // budget, whole steps
-    bool any_persistent = false;
-    for (const bfvm_solver* m : b->inst) any_persistent = any_persistent || persistent_ok(m, 8);
+    bool any_persistent = false, any_planes = false;
+    for (const bfvm_solver* m : b->inst) {
+      any_persistent = any_persistent || persistent_ok(m, 8);
+      any_planes = any_planes || planes_ok(m);
+    }
     float best_ms = 1e30f;
     int64_t best_budget = 0;
     int best_mode = BFVM_BATCH_FUSED, best_pch = best.pch;
-    for (int mode : {BFVM_BATCH_FUSED, BFVM_BATCH_BRANCHES, BFVM_BATCH_PERSISTENT}) {
+    for (int mode :
+         {BFVM_BATCH_FUSED, BFVM_BATCH_BRANCHES, BFVM_BATCH_PERSISTENT, BFVM_BATCH_PLANES}) {
       if (mode == BFVM_BATCH_PERSISTENT && (!any_persistent || !(flags & BFVM_STEP_DIFFUSION)))
+        continue;
+      if (mode == BFVM_BATCH_PLANES && (!any_planes || !(flags & BFVM_STEP_DIFFUSION) || !fp64(b)))
         continue;
       for (int pch : {8, 4, 16, 32, 0}) {
         if (pch != 8 && mode != BFVM_BATCH_PERSISTENT) continue;
@@ -1053,8 +1213,9 @@ int bfvm_batch_get_config(bfvm_batch* b, int* chunk, int* threads, int64_t* grou
 int bfvm_batch_set_mode(bfvm_batch* b, int mode) {
   return BATCH_CALL(b, {
     require(mode == BFVM_BATCH_FUSED || mode == BFVM_BATCH_BRANCHES ||
-                mode == BFVM_BATCH_PERSISTENT,
-            "mode must be BFVM_BATCH_FUSED, BFVM_BATCH_BRANCHES or BFVM_BATCH_PERSISTENT");
+                mode == BFVM_BATCH_PERSISTENT || mode == BFVM_BATCH_PLANES,
+            "mode must be BFVM_BATCH_FUSED, BFVM_BATCH_BRANCHES, BFVM_BATCH_PERSISTENT or "
+            "BFVM_BATCH_PLANES");
     b->cfg.mode = mode;
   });
 }

@@ -76,6 +76,19 @@ struct StepMember {
   const double* ck1[3];
   const double* ckg[3];
   const double* ckc[3];
+  // plane form: densities per xy item (psg) and items per xy plane
+  // (pgroups); columns per z item (pcw) and items per xz plane (pstrips);
+  // tile0[0] / tile0[2] are the member's first xy / z items
+  int psg, pgroups, pcw, pstrips;
+  // plane form, sources by x line (line = k*ny + j): bulk runs {first x, end
+  // x, entry} of line at xruns[xrun_off[line] .. xrun_off[line+1]), rates of
+  // entry e at est / esu [e*S + s]; sorted agents of the line from
+  // xag_off[line] to xag_off[line+1]
+  const int* xrun_off;
+  const int4* xruns;
+  const double* est;
+  const double* esu;
+  const int* xag_off;
 };
 
 struct BatchStepsArgs {
@@ -86,6 +99,7 @@ struct BatchStepsArgs {
   int nsteps;
   double dt;
   int sources;  // any member has bulk or cell updates to apply
+  int* ctr;     // plane form: 2 * nsteps work-item counters, zeroed before the launch
 };
 
 __device__ __forceinline__ double member_cells(const StepMember& m, double x, int r, uint64_t vox,

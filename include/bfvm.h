@@ -397,8 +397,8 @@ BFVM_API int bfvm_batch_step(bfvm_batch* b, double dt, int nsteps, int flags);
 /* Autotuner: times short graph runs (trial_steps steps) of candidate chunk
  * lengths x threads per block for each axis, tunes every member's own sweeps
  * (bfvm_tune_sweeps, which branch mode runs), then candidate group budgets
- * in every mode (BFVM_BATCH_FUSED, BFVM_BATCH_BRANCHES, and
- * BFVM_BATCH_PERSISTENT at 8- and 16-point chunks), and keeps the fastest.  The members' fields are saved before and restored
+ * in every mode (BFVM_BATCH_FUSED, BFVM_BATCH_BRANCHES, BFVM_BATCH_PERSISTENT
+ * at each chunk length, BFVM_BATCH_PLANES), and keeps the fastest.  The members' fields are saved before and restored
  * after, so tuning does not advance the simulation. */
 BFVM_API int bfvm_batch_tune(bfvm_batch* b, double dt, int flags, int trial_steps);
 /* chunk[3] in {8,16,32} with threads[3] in {128,256,512} per axis, or 0/0 to
@@ -423,10 +423,23 @@ BFVM_API int bfvm_batch_get_config(bfvm_batch* b, int* chunk, int* threads, int6
  *                          field and lines of at most 128 points; the others
  *                          run as in BFVM_BATCH_BRANCHES, after the
  *                          persistent groups.
+ *   BFVM_BATCH_PLANES      as BFVM_BATCH_PERSISTENT (one cooperative launch
+ *                          per group for all n steps), with two phases per
+ *                          step: xy planes of a member (all its densities,
+ *                          or as many as fit 111 KB of shared memory) are
+ *                          staged in shared memory and solved along x, then
+ *                          y, one thread per whole line; then strips of xz
+ *                          planes are staged and solved along z, the next
+ *                          step's sources applied as the points are
+ *                          stored.  The field crosses L2 twice per step.
+ *                          Members with an FP64 field, lines of at most 128
+ *                          points and planes that fit; the others run as in
+ *                          BFVM_BATCH_BRANCHES.
  * bfvm_batch_tune chooses between them. */
 #define BFVM_BATCH_FUSED 0
 #define BFVM_BATCH_BRANCHES 1
 #define BFVM_BATCH_PERSISTENT 2
+#define BFVM_BATCH_PLANES 3
 BFVM_API int bfvm_batch_set_mode(bfvm_batch* b, int mode);
 BFVM_API int bfvm_batch_get_mode(bfvm_batch* b, int* mode);
 /* Work split of the persistent mode's kernel: chunks of 8 (default) or 16

@@ -98,7 +98,7 @@ __device__ __forceinline__ void plane_dirichlet(double* ln, int ls, const double
 // current one is solved and stored, so that the dependent chain of a point
 // is one FMA (a load issued after the store of the point before it would
 // otherwise wait for that store: the compiler cannot tell them apart).
-constexpr int kPlaneLineBatch = 8;
+constexpr int kPlaneLineBatch = 4;
 
 __device__ __forceinline__ double plane_forward(double* ln, int ls, int n, const double2* tab,
                                                 int ts) {
@@ -179,14 +179,19 @@ __device__ __noinline__ void plane_line(double* ln, int ls, int n, const double2
 }
 
 // Copies the {1/d, a} pairs of points 0..n-1, densities s0..s0+cnt-1, of a
-// member's axis table (pairs [point][S]) into shared memory as [point][cnt].
+// member's axis table (pairs [point][S], 16-byte aligned) into shared memory
+// as [point][cnt], with asynchronous 16-byte copies that bypass L1 (waited
+// for with the plane's copies).
 __device__ __forceinline__ void plane_stage_pairs(double2* dst, const double* k1, int n, int s0,
                                                   int cnt, int S) {
   const double2* src = reinterpret_cast<const double2*>(k1);
   const uint32_t M = udiv_magic((uint32_t)cnt);
   for (int w = threadIdx.x; w < n * cnt; w += blockDim.x) {
     const int k = (int)udiv((uint32_t)w, M);
-    dst[w] = __ldg(src + k * S + s0 + (w - k * cnt));
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst + w);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d),
+                 "l"(src + k * S + s0 + (w - k * cnt))
+                 : "memory");
   }
 }
 

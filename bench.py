@@ -493,7 +493,7 @@ def other_configs(local):
 
     from biofvm_b200 import STEP_ALL, Batch, Solver, load_scenario
     from biofvm_b200 import workloads as W
-    from biofvm_b200._abi import BATCH_BRANCHES, BATCH_PERSISTENT
+    from biofvm_b200._abi import BATCH_BRANCHES, BATCH_PERSISTENT, BATCH_PLANES
     from oracle import oracle as O
 
     out = {}
@@ -565,8 +565,11 @@ def other_configs(local):
         bt.add(sv)
     modes = {}
     err = 0.0
-    for name, md in (("branches", BATCH_BRANCHES), ("persistent", BATCH_PERSISTENT)):
+    # (mode, group budget): -1 = half of L2, 0 = every member in one group
+    for name, md, budget in (("branches", BATCH_BRANCHES, -1), ("persistent", BATCH_PERSISTENT, -1),
+                             ("planes", BATCH_PLANES, -1), ("planes_one_group", BATCH_PLANES, 0)):
         bt.set_mode(md)
+        bt.set_config((0, 0, 0), (0, 0, 0), budget)
         reset()
         bt.step(dt, 200, STEP_ALL)  # captures the graph
         bt.synchronize()
@@ -588,7 +591,8 @@ def other_configs(local):
     t_batch = modes["branches"]["seconds"]
     out["batched"] = {
         "workload": "64 instances, grids 32^3..128^3, 1-8 substrates, 0-20k agents, 200 steps",
-        "mode": "branches (default group budget, not tuned); the persistent mode beside it",
+        "mode": "branches (default group budget, not tuned); the persistent and plane modes "
+                "beside it",
         "batched_seconds": t_batch, "looped_plain_seconds": t_plain,
         "speedup_vs_looped_plain": t_plain / t_batch,
         "value": vs * 200 / t_batch, "unit": UNIT, "modes": modes,

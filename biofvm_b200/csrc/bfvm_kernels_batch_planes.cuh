@@ -49,11 +49,12 @@
 
 namespace bfvm {
 
-constexpr int kPlaneThreads = 256;
-// Shared memory of one block (two blocks per SM): the plane or strip being
-// solved (kPlaneSmemDoubles doubles, 96 KB) and the {1/d, a} pairs of its
-// lines (kPlaneTabPairs, 16 KB).
-constexpr int kPlaneSmemDoubles = 12288;
+constexpr int kPlaneThreads = 512;
+// Shared memory of the block (one per SM): the plane or strip being solved
+// (kPlaneSmemDoubles doubles, 208 KB: a 128 x 128 plane of one density at
+// its padded pitch fits) and the {1/d, a} pairs of its lines
+// (kPlaneTabPairs, 16 KB).
+constexpr int kPlaneSmemDoubles = 26624;
 constexpr int kPlaneTabPairs = 1024;
 constexpr int kPlaneLoadBatch = 16;   // stores in flight per thread while writing back
 
@@ -171,8 +172,8 @@ __device__ __forceinline__ void plane_backward(double* ln, int ls, int n, const 
 // One line solved in place: forward elimination, then back substitution,
 // with the line's {1/d_k, a_k} pair of point k at tab[k*ts] (shared memory,
 // or the member's table in global memory).  Not inlined: a line's registers
-// are allocated apart from the staging loops' (the kernel runs two blocks of
-// 256 threads per SM, 128 registers).
+// are allocated apart from the staging loops' (the kernel runs one block of
+// 512 threads per SM, 128 registers each).
 __device__ __noinline__ void plane_line(double* ln, int ls, int n, const double2* tab, int ts) {
   const double q = plane_forward(ln, ls, n, tab, ts);
   plane_backward(ln, ls, n, tab, ts, q);
@@ -416,7 +417,7 @@ __device__ __forceinline__ void plane_phase(const BatchStepsArgs& a, int* ctr, d
 // items of a phase; a.ctr holds 2 * nsteps zeroed counters; a.sources: the
 // members' bulk and cell updates run (their runs and agent offsets are in
 // place).
-__global__ void __launch_bounds__(kPlaneThreads, 2) batch_planes_kernel(const BatchStepsArgs a) {
+__global__ void __launch_bounds__(kPlaneThreads, 1) batch_planes_kernel(const BatchStepsArgs a) {
   namespace cg = cooperative_groups;
   cg::grid_group grid = cg::this_grid();
   extern __shared__ __align__(16) double plane_smem[];

@@ -1,7 +1,7 @@
 """Batch plane mode (BFVM_BATCH_PLANES): all steps of a group's members in
 one cooperative launch, two phases per step (xy planes staged in shared
-memory and solved along x then y; xz strips solved along z with the next
-step's sources on the stores).  Every member must end where stepping it
+memory, their x lines given their bulk and agent updates and solved, then
+their y lines; xz strips solved along z).  Every member must end where stepping it
 alone ends: against the oracle, FP64 relative max-norm per substrate
 <= 1e-12; against the plain single-instance path, <= 1e-10."""
 import numpy as np
@@ -90,17 +90,18 @@ def test_planes_graph_replay_and_partial_flags():
 
 def test_planes_split_densities_and_strips():
     """xy planes too large for one item hold a subset of the densities
-    (100 x 90 x 8: one density per item; 60 x 50 x 7: two or three); xz
+    (128 x 120 x 8: one density per item; 100 x 90 x 7: two per item); xz
     planes too large for one item are cut into strips of columns
-    (128 x 7 x 120 x 6: 768 columns of 120 points); 128-point lines on
-    every axis; a 128 x 128 plane (no item holds it) runs on a branch."""
-    scns = [W.mixed_small(shape=(100, 90, 6), S=8, n_agents=300, seed=401),
-            W.mixed_small(shape=(60, 50, 9), S=7, n_agents=200, seed=402),
-            W.mixed_small(shape=(128, 7, 120), S=6, n_agents=100, seed=403),
+    (128 x 7 x 120 x 20: 2560 columns of 120 points, the z pairs read from
+    the member's table); 128-point lines on every axis; a 128 x 128 plane of
+    one density fills an item."""
+    scns = [W.mixed_small(shape=(128, 120, 6), S=8, n_agents=300, seed=401),
+            W.mixed_small(shape=(100, 90, 9), S=7, n_agents=200, seed=402),
+            W.mixed_small(shape=(128, 7, 120), S=20, n_agents=100, seed=403),
             W.mixed_small(shape=(5, 128, 128), S=2, n_agents=100, seed=404),
             W.mixed_small(shape=(128, 128, 3), S=1, n_agents=50, seed=405)]
-    got, (groups, _) = run_planes(scns, 3)
-    assert groups >= 2  # the 128 x 128 member is in a group on branches
+    got, (groups, _) = run_planes(scns, 3, budget=0)
+    assert groups == 1  # every member runs in the plane kernel
     check_oracle(scns, got, 3)
 
 

@@ -119,19 +119,20 @@ void step_keeping_solves(bfvm_solver* m, double dt, int flags, const void* in, u
   }
 }
 
-void dot_into_acc(bfvm_solver* m, AdjointTape& T, const double* y, int axis) {
+// Blocks of the dot-product passes (the same for every solve of a run, so
+// their partial sums can accumulate in place).
+int dot_blocks(const bfvm_solver* m) {
+  const int64_t rows = (int64_t)m->ny * m->nz;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(8 * m->num_sms, rows));
+}
+
+// Adds this solve's -a.(L y) and -a.y partial sums to T.part.
+void dot_into_part(bfvm_solver* m, AdjointTape& T, const double* y, int axis) {
   const int S = m->S;
   const int threads = S * std::max(1, 256 / S);  // a multiple of S (S <= 256)
-  const int64_t rows = (int64_t)m->ny * m->nz;
-  const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(8 * m->num_sms, rows));
-  T.part.ensure((size_t)blocks * 2 * S * sizeof(double));
   const size_t smem = 2 * sizeof(double) * (size_t)threads;
-  adj_axis_dot_kernel<<<blocks, threads, smem, m->stream>>>(
+  adj_axis_dot_kernel<<<dot_blocks(m), threads, smem, m->stream>>>(
       T.abar.as<double>(), y, m->nx, m->ny, m->nz, S, axis, T.part.as<double>());
-  check_launch(m);
-  adj_reduce_parts_kernel<<<2 * S, kAdjReduceThreads, 0, m->stream>>>(T.part.as<double>(),
-                                                                      blocks, S,
-                                                                      T.acc.as<double>());
   check_launch(m);
 }
 
@@ -205,6 +206,9 @@ void adjoint_backward(bfvm_solver* m, const double* seed, int seed_on_device, do
                             st));
   T.acc.ensure(2 * S * sizeof(double));
   BFVM_CUDA(cudaMemsetAsync(T.acc.ptr, 0, 2 * S * sizeof(double), st));
+  const int dblocks = dot_blocks(m);
+  T.part.ensure((size_t)dblocks * 2 * S * sizeof(double));
+  BFVM_CUDA(cudaMemsetAsync(T.part.ptr, 0, (size_t)dblocks * 2 * S * sizeof(double), st));
   if (A > 0) {
     T.gt1.ensure((size_t)A * S * sizeof(double));
     T.gt2.ensure((size_t)A * S * sizeof(double));
@@ -232,7 +236,7 @@ void adjoint_backward(bfvm_solver* m, const double* seed, int seed_on_device, do
             FieldSwap f(m, T.abar.ptr);
             sweep(m, ax, 0, dt);
           }
-          dot_into_acc(m, T, reinterpret_cast<const double*>(ys[ax]), ax);
+          dot_into_part(m, T, reinterpret_cast<const double*>(ys[ax]), ax);
           zero_nodes(m, T);
         }
       }
@@ -253,6 +257,11 @@ void adjoint_backward(bfvm_solver* m, const double* seed, int seed_on_device, do
         check_launch(m);
       }
     }
+  }
+  if (flags & BFVM_STEP_DIFFUSION) {
+    adj_reduce_parts_kernel<<<2 * S, kAdjReduceThreads, 0, st>>>(T.part.as<double>(), dblocks,
+                                                                  S, T.acc.as<double>());
+    check_launch(m);
   }
   std::vector<double> acc(2 * S);
   BFVM_CUDA(cudaMemcpyAsync(acc.data(), T.acc.ptr, acc.size() * sizeof(double),

@@ -20,8 +20,10 @@ namespace bfvm {
 // b + gridDim.x, ...; blockDim.x is a multiple of S, so thread t keeps one
 // density s = t % S and steps through x = t / S, t / S + blockDim.x / S, ...
 // of each row (coalesced; the row's position along y and z is found once per
-// row, and along x by counting).  Each block writes its per-density partial
-// sums to part[block][2S]; the order of every sum is fixed.
+// row, and along x by counting).  Each block adds its per-density partial
+// sums to part[block][2S], which accumulates over every solve of a backward
+// run (zeroed at its start, reduced once at its end); the order of every sum
+// is fixed.
 static __global__ void adj_axis_dot_kernel(const double* __restrict__ a,
                                            const double* __restrict__ y, int nx, int ny, int nz,
                                            int S, int axis, double* __restrict__ part) {
@@ -66,14 +68,14 @@ static __global__ void adj_axis_dot_kernel(const double* __restrict__ a,
       L += sL[u];
       I += sI[u];
     }
-    part[(int64_t)blockIdx.x * 2 * S + t] = L;
-    part[(int64_t)blockIdx.x * 2 * S + S + t] = I;
+    part[(int64_t)blockIdx.x * 2 * S + t] += L;
+    part[(int64_t)blockIdx.x * 2 * S + S + t] += I;
   }
 }
 
 // acc[j] -= sum over blocks of part[.][j], one block of kAdjReduceThreads
 // per output j in [0, 2S) (thread i sums blocks i, i + kAdjReduceThreads, ...,
-// then a fixed tree): the solve's contributions -a.(L y) and -a.y.
+// then a fixed tree): the solves' contributions -a.(L y) and -a.y.
 constexpr int kAdjReduceThreads = 256;
 static __global__ void __launch_bounds__(kAdjReduceThreads)
     adj_reduce_parts_kernel(const double* __restrict__ part, int blocks, int S,

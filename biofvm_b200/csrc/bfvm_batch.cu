@@ -926,6 +926,7 @@ std::string plan_key(const bfvm_batch* b, double dt, int nsteps, int flags) {
       for (int a = 0; a < 3; ++a) {
         buf(m->coef[a]);
         buf(m->chunk[a]);
+        buf(m->chunk_il[a]);
         buf(m->chunk_slots[a]);
       }
       for (const DevBuf* d : {&m->d_bulk_vox, &m->d_bulk_st, &m->d_bulk_su, &m->d_dir_vox,

@@ -76,12 +76,23 @@ __device__ __forceinline__ void st_fold(Pair<float>* p, float a, float b) {
 }
 
 // Chunk tables of one axis in the sweep precision (see chunk_tables()),
-// interleaved [point][density] and stored once per distinct chunk ("slot").
+// stored once per distinct chunk ("slot").  Two layouts, chosen by the PL
+// template flag of the helpers below:
+//   PL = false (interleaved): k1, kg [slot][ch][S][2]; kc [chunk][S][4]
+//   PL = true  (planar):      k1, kg [slot][ch][2][S]; kc [chunk][4][S]
+// In the planar layout the lanes of a warp, which hold consecutive
+// densities, read one component of consecutive densities: 8-byte loads of
+// contiguous words, one shared-memory wavefront for up to 16 densities,
+// where the interleaved slopes and transfer constants sit 16 and 32 bytes
+// apart and cost two or three.  The line and direct kernels use the planar
+// layout; the row kernel and the batch tile form the interleaved one (one
+// 16-byte load per entry, where the row kernel's extra address arithmetic
+// for two planar loads cost more than the wavefronts saved).
 template <typename T>
 struct ChunkCoef {
-  const T* k1;    // [slot][ch][S][2] {1/d, a}
-  const T* kg;    // [slot][ch][S][2] {G, R}
-  const T* kc;    // [chunk][S][4] {P_end, G_start, R_start, 0}
+  const T* k1;    // {1/d, a} per point and density
+  const T* kg;    // {G, R} per point and density
+  const T* kc;    // {P_end, G_start, R_start, 0} per chunk and density
   const int* slot;  // [nc] slot of each chunk of the line
   int ch;
   int nc;
@@ -107,10 +118,19 @@ __device__ __forceinline__ ChunkCoef<T> stage_tables(const ChunkCoef<T>& g, T* s
   return s;
 }
 
-// This density's rows of chunk c: k1 and kg step 2*S elements per point.
-template <bool SMEM, typename T>
+// This density's rows of chunk c: k1 and kg step 2*S elements per point in
+// both layouts.
+template <bool SMEM, typename T, bool PL = false>
 __device__ __forceinline__ size_t chunk_row(const ChunkCoef<T>& cc, int c, int s, int S) {
-  return ((size_t)ld_one<SMEM>(cc.slot + c) * cc.ch * S + s) * 2;
+  const size_t base = (size_t)ld_one<SMEM>(cc.slot + c) * cc.ch * S * 2;
+  return PL ? base + s : base + (size_t)s * 2;
+}
+// {x, y} components of one (point, density) entry of k1 or kg: the second
+// component S elements after the first (planar) or beside it (interleaved).
+template <bool SMEM, bool PL, typename T>
+__device__ __forceinline__ Pair<T> ld_entry(const T* p, int S) {
+  if (PL) return {ld_one<SMEM>(p), ld_one<SMEM>(p + S)};
+  return ld_pair<SMEM>(p);
 }
 
 template <typename T, typename CT = T>
@@ -167,24 +187,25 @@ __device__ __forceinline__ uint32_t smem_pad128(const unsigned char* smem) {
 // apart.  Returns the chunk's last forward value (qe) and first backward
 // value (x0).  The backward pass reads the slopes a_k again (cheaper than
 // holding CH more registers).
-template <bool SMEM, typename T, int CH>
+template <bool SMEM, typename T, int CH, bool PL = false>
 __device__ __forceinline__ void chunk_local(T (&v)[CH], int len, const T* k1, int S, T& qe,
                                             T& x0) {
   T q = T(0);
 #pragma unroll
   for (int m = 0; m < CH; ++m) {
     if (m < len) {
-      const Pair<T> c = ld_pair<SMEM>(k1 + (size_t)2 * S * m);
+      const Pair<T> c = ld_entry<SMEM, PL>(k1 + (size_t)2 * S * m, S);
       q = fma(c.y, q, v[m] * c.x);
       v[m] = q;
     }
   }
   qe = q;
   T x = T(0);
+  const int aoff = PL ? S : 1;  // the slope a_k beside 1/d_k
 #pragma unroll
   for (int m = CH - 1; m >= 0; --m) {
     if (m < len) {
-      x = fma(ld_one<SMEM>(k1 + (size_t)2 * S * m + 1), x, v[m]);
+      x = fma(ld_one<SMEM>(k1 + (size_t)2 * S * m + aoff), x, v[m]);
       v[m] = x;
     }
   }
@@ -194,16 +215,17 @@ __device__ __forceinline__ void chunk_local(T (&v)[CH], int len, const T* k1, in
 // One pass over the chunks of a line: the forward carry into chunk c (cf) and
 // the backward carry into it (cb), from every chunk's (qe, x0) pair in shared
 // memory (fold columns fw apart) and the chunks' transfer constants.
-template <bool SMEM, typename T>
+template <bool SMEM, typename T, bool PL = false>
 __device__ __forceinline__ void chunk_carries(const Pair<T>* fold, int fw, int col, int c, int NC,
                                               const ChunkCoef<T>& tab, int s, int S, T& cf_out,
                                               T& cb_out) {
   T cf = T(0), cb = T(0), w = T(1), my = T(0);
-  const T* t = tab.kc + (size_t)4 * s;
+  const T* t = tab.kc + (PL ? (size_t)s : (size_t)4 * s);
 #pragma unroll 4
   for (int cc = 0; cc < NC; ++cc, t += (size_t)4 * S) {
-    const Pair<T> ag = ld_pair<SMEM>(t);       // {P_end, G_start}
-    const T r0 = ld_one<SMEM>(t + 2);          // R_start
+    // {P_end, G_start} and R_start
+    const Pair<T> ag = PL ? Pair<T>{ld_one<SMEM>(t), ld_one<SMEM>(t + S)} : ld_pair<SMEM>(t);
+    const T r0 = ld_one<SMEM>(t + (PL ? 2 * S : 2));
     const Pair<T> f = ld_fold(fold + cc * fw + col);  // {qe, x0} of chunk cc
     if (cc == c) my = cf;
     if (cc > c) {
@@ -216,12 +238,12 @@ __device__ __forceinline__ void chunk_carries(const Pair<T>* fold, int fw, int c
   cb_out = cb;
 }
 
-template <bool SMEM, typename T, int CH>
+template <bool SMEM, typename T, int CH, bool PL = false>
 __device__ __forceinline__ void chunk_fix(T (&v)[CH], int len, const T* kg, int S, T cf, T cb) {
 #pragma unroll
   for (int m = 0; m < CH; ++m) {
     if (m < len) {
-      const Pair<T> gr = ld_pair<SMEM>(kg + (size_t)2 * S * m);
+      const Pair<T> gr = ld_entry<SMEM, PL>(kg + (size_t)2 * S * m, S);
       v[m] = fma(cf, gr.x, fma(cb, gr.y, v[m]));
     }
   }
@@ -326,9 +348,9 @@ __global__ void __launch_bounds__(W * MAXNC)
 #pragma unroll
     for (int m = 0; m < CH; ++m) v[m] = (m < lenA) ? (CT)buf[m * W] : CT(0);
 
-    const size_t row = chunk_row<SMEM_TAB>(tab, c, s, S);
+    const size_t row = chunk_row<SMEM_TAB, CT, true>(tab, c, s, S);
     CT qe, x0;
-    chunk_local<SMEM_TAB, CT, CH>(v, lenA, tab.k1 + row, S, qe, x0);
+    chunk_local<SMEM_TAB, CT, CH, true>(v, lenA, tab.k1 + row, S, qe, x0);
     Pair<CT>* sF = fold + (i & 1) * NC * W;
     st_fold(sF + c * W + tx, qe, x0);
     // every thread has read its chunk of this stage: it can be refilled
@@ -344,9 +366,9 @@ __global__ void __launch_bounds__(W * MAXNC)
       }
     }
     CT cf, cb;
-    chunk_carries<SMEM_TAB, CT>(sF, W, tx, c, NC, tab, s, S, cf, cb);
+    chunk_carries<SMEM_TAB, CT, true>(sF, W, tx, c, NC, tab, s, S, cf, cb);
     if (lenA == 0) continue;
-    chunk_fix<SMEM_TAB, CT, CH>(v, lenA, tab.kg + row, S, cf, cb);
+    chunk_fix<SMEM_TAB, CT, CH, true>(v, lenA, tab.kg + row, S, cf, cb);
     if (DIR_EPI) {
       const int64_t vcol = (int64_t)outer * a.C + col;
       const int64_t seg = (vcol / S) * a.nchunks + c;
@@ -624,15 +646,15 @@ __global__ void __launch_bounds__(512) lod_sweep_direct_kernel(const DirectArgs<
   ChunkCoef<CT> tab = a.cc;
   tab.kc = kc_sm;
   tab.slot = slot_sm;
-  const size_t row = active ? ((size_t)slot_sm[c] * tab.ch * S + s) * 2 : 0;
+  const size_t row = active ? (size_t)slot_sm[c] * tab.ch * S * 2 + s : 0;  // planar
   CT qe, x0;
-  chunk_local<false, CT, CH>(v, lenA, a.cc.k1 + row, S, qe, x0);
+  chunk_local<false, CT, CH, true>(v, lenA, a.cc.k1 + row, S, qe, x0);
   st_fold(fold + c * W + tx, qe, x0);
   __syncthreads();
   CT cf, cb;
-  chunk_carries<true, CT>(fold, W, tx, c, NC, tab, s, S, cf, cb);
+  chunk_carries<true, CT, true>(fold, W, tx, c, NC, tab, s, S, cf, cb);
   if (lenA == 0) return;
-  chunk_fix<false, CT, CH>(v, lenA, a.cc.kg + row, S, cf, cb);
+  chunk_fix<false, CT, CH, true>(v, lenA, a.cc.kg + row, S, cf, cb);
   if (MODE != kSweepPlain && (a.fuse & kFuseDirEpi))
     apply_dirichlet_seg<CT, CH>(v, a.dir_epi, seg, k0, S, s);
   T* dst = a.out + (ptr - a.p);

@@ -217,8 +217,15 @@ void thomas_setup(bfvm_solver* m, double dt) {
 // bit-identical share one slot: away from the two line ends the Thomas
 // denominators converge to a fixed point, so most interior chunks of a long
 // line are the same and the tables the kernels read stay small enough for L1.
+//
+// Two copies are kept (bfvm::ChunkCoef): the planar one, which the line and
+// direct kernels read (their warps meet up to twenty distinct densities of
+// two chunks, and the planar words cut their shared-memory wavefronts), and
+// the interleaved one, which the row kernel reads (one 16-byte load per
+// entry: measured faster there than two planar loads, whose extra address
+// arithmetic outweighed the wavefronts saved).
 template <typename T>
-bfvm::ChunkCoef<T> chunk_view(bfvm_solver* m, int a) {
+bfvm::ChunkCoef<T> chunk_view(bfvm_solver* m, int a, bool interleaved = false) {
   const int ns[3] = {m->nx, m->ny, m->nz};
   const int n = ns[a], S = m->S, ch = m->axis[a].ch;
   const int nc = (n + ch - 1) / ch;
@@ -256,19 +263,36 @@ bfvm::ChunkCoef<T> chunk_view(bfvm_solver* m, int a) {
     }
     const size_t ns_ = slot_chunk.size();
     const size_t k1n = up4(ns_ * cw), kgn = up4(ns_ * cw), kcn = up4((size_t)nc * S * 4);
-    std::vector<double> tab(k1n + kgn + kcn, 0.0);
+    std::vector<double> tab(k1n + kgn + kcn, 0.0), til(k1n + kgn + kcn, 0.0);
+    // planar (tab): per point the S first components, then the S second
+    // ones; per chunk the S values of each transfer constant in turn.
+    // Interleaved (til): chunk_tables()'s own order.
     for (size_t sl = 0; sl < ns_; ++sl) {
-      const int r = slot_chunk[sl];
-      std::copy_n(&k1[r * cw], cw, &tab[sl * cw]);
-      std::copy_n(&kg[r * cw], cw, &tab[k1n + sl * cw]);
+      const size_t r = (size_t)slot_chunk[sl];
+      std::copy_n(&k1[r * cw], cw, &til[sl * cw]);
+      std::copy_n(&kg[r * cw], cw, &til[k1n + sl * cw]);
+      for (size_t q = 0; q < (size_t)ch; ++q)
+        for (size_t s = 0; s < (size_t)S; ++s)
+          for (size_t j = 0; j < 2; ++j) {
+            const size_t src = r * cw + (q * S + s) * 2 + j;
+            const size_t dst = sl * cw + (q * 2 + j) * S + s;
+            tab[dst] = k1[src];
+            tab[k1n + dst] = kg[src];
+          }
     }
     // transfer constants per chunk (not per slot): the fold reads every chunk
-    std::copy_n(kc.data(), (size_t)nc * S * 4, &tab[k1n + kgn]);
+    std::copy_n(kc.data(), (size_t)nc * S * 4, &til[k1n + kgn]);
+    for (size_t c = 0; c < (size_t)nc; ++c)
+      for (size_t s = 0; s < (size_t)S; ++s)
+        for (size_t j = 0; j < 4; ++j)
+          tab[k1n + kgn + (c * 4 + j) * S + s] = kc[(c * S + s) * 4 + j];
     if (sizeof(T) == sizeof(double)) {
       upload(m->chunk[a], tab, m->stream);
+      upload(m->chunk_il[a], til, m->stream);
     } else {
-      std::vector<float> tf(tab.begin(), tab.end());
+      std::vector<float> tf(tab.begin(), tab.end()), tfi(til.begin(), til.end());
       upload(m->chunk[a], tf, m->stream);
+      upload(m->chunk_il[a], tfi, m->stream);
     }
     upload(m->chunk_slots[a], slot_of, m->stream);
     m->chunk_ch[a] = ch;
@@ -277,7 +301,7 @@ bfvm::ChunkCoef<T> chunk_view(bfvm_solver* m, int a) {
   const size_t cw = (size_t)ch * S * 2;
   const size_t ns_ = (size_t)m->chunk_nslots[a];
   const size_t k1n = up4(ns_ * cw), kgn = up4(ns_ * cw);
-  const T* base = m->chunk[a].as<T>();
+  const T* base = (interleaved ? m->chunk_il[a] : m->chunk[a]).as<T>();
   bfvm::ChunkCoef<T> c;
   c.k1 = base;
   c.kg = base + k1n;
@@ -1100,7 +1124,7 @@ void launch_rows(bfvm_solver* m, const RowsPlan& P, int fuse, double dt, int64_t
   a.nchunks = P.nc;
   a.R = P.R;
   a.pitch = P.pitch;
-  a.cc = chunk_view<CT>(m, 0);
+  a.cc = chunk_view<CT>(m, 0, /*interleaved=*/true);
   a.dt = dt;
   if ((fuse & bfvm::kFuseBulk) && !m->seg_bulk.present) fuse &= ~bfvm::kFuseBulk;
   if ((fuse & bfvm::kFuseCells) && !m->seg_cells.present) fuse &= ~bfvm::kFuseCells;
@@ -1527,6 +1551,7 @@ int bfvm_destroy(bfvm_solver* m) {
     m->d_grad.release();
     adjoint_release(m);
     for (auto& c : m->chunk) c.release();
+    for (auto& c : m->chunk_il) c.release();
     for (auto& c : m->chunk_slots) c.release();
     for (auto& c : m->cl_tab) c.release();
     m->d_grid_maps.release();

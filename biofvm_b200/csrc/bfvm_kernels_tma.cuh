@@ -84,10 +84,13 @@ __device__ __forceinline__ void st_fold(Pair<float>* p, float a, float b) {
 // densities, read one component of consecutive densities: 8-byte loads of
 // contiguous words, one shared-memory wavefront for up to 16 densities,
 // where the interleaved slopes and transfer constants sit 16 and 32 bytes
-// apart and cost two or three.  The line and direct kernels use the planar
-// layout; the row kernel and the batch tile form the interleaved one (one
-// 16-byte load per entry, where the row kernel's extra address arithmetic
-// for two planar loads cost more than the wavefronts saved).
+// apart and cost two or three.  Only the FP64 line kernel at full-width
+// tiles (16 columns: up to twenty distinct densities of two chunks per warp)
+// reads the planar layout (lines_planar()); the row, direct and half-width
+// line kernels and the batch tile form read the interleaved one: where a
+// warp meets at most eight densities one 16-byte load per entry already
+// takes one wavefront, and in the row kernel the extra address arithmetic
+// of two planar loads cost more than the wavefronts it saved.
 template <typename T>
 struct ChunkCoef {
   const T* k1;    // {1/d, a} per point and density
@@ -276,6 +279,10 @@ __device__ __forceinline__ void drain_after_failure(uint64_t* full, int stages, 
 
 // ---------------------------------------------------------------------------
 
+// Whether the line kernel with W columns reads the planar chunk tables (the
+// host passes the matching copy).
+constexpr bool lines_planar(int math_bytes, int w) { return math_bytes == 8 && w == 16; }
+
 // MAXNC: the most chunks per line the kernel is compiled for (block of
 // W x MAXNC threads).  MAXNC = 8 with 32-point chunks (lines of up to 256
 // points) lets the compiler give each thread the registers for its 32 values
@@ -285,6 +292,7 @@ template <typename T, int CH, int W, int STAGES, bool DIR_EPI, bool SMEM_TAB, in
 __global__ void __launch_bounds__(W * MAXNC)
     lod_lines_tma_kernel(const __grid_constant__ CUtensorMap map, const LinesArgs<T, CT> a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
+  constexpr bool PL = lines_planar((int)sizeof(CT), W);
   const int NC = blockDim.y;
   const int npad = a.box_n * a.nboxes;
   const size_t stage_elems = (size_t)npad * W;
@@ -348,9 +356,9 @@ __global__ void __launch_bounds__(W * MAXNC)
 #pragma unroll
     for (int m = 0; m < CH; ++m) v[m] = (m < lenA) ? (CT)buf[m * W] : CT(0);
 
-    const size_t row = chunk_row<SMEM_TAB, CT, true>(tab, c, s, S);
+    const size_t row = chunk_row<SMEM_TAB, CT, PL>(tab, c, s, S);
     CT qe, x0;
-    chunk_local<SMEM_TAB, CT, CH, true>(v, lenA, tab.k1 + row, S, qe, x0);
+    chunk_local<SMEM_TAB, CT, CH, PL>(v, lenA, tab.k1 + row, S, qe, x0);
     Pair<CT>* sF = fold + (i & 1) * NC * W;
     st_fold(sF + c * W + tx, qe, x0);
     // every thread has read its chunk of this stage: it can be refilled
@@ -366,9 +374,9 @@ __global__ void __launch_bounds__(W * MAXNC)
       }
     }
     CT cf, cb;
-    chunk_carries<SMEM_TAB, CT, true>(sF, W, tx, c, NC, tab, s, S, cf, cb);
+    chunk_carries<SMEM_TAB, CT, PL>(sF, W, tx, c, NC, tab, s, S, cf, cb);
     if (lenA == 0) continue;
-    chunk_fix<SMEM_TAB, CT, CH, true>(v, lenA, tab.kg + row, S, cf, cb);
+    chunk_fix<SMEM_TAB, CT, CH, PL>(v, lenA, tab.kg + row, S, cf, cb);
     if (DIR_EPI) {
       const int64_t vcol = (int64_t)outer * a.C + col;
       const int64_t seg = (vcol / S) * a.nchunks + c;
@@ -646,15 +654,15 @@ __global__ void __launch_bounds__(512) lod_sweep_direct_kernel(const DirectArgs<
   ChunkCoef<CT> tab = a.cc;
   tab.kc = kc_sm;
   tab.slot = slot_sm;
-  const size_t row = active ? (size_t)slot_sm[c] * tab.ch * S * 2 + s : 0;  // planar
+  const size_t row = active ? ((size_t)slot_sm[c] * tab.ch * S + s) * 2 : 0;
   CT qe, x0;
-  chunk_local<false, CT, CH, true>(v, lenA, a.cc.k1 + row, S, qe, x0);
+  chunk_local<false, CT, CH>(v, lenA, a.cc.k1 + row, S, qe, x0);
   st_fold(fold + c * W + tx, qe, x0);
   __syncthreads();
   CT cf, cb;
-  chunk_carries<true, CT, true>(fold, W, tx, c, NC, tab, s, S, cf, cb);
+  chunk_carries<true, CT>(fold, W, tx, c, NC, tab, s, S, cf, cb);
   if (lenA == 0) return;
-  chunk_fix<false, CT, CH, true>(v, lenA, a.cc.kg + row, S, cf, cb);
+  chunk_fix<false, CT, CH>(v, lenA, a.cc.kg + row, S, cf, cb);
   if (MODE != kSweepPlain && (a.fuse & kFuseDirEpi))
     apply_dirichlet_seg<CT, CH>(v, a.dir_epi, seg, k0, S, s);
   T* dst = a.out + (ptr - a.p);

@@ -218,12 +218,13 @@ void thomas_setup(bfvm_solver* m, double dt) {
 // denominators converge to a fixed point, so most interior chunks of a long
 // line are the same and the tables the kernels read stay small enough for L1.
 //
-// Two copies are kept (bfvm::ChunkCoef): the planar one, which the line and
-// direct kernels read (their warps meet up to twenty distinct densities of
-// two chunks, and the planar words cut their shared-memory wavefronts), and
-// the interleaved one, which the row kernel reads (one 16-byte load per
-// entry: measured faster there than two planar loads, whose extra address
-// arithmetic outweighed the wavefronts saved).
+// Two copies are kept (bfvm::ChunkCoef): the planar one, which the FP64 line
+// kernel at 16-column tiles reads (its warps meet up to twenty distinct
+// densities of two chunks, and the planar words cut its shared-memory
+// wavefronts: y sweep 0.528 -> 0.486 ms at 256^3 x 10), and the interleaved
+// one, which every other kernel reads (one 16-byte load per entry: faster in
+// the row kernel, 0.656 against 0.828 ms, and in the half-width line tiles
+// of 1024-point lines, whose warps meet at most eight densities).
 template <typename T>
 bfvm::ChunkCoef<T> chunk_view(bfvm_solver* m, int a, bool interleaved = false) {
   const int ns[3] = {m->nx, m->ny, m->nz};
@@ -972,7 +973,7 @@ void launch_lines(bfvm_solver* m, int ax, const LinesPlan& L, bool dir, int64_t 
   a.box_n = L.box_n;
   a.nboxes = L.nboxes;
   a.nchunks = L.nc;
-  a.cc = chunk_view<CT>(m, ax);
+  a.cc = chunk_view<CT>(m, ax, /*interleaved=*/!bfvm::lines_planar((int)sizeof(CT), L.w));
   a.status = m->d_status.as<int>();
   if (dir) a.dir_epi = m->seg_dir_y.view();
   dim3 block(L.w, L.nc);
@@ -1035,7 +1036,7 @@ bool launch_direct(bfvm_solver* m, int ax, int fuse, double dt, int64_t z0 = 0,
   a.out = m->sweep_out ? static_cast<T*>(m->sweep_out) : a.p;
   a.S = (int)S;
   a.nchunks = nc;
-  a.cc = chunk_view<CT>(m, ax);
+  a.cc = chunk_view<CT>(m, ax, /*interleaved=*/true);
   a.dt = dt;
   if ((fuse & bfvm::kFuseBulk) && !m->seg_bulk.present) fuse &= ~bfvm::kFuseBulk;
   if ((fuse & bfvm::kFuseCells) && !m->seg_cells.present) fuse &= ~bfvm::kFuseCells;

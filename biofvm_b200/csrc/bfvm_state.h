@@ -159,8 +159,8 @@ struct bfvm_solver {
   bfvm_rt::DevBuf coef[3];  // per axis: inv_den, fwd, bwd [n*S] then c1 [S], in the sweep precision
   std::vector<double> h_c1[3], h_den[3], h_cx[3];  // FP64 host copies per axis
   bfvm_rt::DevBuf chunk[3];     // per axis: chunk tables k1, kg, kc by slot (sweep precision),
-                                // planar layout (line and direct kernels)
-  bfvm_rt::DevBuf chunk_il[3];  // the same tables interleaved (row kernel)
+                                // planar layout (FP64 line kernel at 16-column tiles)
+  bfvm_rt::DevBuf chunk_il[3];  // the same tables interleaved (every other kernel)
   bfvm_rt::DevBuf chunk_slots[3];  // per axis: slot of every chunk
   int chunk_ch[3] = {0, 0, 0};
   int chunk_nslots[3] = {0, 0, 0};

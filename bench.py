@@ -336,6 +336,9 @@ def run_ours(args, world, rank, local):
     # the per-axis kernel choice timed on this field (which is restored)
     sv.step(dt, args.warmup, STEP_ALL)
     tuned = sv.tune_sweeps(dt, 3) if not args.no_tune else [(0, 0, 0, 0, 0)] * 3
+    if args.row_build is not None:
+        sv.set_row_build(args.row_build)
+    row_build = sv.get_row_build()
     sv.synchronize()
 
     launches0 = sv.launch_count
@@ -462,6 +465,7 @@ def run_ours(args, world, rank, local):
             "tuned_sweeps": [{"axis": "xyz"[i], "kernel": ["default", "register", "tma", "direct"][k],
                               "chunk": ch, "columns": tw, "min_blocks": mb, "row_stages": st}
                              for i, (k, ch, tw, mb, st) in enumerate(tuned)],
+            "row_build": dict(zip(("requested", "effective"), row_build)),
             "slab_planes": sv.get_slab_planes(), "fuse_sources": sv.get_fuse_sources(),
             "gpu_launches": int(launches),
             "e2e": e2e,
@@ -1282,6 +1286,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-configs", action="store_true",
                     help="lod256: skip the brief 50^3 and batched measurements")
+    ap.add_argument("--row-build", type=int, choices=[0, 1, 2], default=None,
+                    help="lod256: x row-kernel build after tuning (0 any density count, "
+                         "1 built for this density count, 2 the same with planar tables)")
     ap.add_argument("--no-tune", action="store_true",
                     help="keep the default kernel per axis (for profiler launch lists)")
     ap.add_argument("--size", type=int, default=256, help="cube edge in voxels (default 256)")

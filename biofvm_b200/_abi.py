@@ -88,6 +88,8 @@ SIGNATURES = {
     "bfvm_set_sweep_config": (c_int, [_P, c_int, c_int, c_int, c_int]),
     "bfvm_get_sweep_config": (c_int, [_P, c_int, _IP]),
     "bfvm_set_row_stages": (c_int, [_P, c_int]),
+    "bfvm_set_row_build": (c_int, [_P, c_int]),
+    "bfvm_get_row_build": (c_int, [_P, _IP, _IP]),
     "bfvm_set_kernel_path": (c_int, [_P, c_int]),
     "bfvm_set_fuse_sources": (c_int, [_P, c_int]),
     "bfvm_get_fuse_sources": (c_int, [_P, _IP]),

@@ -399,15 +399,18 @@ constexpr int rows_min_blocks(int ch, int maxt) { return (ch <= 16 && maxt <= 25
 
 // MINB: resident blocks per SM the kernel is compiled for (two at 32-point
 // chunks caps the registers at 128: more warps, some spilled state).
+// SC > 0: a build for exactly SC densities (a.S == SC), so that every offset
+// along a row (stage, tables, stores: multiples of S) is a compile-time
+// constant; PLR: that build reading the planar chunk tables.
 template <typename T, int CH, int STAGES, bool SMEM_TAB, int MAXT, typename CT = T,
-          int MINB = rows_min_blocks(CH, MAXT)>
+          int MINB = rows_min_blocks(CH, MAXT), int SC = 0, bool PLR = false>
 __global__ void __launch_bounds__(MAXT, MINB)
     lod_rows_tma_kernel(const RowsArgs<T, CT> a) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   // Threads: column (r, s) fastest, then chunk c.  A stage holds R rows at a
   // padded pitch (pitch = S mod 16 elements), so the lanes of a warp, which
   // read consecutive columns, hit consecutive banks.
-  const int S = a.S;
+  const int S = SC > 0 ? SC : a.S;
   const int n = a.n;
   const int R = a.R;
   const int FW = R * S;  // columns per tile
@@ -445,7 +448,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
     tma::fence_barrier_init();
   }
   __syncthreads();
-  const size_t crow = (c < NC) ? chunk_row<SMEM_TAB>(tab, c, s, S) : 0;
+  const size_t crow = (c < NC) ? chunk_row<SMEM_TAB, CT, PLR>(tab, c, s, S) : 0;
   const CT* k1 = tab.k1 + crow;
   const CT* kg = tab.kg + crow;
 
@@ -518,7 +521,7 @@ __global__ void __launch_bounds__(MAXT, MINB)
 
     // ---- sweep
     CT qe, x0;
-    chunk_local<SMEM_TAB, CT, CH>(v, lenA, k1, S, qe, x0);
+    chunk_local<SMEM_TAB, CT, CH, PLR>(v, lenA, k1, S, qe, x0);
     Pair<CT>* sF = fold + (i & 1) * NC * FW;
     if (c < NC && fc < FW) st_fold(sF + c * FW + fc, qe, x0);
     // every thread has its chunk in registers: the stage can be refilled
@@ -535,8 +538,8 @@ __global__ void __launch_bounds__(MAXT, MINB)
     }
     if (lenA == 0) continue;
     CT cf, cb;
-    chunk_carries<SMEM_TAB, CT>(sF, FW, fc, c, NC, tab, s, S, cf, cb);
-    chunk_fix<SMEM_TAB, CT, CH>(v, lenA, kg, S, cf, cb);
+    chunk_carries<SMEM_TAB, CT, PLR>(sF, FW, fc, c, NC, tab, s, S, cf, cb);
+    chunk_fix<SMEM_TAB, CT, CH, PLR>(v, lenA, kg, S, cf, cb);
     // ---- epilogue: Dirichlet before the next axis
     if (a.fuse & kFuseDirEpi) apply_dirichlet_seg<CT, CH>(v, a.dir, seg, k0, S, s);
     // straight to global memory: the lanes of a warp write the S densities of

@@ -786,9 +786,13 @@ LinesPlan plan_lines(const bfvm_solver* m, int ax) {
   return L;
 }
 
+// Density counts the row kernel has builds for (bfvm_set_row_build).
+bool row_build_count(int S) { return S == 4 || S == 8 || S == 10 || S == 16; }
+
 struct RowsPlan {
   bool ok = false;
   bool smem_tab = false;
+  int build = 0;  // row build that runs (Axis::build where it applies, else 0)
   int ch = 0, nc = 0, R = 0, stages = 0, maxt = 256;
   int tpc = 0;  // threads per chunk
   int minb = 1;  // resident blocks per SM the kernel is compiled for
@@ -861,6 +865,14 @@ RowsPlan plan_rows(const bfvm_solver* m) {
         P.smem_tab = staged != 0;
         P.smem = smem;
         P.ok = true;
+        // the builds for one density count exist for FP64 rows at 32-point
+        // chunks, tables in shared memory, one block of <= 256 threads per
+        // SM and a two-tile ring, with 4, 8, 10 or 16 densities
+        const int b = m->axis[0].build;
+        P.build = (b != 0 && es == 8 && m->math_elem() == 8 && P.ch == 32 && P.smem_tab &&
+                   maxt == 256 && minb == 1 && nst == 2 && row_build_count(m->S))
+                      ? b
+                      : 0;
         return P;
       }
     }
@@ -1065,8 +1077,37 @@ bool launch_direct(bfvm_solver* m, int ax, int fuse, double dt, int64_t z0 = 0,
 
 template <typename T, typename CT, int CH, bool TAB, int MAXT, int ST,
           int MINB = bfvm::rows_min_blocks(CH, MAXT)>
-void launch_rows_inst(const bfvm::RowsArgs<T, CT>& a, dim3 block, size_t smem, bfvm_solver* m) {
+void launch_rows_inst(const bfvm::RowsArgs<T, CT>& a, dim3 block, size_t smem, bfvm_solver* m,
+                      int build = 0) {
   auto k = bfvm::lod_rows_tma_kernel<T, CH, ST, TAB, MAXT, CT, MINB>;
+  if constexpr (std::is_same<T, double>::value && std::is_same<CT, double>::value && CH == 32 &&
+                TAB && MAXT == 256 && ST == 2 && MINB == 1) {
+    if (build != 0) {
+      require(row_build_count(a.S), "row build for another density count", BFVM_ERR_STATE);
+      const bool pl = build == 2;
+      using bfvm::lod_rows_tma_kernel;
+      switch (a.S) {
+        case 4:
+          k = pl ? lod_rows_tma_kernel<T, CH, ST, TAB, MAXT, CT, MINB, 4, true>
+                 : lod_rows_tma_kernel<T, CH, ST, TAB, MAXT, CT, MINB, 4, false>;
+          break;
+        case 8:
+          k = pl ? lod_rows_tma_kernel<T, CH, ST, TAB, MAXT, CT, MINB, 8, true>
+                 : lod_rows_tma_kernel<T, CH, ST, TAB, MAXT, CT, MINB, 8, false>;
+          break;
+        case 10:
+          k = pl ? lod_rows_tma_kernel<T, CH, ST, TAB, MAXT, CT, MINB, 10, true>
+                 : lod_rows_tma_kernel<T, CH, ST, TAB, MAXT, CT, MINB, 10, false>;
+          break;
+        default:
+          k = pl ? lod_rows_tma_kernel<T, CH, ST, TAB, MAXT, CT, MINB, 16, true>
+                 : lod_rows_tma_kernel<T, CH, ST, TAB, MAXT, CT, MINB, 16, false>;
+          break;
+      }
+    }
+  } else {
+    require(build == 0, "row build without a kernel", BFVM_ERR_STATE);
+  }
   allow_smem((const void*)k, m->device, smem);
   int per_sm = 0;
   BFVM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, block.x * block.y, smem));
@@ -1084,7 +1125,7 @@ void launch_rows_st(const bfvm::RowsArgs<T, CT>& a, const RowsPlan& P, dim3 bloc
       launch_rows_inst<T, CT, CH, false, 256, ST, 2>(a, block, P.smem, m);
   } else if (P.maxt == 256) {
     if (P.smem_tab)
-      launch_rows_inst<T, CT, CH, true, 256, ST>(a, block, P.smem, m);
+      launch_rows_inst<T, CT, CH, true, 256, ST>(a, block, P.smem, m, P.build);
     else
       launch_rows_inst<T, CT, CH, false, 256, ST>(a, block, P.smem, m);
   } else {
@@ -1125,7 +1166,7 @@ void launch_rows(bfvm_solver* m, const RowsPlan& P, int fuse, double dt, int64_t
   a.nchunks = P.nc;
   a.R = P.R;
   a.pitch = P.pitch;
-  a.cc = chunk_view<CT>(m, 0, /*interleaved=*/true);
+  a.cc = chunk_view<CT>(m, 0, /*interleaved=*/P.build != 2);
   a.dt = dt;
   if ((fuse & bfvm::kFuseBulk) && !m->seg_bulk.present) fuse &= ~bfvm::kFuseBulk;
   if ((fuse & bfvm::kFuseCells) && !m->seg_cells.present) fuse &= ~bfvm::kFuseCells;
@@ -2613,7 +2654,7 @@ void tune_sweeps(bfvm_solver* m, double dt, int reps) {
   BFVM_CUDA(cudaEventCreate(&e0));
   BFVM_CUDA(cudaEventCreate(&e1));
   struct Choice {
-    int kind, ch, tw, stages, minb;
+    int kind, ch, tw, stages, minb, build;
   };
   const int ns[3] = {m->nx, m->ny, m->nz};
   const int fuses[3] = {bfvm::kFuseDirPro | bfvm::kFuseDirEpi, bfvm::kFuseDirEpi, 0};
@@ -2626,15 +2667,24 @@ void tune_sweeps(bfvm_solver* m, double dt, int reps) {
         if (nc > 64) continue;
         for (int tw : {32, 16, 8})
           if (nc * tw <= bfvm::sweep_max_threads(ch))
-            cand.push_back({BFVM_PATH_GENERIC, ch, tw, 0, 1});
+            cand.push_back({BFVM_PATH_GENERIC, ch, tw, 0, 1, 0});
         // the line kernel also takes 17-32 chunks of 32 points (x: where the
         // rows are too long for the row kernel)
-        if (nc <= 16 || (ch == 32 && nc <= 32)) cand.push_back({BFVM_PATH_TMA, ch, 16, 0, 1});
+        if (nc <= 16 || (ch == 32 && nc <= 32))
+          cand.push_back({BFVM_PATH_TMA, ch, 16, 0, 1, 0});
         // the row kernel (x) with a ring of three tiles, and at 32-point
-        // chunks compiled for two blocks per SM
-        if (ax == 0 && nc <= 16) cand.push_back({BFVM_PATH_TMA, ch, 16, 3, 1});
-        if (ax == 0 && nc <= 16 && ch == 32) cand.push_back({BFVM_PATH_TMA, ch, 16, 0, 2});
-        if (nc <= 16) cand.push_back({BFVM_PATH_DIRECT, ch, 16, 0, 1});
+        // chunks compiled for two blocks per SM or for this density count
+        // (interleaved or planar tables; the plan falls back to the general
+        // build where these do not apply)
+        if (ax == 0 && nc <= 16) cand.push_back({BFVM_PATH_TMA, ch, 16, 3, 1, 0});
+        if (ax == 0 && nc <= 16 && ch == 32) {
+          cand.push_back({BFVM_PATH_TMA, ch, 16, 0, 2, 0});
+          if (row_build_count(m->S)) {
+            cand.push_back({BFVM_PATH_TMA, ch, 16, 0, 1, 1});
+            cand.push_back({BFVM_PATH_TMA, ch, 16, 0, 1, 2});
+          }
+        }
+        if (nc <= 16) cand.push_back({BFVM_PATH_DIRECT, ch, 16, 0, 1, 0});
       }
       Axis best = m->axis[ax];
       float best_ms = 1e30f;
@@ -2646,6 +2696,7 @@ void tune_sweeps(bfvm_solver* m, double dt, int reps) {
         A.minb = c.minb;
         A.kind = c.kind;
         A.stages = c.stages;
+        A.build = c.build;
         A.user = true;
         build_all(m);
         sweep(m, ax, fuses[ax], dt);  // warm-up: tables and plans
@@ -2751,6 +2802,22 @@ int bfvm_get_sweep_config(bfvm_solver* m, int axis, int* config) {
     config[1] = m->axis[axis].tw;
     config[2] = m->axis[axis].minb;
     config[3] = m->axis[axis].stages == 3 ? 3 : 2;
+  });
+}
+
+int bfvm_set_row_build(bfvm_solver* m, int build) {
+  return SOLVER_CALL(m, {
+    require(build >= 0 && build <= 2, "row build must be 0, 1 or 2");
+    m->axis[0].build = build;
+  });
+}
+
+int bfvm_get_row_build(bfvm_solver* m, int* requested, int* effective) {
+  return SOLVER_CALL(m, {
+    require(requested != nullptr && effective != nullptr, "bad arguments");
+    *requested = m->axis[0].build;
+    const RowsPlan P = plan_rows(m);
+    *effective = P.ok ? P.build : 0;
   });
 }
 

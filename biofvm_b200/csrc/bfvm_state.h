@@ -93,6 +93,9 @@ struct Axis {
   int minb = 1; // resident blocks per SM the kernel is compiled for (1 or 2)
   int kind = 0; // kernel under BFVM_PATH_AUTO: 0 = default, else a BFVM_PATH_* value
   int stages = 0;  // x row kernel: tiles in its shared-memory ring (0 = 2)
+  int build = 2;   // x row kernel: 0 any density count, 1 a build for this
+                   // density count, 2 the same reading planar tables
+                   // (bfvm_set_row_build; 2 runs where it applies)
   bool user = false;  // set through bfvm_set_sweep_config or the tuner
 };
 

@@ -255,6 +255,18 @@ class Solver:
         """Tiles in the x row kernel's shared-memory ring: 2 or 3."""
         call("bfvm_set_row_stages", self._h, stages)
 
+    def set_row_build(self, build: int) -> None:
+        """Build of the x row kernel: 0 any density count, 1 a build for this
+        density count, 2 (default) the same reading planar chunk tables
+        (FP64, 4, 8, 10 or 16 densities; elsewhere build 0 runs)."""
+        call("bfvm_set_row_build", self._h, build)
+
+    def get_row_build(self):
+        """(requested, effective) row-kernel build."""
+        req, eff = ctypes.c_int(), ctypes.c_int()
+        call("bfvm_get_row_build", self._h, ctypes.byref(req), ctypes.byref(eff))
+        return req.value, eff.value
+
     def set_kernel_path(self, path: int) -> None:
         call("bfvm_set_kernel_path", self._h, path)
 

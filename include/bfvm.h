@@ -245,6 +245,20 @@ BFVM_API int bfvm_set_sweep_config(bfvm_solver* m, int axis, int chunk, int colu
  * tile in flight while a tile is solved; fewer rows per tile where shared
  * memory runs short).  Kept until the next resize or tuning. */
 BFVM_API int bfvm_set_row_stages(bfvm_solver* m, int stages);
+/* Build of the x row kernel (a tuning choice with no counterpart in the
+ * reference, like the ring depth above): 0 any density count; 1 a build for
+ * exactly this density count, so that the offsets along a row are
+ * compile-time constants; 2 (default) that build reading the chunk tables
+ * in their planar layout.  Builds 1 and 2 exist for FP64 fields of 4, 8, 10
+ * or 16 densities at 32-point chunks with the tables in shared memory, one
+ * block per SM and a two-tile ring; elsewhere the row kernel runs build 0.
+ * Same results bit for bit.  bfvm_tune_sweeps tries all three.  Kept until
+ * the next resize or tuning. */
+BFVM_API int bfvm_set_row_build(bfvm_solver* m, int build);
+/* requested = the build set above; effective = the build the next x sweep
+ * on the row kernel runs under the current plan (0 where builds 1 and 2 do
+ * not apply, or where the row kernel does not run the x sweep). */
+BFVM_API int bfvm_get_row_build(bfvm_solver* m, int* requested, int* effective);
 /* Which sweep kernels run (all compute the same sweep):
  *   BFVM_PATH_AUTO    (default) the register kernel for x, the TMA-fed
  *                     persistent kernel for y and z where the layout allows

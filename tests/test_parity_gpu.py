@@ -570,6 +570,48 @@ def test_sweep_tuner_keeps_the_field_and_the_results(shape):
     assert np.all(rel_err(got, O.oracle_run(scn, 3, 7)) <= TOL64), chosen
 
 
+@pytest.mark.parametrize("shape,S", [((256, 12, 9), 10), ((128, 10, 6), 8), ((224, 7, 5), 10),
+                                     ((128, 12, 7), 4), ((256, 6, 5), 16)])
+def test_row_kernel_builds_for_one_density_count(shape, S):
+    """The x row kernel compiled for exactly S densities (constant offsets
+    along the rows), with interleaved and with planar chunk tables: the same
+    arithmetic as the general build, so bit-identical results, and within
+    the oracle bar; the plan reports the build it runs."""
+    scn = W.mixed_small(shape=shape, S=S, n_agents=500, seed=sum(shape) + 3 * S)
+    ref = O.oracle_run(scn, 3, 7)
+    got = {}
+    for build in (0, 1, 2):
+        with Solver(0) as sv:
+            load_scenario(sv, scn)
+            sv.set_kernel_path(PATH_TMA)
+            sv.set_sweep_config(0, 32, 16, 1)
+            sv.set_row_build(build)
+            sv.step(scn.dt, 3)
+            assert sv.get_row_build() == (build, build)
+            got[build] = sv.get_densities()
+        assert np.all(rel_err(got[build], ref) <= TOL64), build
+    assert np.array_equal(got[1], got[0]) and np.array_equal(got[2], got[0])
+
+
+def test_row_build_falls_back_where_it_does_not_apply():
+    """Builds 1 and 2 exist for 4, 8, 10 and 16 densities only: with 6
+    densities the general build runs (effective 0) and the sweep still meets
+    the oracle; a solver starts with build 2 requested."""
+    scn = W.mixed_small(shape=(128, 9, 5), S=6, n_agents=300, seed=77)
+    with Solver(0) as sv:
+        load_scenario(sv, scn)
+        assert sv.get_row_build()[0] == 2
+        sv.set_kernel_path(PATH_TMA)
+        sv.set_sweep_config(0, 32, 16, 1)
+        sv.set_row_build(2)
+        sv.step(scn.dt, 3)
+        assert sv.get_row_build() == (2, 0)
+        got = sv.get_densities()
+        with pytest.raises(BfvmError):
+            sv.set_row_build(3)
+    assert np.all(rel_err(got, O.oracle_run(scn, 3, 7)) <= TOL64)
+
+
 @pytest.mark.parametrize("shape,S", [((256, 12, 9), 10), ((160, 20, 7), 4), ((96, 9, 5), 7)])
 def test_row_kernel_with_three_stage_ring(shape, S):
     """The x row kernel with a ring of three tiles (and whole warps per

@@ -132,20 +132,23 @@ class ClockSampler:
 TRAFFIC_PROFILE = os.path.join(ROOT, "profiles", "sweeps_traffic_lod256.json")
 
 
-def ncu_traffic(axis_key: str, kernel_kind: int):
+def ncu_traffic(axis_key: str, kernel_kind: int, chunk: int, row_build: int):
     """DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch
     of the sweep kernel of an axis at the full 256^3 x 10 size, from the
     one-pass ncu capture recorded in profiles/sweeps_traffic_lod256.json
     (the capture's command is in the file).  None when the file lacks the
-    axis or the capture ran another kernel than the one timed here
-    (kernel_kind: the tuner's choice, a BFVM_PATH_* value, 0 = the default,
-    which the capture ran)."""
+    axis or the capture ran another kernel than the one timed here: another
+    kernel kind (kernel_kind: the tuner's choice, a BFVM_PATH_* value, 0 =
+    the default, which the capture ran), chunk length or x row-kernel
+    build."""
     if not os.path.exists(TRAFFIC_PROFILE):
         return None, None
     with open(TRAFFIC_PROFILE) as f:
         d = json.load(f)
     k = d.get("launches", {}).get(axis_key)
     if not k or (kernel_kind != 0 and kernel_kind != k.get("path")):
+        return None, None
+    if k.get("chunk") != chunk or (axis_key == "x_sweep" and k.get("row_build") != row_build):
         return None, None
     return float(k["dram_bytes_read"]) + float(k["dram_bytes_write"]), k["kernel"]
 
@@ -336,6 +339,9 @@ def run_ours(args, world, rank, local):
     # the per-axis kernel choice timed on this field (which is restored)
     sv.step(dt, args.warmup, STEP_ALL)
     tuned = sv.tune_sweeps(dt, 3) if not args.no_tune else [(0, 0, 0, 0, 0)] * 3
+    if args.sweep_chunks:
+        for ax, ch in enumerate(int(c) for c in args.sweep_chunks.split(",")):
+            sv.set_sweep_config(ax, ch, 16, 1)
     if args.row_build is not None:
         sv.set_row_build(args.row_build)
     row_build = sv.get_row_build()
@@ -374,8 +380,9 @@ def run_ours(args, world, rank, local):
     hbm, peak_kind = peaks()
     achieved = sweeps_in[dom] * BYTES_PER_VS_SWEEP * N * S / (per[dom] / 1e3) / 1e9
     dom_axis = {"x_sweep": 0, "y_sweep": 1, "z_sweep": 2}.get(dom)
-    traffic, traffic_kernel = (ncu_traffic(dom, tuned[dom_axis][0]) if dom_axis is not None
-                               else (None, None))
+    traffic, traffic_kernel = (ncu_traffic(dom, tuned[dom_axis][0],
+                                           sv.get_sweep_config(dom_axis)[0], row_build[1])
+                               if dom_axis is not None else (None, None))
 
     # end to end through the C ABI with host buffers: every step uploads the
     # agents' voxels and secretion/uptake constants (as when agents move and
@@ -1289,6 +1296,9 @@ def main():
     ap.add_argument("--row-build", type=int, choices=[0, 1, 2], default=None,
                     help="lod256: x row-kernel build after tuning (0 any density count, "
                          "1 built for this density count, 2 the same with planar tables)")
+    ap.add_argument("--sweep-chunks", default=None,
+                    help="lod256: chunk lengths of the x, y and z sweeps after tuning, "
+                         "e.g. 32,32,16")
     ap.add_argument("--no-tune", action="store_true",
                     help="keep the default kernel per axis (for profiler launch lists)")
     ap.add_argument("--size", type=int, default=256, help="cube edge in voxels (default 256)")

@@ -340,8 +340,11 @@ def run_ours(args, world, rank, local):
     sv.step(dt, args.warmup, STEP_ALL)
     tuned = sv.tune_sweeps(dt, 3) if not args.no_tune else [(0, 0, 0, 0, 0)] * 3
     if args.sweep_chunks:
+        # only where the chunk length changes: a set configuration also
+        # returns the axis to its default kernel kind
         for ax, ch in enumerate(int(c) for c in args.sweep_chunks.split(",")):
-            sv.set_sweep_config(ax, ch, 16, 1)
+            if sv.get_sweep_config(ax)[0] != ch:
+                sv.set_sweep_config(ax, ch, 16, 1)
     if args.row_build is not None:
         sv.set_row_build(args.row_build)
     row_build = sv.get_row_build()

@@ -255,9 +255,9 @@ BFVM_API int bfvm_set_row_stages(bfvm_solver* m, int stages);
  * Same results bit for bit.  bfvm_tune_sweeps tries all three.  Kept until
  * the next resize or tuning. */
 BFVM_API int bfvm_set_row_build(bfvm_solver* m, int build);
-/* requested = the build set above; effective = the build the next x sweep
- * on the row kernel runs under the current plan (0 where builds 1 and 2 do
- * not apply, or where the row kernel does not run the x sweep). */
+/* requested = the build set above; effective = the build the row kernel
+ * runs under the current plan when it sweeps x (0 where builds 1 and 2 do
+ * not apply). */
 BFVM_API int bfvm_get_row_build(bfvm_solver* m, int* requested, int* effective);
 /* Which sweep kernels run (all compute the same sweep):
  *   BFVM_PATH_AUTO    (default) the register kernel for x, the TMA-fed

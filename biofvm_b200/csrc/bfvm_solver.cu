@@ -814,7 +814,7 @@ RowsPlan plan_rows(const bfvm_solver* m) {
   P.ch = m->axis[0].ch;
   P.nc = (m->nx + P.ch - 1) / P.ch;
   const int cols = m->S * P.nc;  // threads of one row
-  if (cols > 512) return P;
+  if (cols <= 0 || cols > 512) return P;
   // pitch: row_elems rounded up so that pitch == S (mod 16 elements of 8 B,
   // 32 of 4 B) and pitch*es is a multiple of 16 bytes
   const int64_t mod = (es == 8) ? 16 : 32, step = 16 / es;

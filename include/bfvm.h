@@ -257,7 +257,7 @@ BFVM_API int bfvm_set_row_stages(bfvm_solver* m, int stages);
 BFVM_API int bfvm_set_row_build(bfvm_solver* m, int build);
 /* requested = the build set above; effective = the build the row kernel
  * runs under the current plan when it sweeps x (0 where builds 1 and 2 do
- * not apply). */
+ * not apply, and before the first sweep has built the chunk tables). */
 BFVM_API int bfvm_get_row_build(bfvm_solver* m, int* requested, int* effective);
 /* Which sweep kernels run (all compute the same sweep):
  *   BFVM_PATH_AUTO    (default) the register kernel for x, the TMA-fed
